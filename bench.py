@@ -1,0 +1,383 @@
+"""Benchmark of the rank + IC hot path (cs_rank + rolling_ic over F factors).
+
+Workload: T=1218 dates x N=5000 stocks x F=12 factors, f32 -- the corpus shape
+the reference publishes its numbers on.  Synthetic, seeded: 6 Gaussian, 3
+lognormal(sigma=1), 3 Student-t(3) factors; per-stock pre-listing gaps plus 1%
+random NaN (~8% missing); 5% of values rounded to 1e-3 (ties); forward returns
+0.03*factor0 + t(4) noise.  One step = cs_rank of every factor (ranks written)
+plus the daily Spearman IC of every factor against the forward returns.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--method radix|learned]
+
+Prints one JSON line (rank 0).  ``value`` is device-resident throughput
+(inputs in HBM, CUDA events on the launching stream, inputs larger than L2
+so no flush is needed); ``e2e`` is the same metric through the C ABI host
+entry point with pinned host buffers (copies inside the timed region).
+With --gpus N (torchrun) every rank runs an independent replica of the
+workload on its own GPU ("replicas only": the path has no exchange step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+PKG = ROOT / "factor-cuda_b200"
+for _p in (str(ROOT), str(PKG)):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+T_DEF, N_DEF, F_DEF = 1218, 5000, 12
+MIN_VALID = 30
+METRIC = "rank+IC Gelem/s @1218x5000x12"
+
+
+# ---------------------------------------------------------------- workload
+def make_panel(T=T_DEF, N=N_DEF, F=F_DEF, seed=20261203):
+    """Seeded synthetic stand-in for the 1218x5000x12 corpus panel."""
+    rng = np.random.default_rng(seed)
+    X = np.empty((F, T, N), np.float32)
+    for f in range(F):
+        if f < 6:
+            X[f] = rng.standard_normal((T, N), dtype=np.float32)
+        elif f < 9:
+            X[f] = rng.lognormal(0.0, 1.0, (T, N)).astype(np.float32)
+        else:
+            X[f] = rng.standard_t(3, (T, N)).astype(np.float32)
+    start = rng.integers(0, max(1, int(0.14 * T)), N)       # pre-listing gaps (~7%)
+    listed = np.arange(T)[:, None] >= start[None, :]
+    nan_cells = rng.random((F, T, N)) < 0.01                 # 1% random NaN
+    X[nan_cells] = np.nan
+    X[:, ~listed] = np.nan
+    tie = rng.random((F, T, N)) < 0.05                       # ties
+    X[tie] = np.round(X[tie], 3)
+    R = (0.03 * np.nan_to_num(X[0]) + rng.standard_t(4, (T, N))).astype(np.float32)
+    R[~listed] = np.nan
+    fmask = listed.astype(np.uint8)
+    rmask = np.isfinite(R).astype(np.uint8)
+    return X, R, fmask, rmask
+
+
+def algorithmic_bytes(F, T, N):
+    """Bytes one launch must move: factor read + rank write (4+4 B/cell),
+    returns + two masks per (t,i) (4+1+1 B), IC out (8 B per (f,t))."""
+    return F * T * N * 8 + T * N * 6 + F * T * 8
+
+
+# ---------------------------------------------------------------- helpers
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.idx)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU legs
+def _cpu_work(args):
+    import sys as _s
+    _s.path.insert(0, str(ROOT))
+    from oracle import fc_oracle as O
+    X, R, fm, rm = args
+    t0 = time.perf_counter()
+    for f in range(X.shape[0]):
+        O.cs_rank(X[f], fm.astype(bool), False)
+        O.rolling_ic(X[f], R, fm.astype(bool), rm.astype(bool), MIN_VALID)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(X, R, fm, rm, budget_s=12.0, procs=1):
+    """Oracle port timed on a bounded sample of dates (all factors)."""
+    F, T, N = X.shape
+    per = 16
+    chunks = []
+    for t0 in range(0, T, per):
+        chunks.append((X[:, t0:t0 + per], R[t0:t0 + per], fm[t0:t0 + per], rm[t0:t0 + per]))
+    done_cells = 0
+    t_start = time.perf_counter()
+    if procs <= 1:
+        for c in chunks:
+            _cpu_work(c)
+            done_cells += c[0].size
+            if time.perf_counter() - t_start > budget_s:
+                break
+        el = time.perf_counter() - t_start
+    else:
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        n = 0
+        with ctx.Pool(procs) as pool:
+            t_start = time.perf_counter()
+            while time.perf_counter() - t_start < budget_s and n < len(chunks):
+                batch = chunks[n:n + procs]
+                pool.map(_cpu_work, batch)
+                done_cells += sum(c[0].size for c in batch)
+                n += len(batch)
+            el = time.perf_counter() - t_start
+    dates = done_cells // (F * N)
+    return done_cells / el / 1e9, el, dates
+
+
+# ---------------------------------------------------------------- GPU legs
+def run_b200(args, rank, world):
+    import torch
+    from fcb200 import _native as nat
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    lib = nat.lib()
+    X, R, fm, rm = make_panel(T=args.T, N=args.N, F=args.F, seed=20261203 + rank)
+    F, T, N = X.shape
+    method = {"radix": 0, "learned": 1}[args.method]
+    dX = torch.from_numpy(X).to(dev)
+    dR = torch.from_numpy(R).to(dev)
+    dfm = torch.from_numpy(fm).to(dev)
+    drm = torch.from_numpy(rm).to(dev)
+    dranks = torch.empty((F, T, N), dtype=torch.float32, device=dev)
+    dic = torch.empty((F, T), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        rc = lib.fcb_dev_rank_ic_panel(dX.data_ptr(), dR.data_ptr(), dfm.data_ptr(), drm.data_ptr(), F, T, N,
+                                       MIN_VALID, dranks.data_ptr(), dic.data_ptr(), method, stream.cuda_stream)
+        nat.check(rc, "fcb_dev_rank_ic_panel")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    # parity spot check of the timed outputs against the oracle (a few dates)
+    spot = check_spot(X, R, fm, rm, dranks, dic)
+
+    # e2e: host entry point, pinned buffers, copies in the timed region
+    if args.no_e2e:
+        return finish(args, world, X, R, fm, rm, ms, None, None, clk, spot, dev)
+    hX = torch.from_numpy(X).pin_memory()
+    hR = torch.from_numpy(R).pin_memory()
+    hfm = torch.from_numpy(fm).pin_memory()
+    hrm = torch.from_numpy(rm).pin_memory()
+    hranks = torch.empty((F, T, N), dtype=torch.float32).pin_memory()
+    hic = torch.empty((F, T), dtype=torch.float64).pin_memory()
+    ws = lib.fcb_workspace_create()
+
+    def host_step():
+        rc = lib.fcb_rank_ic_panel(hX.data_ptr(), hR.data_ptr(), hfm.data_ptr(), hrm.data_ptr(), F, T, N,
+                                   MIN_VALID, hranks.data_ptr(), hic.data_ptr(), method, ws)
+        nat.check(rc, "fcb_rank_ic_panel")
+
+    for _ in range(max(1, args.warmup)):
+        host_step()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        host_step()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    lib.fcb_workspace_destroy(ws)
+    e2e_ok = bool(np.array_equal(hranks.numpy().view(np.uint32), dranks.cpu().numpy().view(np.uint32)))
+    return finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev)
+
+
+def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev):
+    import torch
+    F, T, N = X.shape
+    ms_all, e2e_all = ms, (e2e_s if e2e_s is not None else 0.0)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_all, e2e_all = float(t[0]), float(t[1])
+    cells = F * T * N
+    peak, peak_kind = measured_peaks()
+    bytes_launch = algorithmic_bytes(F, T, N)
+    achieved = bytes_launch / (ms / 1e3) / 1e9
+    res = {
+        "metric": METRIC, "value": world * cells / (ms_all / 1e3) / 1e9, "unit": "Gelem/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded stand-in for the 1218x5000x12 corpus panel)",
+        "config": {"workload": "cs_rank + rolling_ic(min_valid=30), F=12 factor panels vs one "
+                               "forward-return panel", "T": T, "N": N, "F": F, "method": args.method,
+                   "parallelism": f"replicas{world}",
+                   "l2": "inputs (292 MB factors) larger than the 126 MB L2; no flush"},
+        "e2e": None if e2e_s is None else {"value": world * cells / e2e_all / 1e9, "unit": "Gelem/s",
+                "h2d_bytes_per_step": int(X.nbytes + R.nbytes + fm.nbytes + rm.nbytes),
+                "d2h_bytes_per_step": int(F * T * N * 4 + F * T * 8),
+                "api": "fcb_rank_ic_panel (C ABI, pinned host buffers, date-chunked streaming)",
+                "matches_device_path": e2e_ok},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                     "kernel": "k_rank_ic", "algorithmic_bytes_per_launch": bytes_launch},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+        "parity_spot_check": spot,
+    }
+    return res
+
+
+def check_spot(X, R, fm, rm, dranks, dic):
+    from oracle import fc_oracle as O
+    F, T, N = X.shape
+    ts = [0, T // 2, T - 1]
+    ok = True
+    for f in (0, F - 1):
+        sl = slice(ts[1], ts[1] + 2)
+        exp_r = O.cs_rank(X[f, sl], fm[sl].astype(bool), False)
+        got_r = dranks[f, sl].cpu().numpy()
+        ok &= bool(np.array_equal(exp_r.view(np.uint32), got_r.view(np.uint32)))
+        exp_ic = O.rolling_ic(X[f, sl], R[sl], fm[sl].astype(bool), rm[sl].astype(bool), MIN_VALID)
+        got_ic = dic[f, sl].cpu().numpy()
+        ok &= bool(np.array_equal(np.nan_to_num(exp_ic, nan=7.0), np.nan_to_num(got_ic, nan=7.0)))
+    return "bit-exact" if ok else "MISMATCH"
+
+
+def run_reference(args):
+    """The reference arm: the oracle port of the reference CPU path
+    (fc/_cpu_core.py np_cs_rank + np_rolling_ic) on the host cores."""
+    X, R, fm, rm = make_panel()
+    F, T, N = X.shape
+    procs = max(1, min(os.cpu_count() or 1, 32))
+    for _ in range(args.warmup):
+        cpu_baseline(X, R, fm, rm, budget_s=1.0, procs=1)
+    vals = []
+    els = []
+    for _ in range(args.steps):
+        v, el, dates = cpu_baseline(X, R, fm, rm, budget_s=6.0, procs=procs)
+        vals.append(v)
+        els.append(el)
+    v = statistics.median(vals)
+    return {
+        "metric": METRIC, "value": v, "unit": "Gelem/s", "impl": "reference", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(els) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded stand-in for the 1218x5000x12 corpus panel)",
+        "config": {"workload": "cs_rank + rolling_ic(min_valid=30), F=12 factor panels vs one "
+                               "forward-return panel", "T": T, "N": N, "F": F},
+        "cpu_baseline": {"value": v, "unit": "Gelem/s", "cores": procs, "kind": "port",
+                         "sample": "16-date chunks of all 12 factors, ~6 s per step, spawn pool"},
+        "e2e": {"value": v, "unit": "Gelem/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--method", choices=["radix", "learned"], default="radix")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--T", type=int, default=T_DEF)
+    ap.add_argument("--N", type=int, default=N_DEF)
+    ap.add_argument("--F", type=int, default=F_DEF)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_b200(args, rank, world)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            X, R, fm, rm = make_panel()
+            v, el, dates = cpu_baseline(X, R, fm, rm, budget_s=12.0, procs=1)
+            res["cpu_baseline"] = {"value": v, "unit": "Gelem/s", "cores": 1, "kind": "port",
+                                   "sample": f"{dates} dates x 12 factors x 5000 stocks "
+                                             f"({el:.1f} s, single thread, oracle port of "
+                                             "np_cs_rank + np_rolling_ic)"}
+        print(json.dumps(res))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

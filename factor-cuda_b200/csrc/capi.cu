@@ -1,0 +1,566 @@
+// capi.cu -- host drivers behind the C ABI (include/fcb200.h).
+//
+// Each entry point validates its arguments with the reference's status codes,
+// acquires device buffers from a workspace arena (cached across calls when the
+// caller passes a workspace, temporary otherwise), uploads, launches, downloads
+// and synchronises.  Device buffers are accounted (live / high-water bytes),
+// the equivalent of the reference's MemTracker (src/mem_tracker.cu:15-68).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/fcb200.h"
+#include "fcb_kernels.h"
+
+using namespace fcb;
+
+// ---------------------------------------------------------------------------
+// workspace arena
+// ---------------------------------------------------------------------------
+enum Slot : int {
+  S_X = 0, S_X2, S_MASK, S_MASK2, S_OUT, S_OUT1, S_OUT2, S_OUT3, S_STATUS, S_IC, S_RF, S_RR,
+  S_SC_RAW, S_SC_C, S_SC_M, S_SC_ST, S_SC_SUM, S_FB_LIST, S_FB_CNT,
+  S_FC_COLPART, S_FC_COLSTAT, S_FC_GRAM, S_FC_FLAGS,
+  // streamed panel: two chunk buffers each
+  S_PX0, S_PX1, S_PR0, S_PR1, S_PFM0, S_PFM1, S_PRM0, S_PRM1, S_PRK0, S_PRK1, S_PIC0, S_PIC1,
+  S_COUNT
+};
+
+struct fcb_workspace {
+  int device = -1;
+  cudaStream_t stream[2] = {nullptr, nullptr};
+  void* ptr[S_COUNT] = {};
+  size_t cap[S_COUNT] = {};
+  uint64_t live = 0, peak = 0, nalloc = 0;
+
+  cudaError_t bind() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev != device) {
+      release();
+      device = dev;
+    }
+    for (int i = 0; i < 2; ++i)
+      if (stream[i] == nullptr) {
+        e = cudaStreamCreateWithFlags(&stream[i], cudaStreamNonBlocking);
+        if (e != cudaSuccess) return e;
+      }
+    return cudaSuccess;
+  }
+  template <typename T>
+  cudaError_t get(Slot s, size_t bytes, T** out) {
+    if (bytes == 0) bytes = 16;
+    if (cap[s] < bytes) {
+      if (ptr[s] != nullptr) {
+        cudaFree(ptr[s]);
+        live -= cap[s];
+        ptr[s] = nullptr;
+        cap[s] = 0;
+      }
+      cudaError_t e = cudaMalloc(&ptr[s], bytes);
+      if (e != cudaSuccess) {
+        ptr[s] = nullptr;
+        return e;
+      }
+      cap[s] = bytes;
+      live += bytes;
+      ++nalloc;
+      if (live > peak) peak = live;
+    }
+    *out = static_cast<T*>(ptr[s]);
+    return cudaSuccess;
+  }
+  void release() {
+    for (int s = 0; s < S_COUNT; ++s) {
+      if (ptr[s] != nullptr) cudaFree(ptr[s]);
+      ptr[s] = nullptr;
+      cap[s] = 0;
+    }
+    for (int i = 0; i < 2; ++i) {
+      if (stream[i] != nullptr) cudaStreamDestroy(stream[i]);
+      stream[i] = nullptr;
+    }
+    live = 0;
+  }
+};
+
+namespace {
+
+// RAII: the caller's workspace, or a temporary one released on return.
+struct WsScope {
+  fcb_workspace* ws;
+  fcb_workspace tmp;
+  explicit WsScope(fcb_workspace* w) : ws(w != nullptr ? w : &tmp) {}
+  ~WsScope() {
+    if (ws == &tmp) tmp.release();
+  }
+};
+
+inline int rc(cudaError_t e) { return static_cast<int>(e); }
+
+#define FCB_TRY(...)                           \
+  do {                                         \
+    cudaError_t _e = (__VA_ARGS__);            \
+    if (_e != cudaSuccess) return rc(_e);      \
+  } while (0)
+
+// Read and check the device status word after a synchronising copy.
+int check_status(const int* h_status) { return *h_status != 0 ? FCB_ERR_DEVICE_WAIT : FCB_OK; }
+
+bool is_group_whitelist(cudaError_t e) {
+  return e == cudaErrorInvalidConfiguration || e == cudaErrorLaunchOutOfResources;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// housekeeping
+// ---------------------------------------------------------------------------
+extern "C" fcb_workspace* fcb_workspace_create(void) { return new (std::nothrow) fcb_workspace(); }
+
+extern "C" void fcb_workspace_clear(fcb_workspace* ws) {
+  if (ws != nullptr) ws->release();
+}
+
+extern "C" void fcb_workspace_destroy(fcb_workspace* ws) {
+  if (ws == nullptr) return;
+  ws->release();
+  delete ws;
+}
+
+extern "C" int fcb_workspace_stats(const fcb_workspace* ws, uint64_t* live, uint64_t* peak, uint64_t* n) {
+  if (ws == nullptr) return FCB_ERR_ARG;
+  if (live) *live = ws->live;
+  if (peak) *peak = ws->peak;
+  if (n) *n = ws->nalloc;
+  return FCB_OK;
+}
+
+extern "C" int fcb_version(void) { return 10000; }
+
+extern "C" int fcb_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+extern "C" const char* fcb_status_string(int s) {
+  switch (s) {
+    case FCB_OK: return "ok";
+    case FCB_ERR_ARG: return "null pointer or dimension < 1";
+    case FCB_ERR_CAP2: return "size cap exceeded (-2)";
+    case FCB_ERR_CAP3: return "size cap exceeded (-3)";
+    case FCB_ERR_CAP4: return "domain / min_valid contract violated (-4)";
+    case FCB_ERR_UNSUPPORTED: return "request not supported by this build";
+    case FCB_ERR_DEVICE_WAIT: return "a bounded device-side wait gave up";
+    default: return s > 0 ? cudaGetErrorString(static_cast<cudaError_t>(s)) : "contract error";
+  }
+}
+
+extern "C" void* fcb_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+  return p;
+}
+
+extern "C" void fcb_host_free(void* p) {
+  if (p != nullptr) cudaFreeHost(p);
+}
+
+// ---------------------------------------------------------------------------
+// cs_rank
+// ---------------------------------------------------------------------------
+extern "C" int fcb_dev_cs_rank_f32(const float* d_x, const uint8_t* d_mask, int T, int N, int desc, float* d_out,
+                                   void* stream) {
+  if (d_x == nullptr || d_out == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
+  if (N > (1 << 24)) return FCB_ERR_CAP2;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
+  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
+  static int* d_status = nullptr;  // status sink for the asynchronous variant
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (d_status == nullptr) FCB_TRY(cudaMalloc(&d_status, sizeof(int)));
+  }
+  return rc(launch_cs_rank(d_x, d_mask, T, N, desc, d_out, d_status, static_cast<cudaStream_t>(stream)));
+}
+
+extern "C" int fcb_cs_rank_f32(const float* x, const uint8_t* mask, int T, int N, int desc, float* out,
+                               fcb_workspace* wsp) {
+  if (x == nullptr || out == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
+  if (N > (1 << 24)) return FCB_ERR_CAP2;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
+  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
+  WsScope sc(wsp);
+  fcb_workspace& ws = *sc.ws;
+  FCB_TRY(ws.bind());
+  cudaStream_t s = ws.stream[0];
+  const size_t n = static_cast<size_t>(T) * N;
+  float *dx, *dout;
+  uint8_t* dm = nullptr;
+  int* dst;
+  FCB_TRY(ws.get(S_X, n * 4, &dx));
+  FCB_TRY(ws.get(S_OUT, n * 4, &dout));
+  FCB_TRY(ws.get(S_STATUS, 64, &dst));
+  if (mask != nullptr) FCB_TRY(ws.get(S_MASK, n, &dm));
+  FCB_TRY(cudaMemcpyAsync(dx, x, n * 4, cudaMemcpyHostToDevice, s));
+  if (mask != nullptr) FCB_TRY(cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, s));
+  FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), s));
+  FCB_TRY(launch_cs_rank(dx, dm, T, N, desc, dout, dst, s));
+  int hst = 0;
+  FCB_TRY(cudaMemcpyAsync(out, dout, n * 4, cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaMemcpyAsync(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaStreamSynchronize(s));
+  return check_status(&hst);
+}
+
+// ---------------------------------------------------------------------------
+// parameter_scan
+// ---------------------------------------------------------------------------
+extern "C" int fcb_parameter_scan_f32(const float* x, const uint8_t* mask, int T, int N, float* const out[4],
+                                      int group_status[4], double time_ms[4], float time_gpu_ms[4],
+                                      const int active[4], fcb_workspace* wsp) {
+  if (group_status != nullptr)
+    for (int g = 0; g < 4; ++g) group_status[g] = FCB_GROUP_NOT_EXECUTED;
+  if (x == nullptr || out == nullptr || group_status == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
+  int act[4];
+  int nact = 0;
+  for (int g = 0; g < 4; ++g) {
+    act[g] = (active == nullptr || active[g]) ? 1 : 0;
+    if (act[g] && out[g] == nullptr) return FCB_ERR_ARG;
+    nact += act[g];
+  }
+  if (N > (1 << 24)) return FCB_ERR_CAP2;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
+  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
+  for (int g = 0; g < 4; ++g) {
+    if (time_ms) time_ms[g] = 0.0;
+    if (time_gpu_ms) time_gpu_ms[g] = 0.0f;
+  }
+  WsScope sc(wsp);
+  fcb_workspace& ws = *sc.ws;
+  FCB_TRY(ws.bind());
+  cudaStream_t s = ws.stream[0];
+  const size_t n = static_cast<size_t>(T) * N;
+  float* dx;
+  uint8_t* dm = nullptr;
+  int* dst;
+  FCB_TRY(ws.get(S_X, n * 4, &dx));
+  FCB_TRY(ws.get(S_STATUS, 64, &dst));
+  if (mask != nullptr) FCB_TRY(ws.get(S_MASK, n, &dm));
+  ScanOut so{};
+  const Slot oslot[4] = {S_OUT, S_OUT1, S_OUT2, S_OUT3};
+  for (int g = 0; g < 4; ++g)
+    if (act[g]) FCB_TRY(ws.get(oslot[g], n * 4, &so.out[g]));
+  FCB_TRY(cudaMemcpyAsync(dx, x, n * 4, cudaMemcpyHostToDevice, s));
+  if (mask != nullptr) FCB_TRY(cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, s));
+  FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), s));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  FCB_TRY(cudaEventCreate(&e0));
+  cudaError_t e = cudaEventCreate(&e1);
+  if (e != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return rc(e);
+  }
+  auto cleanup = [&]() {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  };
+  e = cudaEventRecord(e0, s);
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaError_t le = (e == cudaSuccess) ? launch_param_scan(dx, dm, T, N, so, dst, s) : e;
+  if (le != cudaSuccess) {
+    cudaError_t se = cudaStreamSynchronize(s);
+    cleanup();
+    if (is_group_whitelist(le) && se == cudaSuccess) {
+      for (int g = 0; g < 4; ++g)
+        if (act[g]) group_status[g] = rc(le);
+      return FCB_OK;  // every active group failed at launch; results None
+    }
+    return rc(le);
+  }
+  e = cudaEventRecord(e1, s);
+  int hst = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost, s);
+  for (int g = 0; g < 4 && e == cudaSuccess; ++g)
+    if (act[g]) e = cudaMemcpyAsync(out[g], so.out[g], n * 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  const auto t1 = std::chrono::steady_clock::now();
+  float gpu_ms = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&gpu_ms, e0, e1);
+  cleanup();
+  if (e != cudaSuccess) return rc(e);
+  if (hst != 0) return FCB_ERR_DEVICE_WAIT;
+  const double host_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  for (int g = 0; g < 4; ++g) {
+    if (!act[g]) continue;
+    group_status[g] = 0;
+    if (time_ms) time_ms[g] = host_ms / nact;
+    if (time_gpu_ms) time_gpu_ms[g] = gpu_ms / static_cast<float>(nact);
+  }
+  return FCB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// rolling_ic (single factor) and the batched panel
+// ---------------------------------------------------------------------------
+template <typename TF, typename TR>
+static int run_rank_ic(const RankIcArgs<TF, TR>& a, int* dst, cudaStream_t s) {
+  return rc(launch_rank_ic<TF, TR>(a, dst, s));
+}
+
+extern "C" int fcb_rolling_ic(const void* f, int fdt, const void* r, int rdt, const uint8_t* fmask,
+                              const uint8_t* rmask, int T, int N, int min_valid, double* ic, double* rank_f,
+                              double* rank_r, fcb_workspace* wsp) {
+  if (f == nullptr || r == nullptr || ic == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
+  if ((rank_f == nullptr) != (rank_r == nullptr)) return FCB_ERR_ARG;
+  if (min_valid < 2) return FCB_ERR_CAP4;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
+  if ((fdt != FCB_DTYPE_F32 && fdt != FCB_DTYPE_F64) || (rdt != FCB_DTYPE_F32 && rdt != FCB_DTYPE_F64))
+    return FCB_ERR_ARG;
+  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
+  WsScope sc(wsp);
+  fcb_workspace& ws = *sc.ws;
+  FCB_TRY(ws.bind());
+  cudaStream_t s = ws.stream[0];
+  const size_t n = static_cast<size_t>(T) * N;
+  const size_t fsz = fdt == FCB_DTYPE_F32 ? 4 : 8, rsz = rdt == FCB_DTYPE_F32 ? 4 : 8;
+  void *df, *dr;
+  uint8_t *dfm = nullptr, *drm = nullptr;
+  double *dic, *drf = nullptr, *drr = nullptr;
+  int* dst;
+  FCB_TRY(ws.get(S_X, n * fsz, &df));
+  FCB_TRY(ws.get(S_X2, n * rsz, &dr));
+  FCB_TRY(ws.get(S_IC, static_cast<size_t>(T) * 8, &dic));
+  FCB_TRY(ws.get(S_STATUS, 64, &dst));
+  if (fmask) FCB_TRY(ws.get(S_MASK, n, &dfm));
+  if (rmask) FCB_TRY(ws.get(S_MASK2, n, &drm));
+  if (rank_f) {
+    FCB_TRY(ws.get(S_RF, n * 8, &drf));
+    FCB_TRY(ws.get(S_RR, n * 8, &drr));
+  }
+  FCB_TRY(cudaMemcpyAsync(df, f, n * fsz, cudaMemcpyHostToDevice, s));
+  FCB_TRY(cudaMemcpyAsync(dr, r, n * rsz, cudaMemcpyHostToDevice, s));
+  if (fmask) FCB_TRY(cudaMemcpyAsync(dfm, fmask, n, cudaMemcpyHostToDevice, s));
+  if (rmask) FCB_TRY(cudaMemcpyAsync(drm, rmask, n, cudaMemcpyHostToDevice, s));
+  FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), s));
+  int e;
+  if (fdt == FCB_DTYPE_F32 && rdt == FCB_DTYPE_F32)
+    e = run_rank_ic(RankIcArgs<float, float>{static_cast<const float*>(df), static_cast<const float*>(dr), dfm, drm,
+                                             1, T, N, min_valid, nullptr, dic, drf, drr},
+                    dst, s);
+  else if (fdt == FCB_DTYPE_F32)
+    e = run_rank_ic(RankIcArgs<float, double>{static_cast<const float*>(df), static_cast<const double*>(dr), dfm,
+                                              drm, 1, T, N, min_valid, nullptr, dic, drf, drr},
+                    dst, s);
+  else if (rdt == FCB_DTYPE_F32)
+    e = run_rank_ic(RankIcArgs<double, float>{static_cast<const double*>(df), static_cast<const float*>(dr), dfm,
+                                              drm, 1, T, N, min_valid, nullptr, dic, drf, drr},
+                    dst, s);
+  else
+    e = run_rank_ic(RankIcArgs<double, double>{static_cast<const double*>(df), static_cast<const double*>(dr),
+                                               dfm, drm, 1, T, N, min_valid, nullptr, dic, drf, drr},
+                    dst, s);
+  if (e != 0) return e;
+  int hst = 0;
+  FCB_TRY(cudaMemcpyAsync(ic, dic, static_cast<size_t>(T) * 8, cudaMemcpyDeviceToHost, s));
+  if (rank_f) {
+    FCB_TRY(cudaMemcpyAsync(rank_f, drf, n * 8, cudaMemcpyDeviceToHost, s));
+    FCB_TRY(cudaMemcpyAsync(rank_r, drr, n * 8, cudaMemcpyDeviceToHost, s));
+  }
+  FCB_TRY(cudaMemcpyAsync(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaStreamSynchronize(s));
+  return check_status(&hst);
+}
+
+static int panel_args_check(const void* x, const void* r, const double* ic, int F, int T, int N, int min_valid,
+                            int method) {
+  if (x == nullptr || r == nullptr || ic == nullptr || F < 1 || T < 1 || N < 1) return FCB_ERR_ARG;
+  if (min_valid < 2) return FCB_ERR_CAP4;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
+  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
+  if (method != 0) return FCB_ERR_UNSUPPORTED;
+  return FCB_OK;
+}
+
+extern "C" int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const uint8_t* d_fmask,
+                                     const uint8_t* d_rmask, int F, int T, int N, int min_valid, float* d_ranks,
+                                     double* d_ic, int method, void* stream) {
+  const int chk = panel_args_check(d_x, d_r, d_ic, F, T, N, min_valid, method);
+  if (chk != FCB_OK) return chk;
+  static int* d_status = nullptr;
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (d_status == nullptr) FCB_TRY(cudaMalloc(&d_status, sizeof(int)));
+  }
+  RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr};
+  return rc(launch_rank_ic<float, float>(a, d_status, static_cast<cudaStream_t>(stream)));
+}
+
+// Host panel: dates are streamed in chunks over two streams so that the
+// upload of chunk k+1 and the download of chunk k-1 overlap the kernel on k.
+extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* fmask, const uint8_t* rmask,
+                                 int F, int T, int N, int min_valid, float* ranks, double* ic, int method,
+                                 fcb_workspace* wsp) {
+  const int chk = panel_args_check(x, r, ic, F, T, N, min_valid, method);
+  if (chk != FCB_OK) return chk;
+  WsScope sc(wsp);
+  fcb_workspace& ws = *sc.ws;
+  FCB_TRY(ws.bind());
+  // chunk: about 32 MB of factor input per chunk, at least one date
+  const size_t per_date = static_cast<size_t>(F) * N * 4;
+  int Tc = static_cast<int>((32ull << 20) / (per_date > 0 ? per_date : 1));
+  if (Tc < 1) Tc = 1;
+  if (Tc > T) Tc = T;
+  const int nchunk = (T + Tc - 1) / Tc;
+  float* dx[2];
+  float* dr[2];
+  uint8_t* dfm[2] = {nullptr, nullptr};
+  uint8_t* drm[2] = {nullptr, nullptr};
+  float* drk[2] = {nullptr, nullptr};
+  double* dic[2];
+  int* dst;
+  const size_t cn = static_cast<size_t>(Tc) * N;
+  FCB_TRY(ws.get(S_STATUS, 64, &dst));
+  for (int b = 0; b < 2; ++b) {
+    FCB_TRY(ws.get(static_cast<Slot>(S_PX0 + b), cn * F * 4, &dx[b]));
+    FCB_TRY(ws.get(static_cast<Slot>(S_PR0 + b), cn * 4, &dr[b]));
+    FCB_TRY(ws.get(static_cast<Slot>(S_PIC0 + b), static_cast<size_t>(F) * Tc * 8, &dic[b]));
+    if (fmask) FCB_TRY(ws.get(static_cast<Slot>(S_PFM0 + b), cn, &dfm[b]));
+    if (rmask) FCB_TRY(ws.get(static_cast<Slot>(S_PRM0 + b), cn, &drm[b]));
+    if (ranks) FCB_TRY(ws.get(static_cast<Slot>(S_PRK0 + b), cn * F * 4, &drk[b]));
+  }
+  FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), ws.stream[0]));
+  FCB_TRY(cudaStreamSynchronize(ws.stream[0]));
+  for (int c = 0; c < nchunk; ++c) {
+    const int b = c & 1;
+    cudaStream_t s = ws.stream[b];
+    const int t0 = c * Tc;
+    const int tc = (t0 + Tc <= T) ? Tc : (T - t0);
+    const size_t cnn = static_cast<size_t>(tc) * N;
+    for (int f = 0; f < F; ++f)
+      FCB_TRY(cudaMemcpyAsync(dx[b] + static_cast<size_t>(f) * tc * N,
+                              x + (static_cast<size_t>(f) * T + t0) * N, cnn * 4, cudaMemcpyHostToDevice, s));
+    FCB_TRY(cudaMemcpyAsync(dr[b], r + static_cast<size_t>(t0) * N, cnn * 4, cudaMemcpyHostToDevice, s));
+    if (fmask) FCB_TRY(cudaMemcpyAsync(dfm[b], fmask + static_cast<size_t>(t0) * N, cnn, cudaMemcpyHostToDevice, s));
+    if (rmask) FCB_TRY(cudaMemcpyAsync(drm[b], rmask + static_cast<size_t>(t0) * N, cnn, cudaMemcpyHostToDevice, s));
+    RankIcArgs<float, float> a{dx[b], dr[b], dfm[b], drm[b], F, tc, N, min_valid, drk[b], dic[b], nullptr, nullptr};
+    FCB_TRY(launch_rank_ic<float, float>(a, dst, s));
+    for (int f = 0; f < F; ++f) {
+      FCB_TRY(cudaMemcpyAsync(ic + static_cast<size_t>(f) * T + t0, dic[b] + static_cast<size_t>(f) * tc,
+                              static_cast<size_t>(tc) * 8, cudaMemcpyDeviceToHost, s));
+      if (ranks)
+        FCB_TRY(cudaMemcpyAsync(ranks + (static_cast<size_t>(f) * T + t0) * N, drk[b] + static_cast<size_t>(f) * tc * N,
+                                cnn * 4, cudaMemcpyDeviceToHost, s));
+    }
+  }
+  int hst = 0;
+  FCB_TRY(cudaStreamSynchronize(ws.stream[0]));
+  FCB_TRY(cudaStreamSynchronize(ws.stream[1]));
+  FCB_TRY(cudaMemcpy(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost));
+  return check_status(&hst);
+}
+
+// ---------------------------------------------------------------------------
+// correlations
+// ---------------------------------------------------------------------------
+extern "C" int fcb_stock_corr(const void* x, int dtype, const uint8_t* mask, int T, int N, double* out,
+                              int* selected_path, int* fallback_count) {
+  if (x == nullptr || out == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
+  if (dtype != FCB_DTYPE_F32 && dtype != FCB_DTYPE_F64) return FCB_ERR_ARG;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP2;
+  if (static_cast<long long>(N) * N > INT32_MAX) return FCB_ERR_CAP3;
+  fcb_workspace ws;
+  struct Rel {
+    fcb_workspace& w;
+    ~Rel() { w.release(); }
+  } rel{ws};
+  FCB_TRY(ws.bind());
+  cudaStream_t s = ws.stream[0];
+  const int Tp = (T + 31) / 32 * 32;
+  const size_t n = static_cast<size_t>(T) * N;
+  const size_t esz = dtype == FCB_DTYPE_F32 ? 4 : 8;
+  void* dx;
+  uint8_t* dm = nullptr;
+  double *xraw, *xc, *mc, *dout, *sum;
+  ColStat* st;
+  int *fbl, *fbc;
+  FCB_TRY(ws.get(S_X, n * esz, &dx));
+  if (mask) FCB_TRY(ws.get(S_MASK, n, &dm));
+  FCB_TRY(ws.get(S_SC_RAW, static_cast<size_t>(N) * Tp * 8, &xraw));
+  FCB_TRY(ws.get(S_SC_C, static_cast<size_t>(N) * Tp * 8, &xc));
+  FCB_TRY(ws.get(S_SC_M, static_cast<size_t>(N) * Tp * 8, &mc));
+  FCB_TRY(ws.get(S_SC_ST, static_cast<size_t>(N) * sizeof(ColStat), &st));
+  FCB_TRY(ws.get(S_SC_SUM, 64, &sum));
+  FCB_TRY(ws.get(S_OUT, static_cast<size_t>(N) * N * 8, &dout));
+  const size_t upper = static_cast<size_t>(N) * (N - 1) / 2;
+  FCB_TRY(ws.get(S_FB_LIST, (upper > 0 ? upper : 1) * 4, &fbl));
+  FCB_TRY(ws.get(S_FB_CNT, 64, &fbc));
+  FCB_TRY(cudaMemcpyAsync(dx, x, n * esz, cudaMemcpyHostToDevice, s));
+  if (mask) FCB_TRY(cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, s));
+  FCB_TRY(launch_stock_corr_prep(dx, dtype, dm, T, N, Tp, xraw, xc, mc, st, sum, s));
+  double hs[3];
+  FCB_TRY(cudaMemcpyAsync(hs, sum, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaStreamSynchronize(s));
+  if (hs[0] > 1e150 || hs[1] < 1e-150) return FCB_ERR_CAP4;
+  if (selected_path) *selected_path = hs[2] != 0.0 ? 0 : 1;
+  FCB_TRY(cudaMemsetAsync(fbc, 0, sizeof(int), s));
+  FCB_TRY(launch_stock_corr_gram(xraw, xc, mc, st, T, N, Tp, dout, fbl, fbc, s));
+  int hfb = 0;
+  FCB_TRY(cudaMemcpyAsync(out, dout, static_cast<size_t>(N) * N * 8, cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaMemcpyAsync(&hfb, fbc, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaStreamSynchronize(s));
+  if (fallback_count) *fallback_count = hfb;
+  return FCB_OK;
+}
+
+extern "C" int fcb_factor_corr(const void* x, int dtype, const uint8_t* mask, int T, int N, int F, double* out,
+                               uint8_t* fallback_out) {
+  if (x == nullptr || out == nullptr || T < 1 || N < 1 || F < 1) return FCB_ERR_ARG;
+  if (dtype != FCB_DTYPE_F32 && dtype != FCB_DTYPE_F64) return FCB_ERR_ARG;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP2;
+  if (F > 128) return FCB_ERR_CAP3;
+  fcb_workspace ws;
+  struct Rel {
+    fcb_workspace& w;
+    ~Rel() { w.release(); }
+  } rel{ws};
+  FCB_TRY(ws.bind());
+  cudaStream_t s = ws.stream[0];
+  const long long R = static_cast<long long>(T) * N;
+  const int Fp = (F + 3) / 4 * 4;
+  const size_t esz = dtype == FCB_DTYPE_F32 ? 4 : 8;
+  FcWork w{};
+  w.nblk_cols = static_cast<int>(std::min<long long>(592, std::max<long long>(1, R / 2048)));
+  w.nblk_gram = static_cast<int>(std::min<long long>(F <= 32 ? 296 : 148, std::max<long long>(1, R / 1024)));
+  void* dx;
+  uint8_t* dm = nullptr;
+  double* dout;
+  uint8_t* dflags = nullptr;
+  FCB_TRY(ws.get(S_X, static_cast<size_t>(R) * F * esz, &dx));
+  if (mask) FCB_TRY(ws.get(S_MASK, static_cast<size_t>(R), &dm));
+  FCB_TRY(ws.get(S_FC_COLPART, static_cast<size_t>(w.nblk_cols) * F * sizeof(FcColPart), &w.colpart));
+  FCB_TRY(ws.get(S_FC_COLSTAT, static_cast<size_t>(F) * sizeof(FcColStat), &w.colstat));
+  FCB_TRY(ws.get(S_FC_GRAM, static_cast<size_t>(w.nblk_gram) * 4 * Fp * Fp * 8, &w.gram));
+  FCB_TRY(ws.get(S_FB_LIST, static_cast<size_t>(F) * F * 4, &w.fb_list));
+  FCB_TRY(ws.get(S_FB_CNT, 64, &w.fb_count));
+  FCB_TRY(ws.get(S_OUT, static_cast<size_t>(F) * F * 8, &dout));
+  if (fallback_out) {
+    FCB_TRY(ws.get(S_FC_FLAGS, static_cast<size_t>(F) * F, &dflags));
+    FCB_TRY(cudaMemsetAsync(dflags, 0, static_cast<size_t>(F) * F, s));
+  }
+  FCB_TRY(cudaMemcpyAsync(dx, x, static_cast<size_t>(R) * F * esz, cudaMemcpyHostToDevice, s));
+  if (mask) FCB_TRY(cudaMemcpyAsync(dm, mask, static_cast<size_t>(R), cudaMemcpyHostToDevice, s));
+  FCB_TRY(launch_factor_corr(dx, dtype, dm, R, F, w, dout, dflags, s));
+  FCB_TRY(cudaMemcpyAsync(out, dout, static_cast<size_t>(F) * F * 8, cudaMemcpyDeviceToHost, s));
+  if (fallback_out)
+    FCB_TRY(cudaMemcpyAsync(fallback_out, dflags, static_cast<size_t>(F) * F, cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaStreamSynchronize(s));
+  return FCB_OK;
+}

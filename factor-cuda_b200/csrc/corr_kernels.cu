@@ -1,0 +1,797 @@
+// corr_kernels.cu -- FP64 pairwise-complete Pearson correlations (drop-in path).
+//
+// stock_corr (N,N) over t and factor_corr (F,F) over pooled (t,i) rows, with
+// the reference's numeric contract (|dr| <= 1e-12 against np.corrcoef on the
+// joint subset, serial-Kahan semantics on reduction-sensitive inputs):
+//
+//  1. column statistics: count, serial-Kahan mean in row order, min/max,
+//     |x| extrema for the domain check (stock_corr_gpu's col_stats_kernel,
+//     src/stock_corr.cu:73-116, with the demean_kernel's serial Kahan mean,
+//     :244-261);
+//  2. a Gram pass on column-centred values: n, sum x', sum y', sum x'y',
+//     sum x'^2, sum y'^2 over each pair's joint valid set (the six masked
+//     products of _masked_gemm_stats, fc/_cpu_core.py:139-169), accumulated
+//     hierarchically (per 32-wide k tile, then into the running total);
+//  3. finalize: the cancellation gate of _gemm_cancel_mask (ratio 3 on the
+//     uncentred sums, reconstructed from the centred ones), |r|>1, the
+//     near-zero-variance gate of finalize_cell (src/stock_corr_impl.cuh:102-132);
+//     flagged pairs are recomputed by
+//  4. the two-pass fallback on the original values: Kahan mean in row order,
+//     exact-constant (min==max) gate, centred second pass (Kahan above T=2048),
+//     sequential (sxy/sqrt(sxx))/sqrt(syy) (two_pass_centered,
+//     src/stock_corr_impl.cuh:150-201; _two_pass_corr, fc/_cpu_core.py:111-137).
+// The diagonal is 1.0 iff the column has n>=2, is not constant and its centred
+// sum of squares is positive and finite; the lower triangle mirrors the upper
+// bitwise.
+#include <cmath>
+
+#include "fcb_common.cuh"
+#include "fcb_kernels.h"
+
+namespace fcb {
+
+constexpr double kBigPos = 1e300;
+constexpr double kCancelRatio = 3.0;
+constexpr double kConstVarRel = 1e-10;
+constexpr double kTiny = 1e-300;
+constexpr int kTwoPassKahanT = 2048;
+
+struct Kahan {
+  double s = 0.0, c = 0.0;
+  FCB_DEV void add(double x) {
+    const double y = x - c;
+    const double t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  FCB_DEV void merge(const Kahan& o) {
+    add(o.s);
+    add(-o.c);
+  }
+};
+
+FCB_DEV double dnan() { return __longlong_as_double(0x7ff8000000000000ll); }
+
+FCB_DEV double safe_pearson(double sxy, double sxx, double syy) {
+  if (!(sxx > 0.0 && syy > 0.0) || !isfinite(sxx) || !isfinite(syy) || !isfinite(sxy)) return dnan();
+  const double r = (sxy / sqrt(sxx)) / sqrt(syy);
+  return isfinite(r) ? r : dnan();
+}
+
+// Decide from the centred moment sums of one pair whether the Gram value is
+// trustworthy; returns NaN + flag when the pair must go to the fallback.
+FCB_DEV double finalize_pair(double n, double sx, double sy, double sxy, double sx2, double sy2, double mux,
+                             double muy, bool& flag) {
+  flag = false;
+  if (n < 2.0) return dnan();
+  const double cov = sxy - sx * sy / n;
+  const double vx = sx2 - sx * sx / n;
+  const double vy = sy2 - sy * sy / n;
+  // uncentred sums of the reference's one-pass Gram, reconstructed
+  const double sxr = sx + n * mux;
+  const double syr = sy + n * muy;
+  const double sx2r = sx2 + 2.0 * mux * sx + n * mux * mux;
+  const double sy2r = sy2 + 2.0 * muy * sy + n * muy * muy;
+  bool fix = (fabs(sxr * syr / n) > kCancelRatio * fabs(cov)) ||
+             (fabs(sxr * sxr / n) > kCancelRatio * fabs(vx)) ||
+             (fabs(syr * syr / n) > kCancelRatio * fabs(vy));
+  const double xmag = fmax(fabs(sx2r), fabs(sxr * sxr / n));
+  const double ymag = fmax(fabs(sy2r), fabs(syr * syr / n));
+  if (fabs(vx) <= kConstVarRel * (xmag + kTiny) || fabs(vy) <= kConstVarRel * (ymag + kTiny)) fix = true;
+  const double r = safe_pearson(cov, vx, vy);
+  if (!isfinite(r) || fabs(r) > 1.0) fix = true;
+  flag = fix;
+  return fix ? dnan() : r;
+}
+
+// ---------------------------------------------------------------------------
+// stock_corr
+// ---------------------------------------------------------------------------
+
+// (T,N) row-major -> column-major Xraw/Xc/Mc (N, Tp), zero padded, tiled.
+template <typename TIN>
+__global__ void k_sc_transpose(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, int T, int N, int Tp,
+                               double* __restrict__ Xraw, double* __restrict__ Mc) {
+  __shared__ double tx[32][33];
+  __shared__ double tm[32][33];
+  const int t0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int t = t0 + r, i = i0 + threadIdx.x;
+    double v = 0.0, m = 0.0;
+    if (t < T && i < N) {
+      const size_t e = static_cast<size_t>(t) * N + i;
+      const double x = static_cast<double>(X[e]);
+      const bool ok = finite_f64(x) && (mask == nullptr || mask[e] != 0);
+      v = ok ? x : 0.0;
+      m = ok ? 1.0 : 0.0;
+    }
+    tx[r][threadIdx.x] = v;
+    tm[r][threadIdx.x] = m;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, t = t0 + threadIdx.x;
+    if (i < N && t < Tp) {
+      Xraw[static_cast<size_t>(i) * Tp + t] = tx[threadIdx.x][r];
+      Mc[static_cast<size_t>(i) * Tp + t] = tm[threadIdx.x][r];
+    }
+  }
+}
+
+// One warp per column: serial Kahan mean in row order, extrema, centred
+// copy Xc = valid ? x - mu : 0, centred sum of squares for the diagonal.
+__global__ void k_sc_colstats(const double* __restrict__ Xraw, const double* __restrict__ Mc, int T, int N, int Tp,
+                              double* __restrict__ Xc, ColStat* __restrict__ st) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= N) return;
+  const double* x = Xraw + static_cast<size_t>(w) * Tp;
+  const double* m = Mc + static_cast<size_t>(w) * Tp;
+  Kahan k;
+  double cnt = 0.0, mn = kBigPos, mx = -kBigPos, mna = kBigPos, mxa = 0.0;
+  for (int t0 = 0; t0 < T; t0 += 32) {
+    const int t = t0 + lane;
+    const double xv = (t < T) ? x[t] : 0.0;
+    const bool ok = (t < T) && m[t] != 0.0;
+    const unsigned vb = __ballot_sync(kFull, ok);
+    // serial Kahan in row order: lane 0 consumes the 32 values in order
+    for (int l = 0; l < 32; ++l) {
+      const double v = __shfl_sync(kFull, xv, l);
+      if ((vb >> l) & 1u) k.add(v);
+    }
+    if (ok) {
+      cnt += 1.0;
+      mn = fmin(mn, xv);
+      mx = fmax(mx, xv);
+      const double ax = fabs(xv);
+      mxa = fmax(mxa, ax);
+      if (ax != 0.0) mna = fmin(mna, ax);
+    }
+  }
+  cnt = warp_sum(cnt);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_xor_sync(kFull, mn, o));
+    mx = fmax(mx, __shfl_xor_sync(kFull, mx, o));
+    mna = fmin(mna, __shfl_xor_sync(kFull, mna, o));
+    mxa = fmax(mxa, __shfl_xor_sync(kFull, mxa, o));
+  }
+  const double mu = cnt > 0.0 ? k.s / cnt : 0.0;
+  double s2 = 0.0, s1 = 0.0;
+  for (int t = lane; t < Tp; t += 32) {
+    const bool ok = (t < T) && m[t] != 0.0;
+    const double d = ok ? x[t] - mu : 0.0;
+    Xc[static_cast<size_t>(w) * Tp + t] = d;
+    s2 += d * d;
+    s1 += d;
+  }
+  s2 = warp_sum(s2);
+  s1 = warp_sum(s1);
+  if (lane == 0) {
+    ColStat c;
+    c.count = cnt;
+    c.mean = mu;
+    c.min = mn;
+    c.max = mx;
+    c.min_abs = mna;
+    c.max_abs = mxa;
+    c.s2 = s2;
+    c.s1 = s1;
+    st[w] = c;
+  }
+}
+
+// Domain check + full-validity over the column stats (single block).
+__global__ void k_sc_summary(const ColStat* __restrict__ st, int N, int T, double* __restrict__ out3) {
+  double mxa = 0.0, mna = kBigPos;
+  int full = 1;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    mxa = fmax(mxa, st[i].max_abs);
+    mna = fmin(mna, st[i].min_abs);
+    if (st[i].count < static_cast<double>(T)) full = 0;
+  }
+  __shared__ double smx[32], smn[32];
+  __shared__ int sf[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mxa = fmax(mxa, __shfl_xor_sync(kFull, mxa, o));
+    mna = fmin(mna, __shfl_xor_sync(kFull, mna, o));
+    full = min(full, __shfl_xor_sync(kFull, full, o));
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    smx[w] = mxa;
+    smn[w] = mna;
+    sf[w] = full;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (blockDim.x + 31) / 32; ++i) {
+      mxa = fmax(mxa, smx[i]);
+      mna = fmin(mna, smn[i]);
+      full = min(full, sf[i]);
+    }
+    out3[0] = mxa;
+    out3[1] = mna;
+    out3[2] = full;
+  }
+}
+
+// Upper-triangle 32x32 tiles; 256 threads, 2x2 cells per thread; six
+// accumulators per cell; 32-wide k tiles staged in shared memory.
+constexpr int kScTile = 32, kScK = 32;
+
+FCB_DEV void tri_tile(int b, int nt, int& ib, int& jb) {
+  int lo = 0, hi = nt - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    const long long pm = static_cast<long long>(mid) * nt - static_cast<long long>(mid) * (mid - 1) / 2;
+    if (pm <= b) lo = mid; else hi = mid - 1;
+  }
+  ib = lo;
+  const long long p = static_cast<long long>(ib) * nt - static_cast<long long>(ib) * (ib - 1) / 2;
+  jb = ib + static_cast<int>(b - p);
+}
+
+__global__ void __launch_bounds__(256, 2)
+    k_sc_gram(const double* __restrict__ Xc, const double* __restrict__ Mc, const ColStat* __restrict__ st, int N,
+              int Tp, int nt, double* __restrict__ out, int* __restrict__ fb_list, int* __restrict__ fb_count,
+              int full) {
+  __shared__ double Ax[kScTile][kScK + 1], Am[kScTile][kScK + 1], Bx[kScTile][kScK + 1], Bm[kScTile][kScK + 1];
+  int ib, jb;
+  tri_tile(blockIdx.x, nt, ib, jb);
+  const int i0 = ib * kScTile, j0 = jb * kScTile;
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+  double acc[4][6], part[4][6];
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[c][q] = 0.0;
+  for (int k0 = 0; k0 < Tp; k0 += kScK) {
+    for (int e = threadIdx.x; e < kScTile * kScK; e += 256) {
+      const int r = e / kScK, kk = e % kScK;
+      const int gi = i0 + r, gj = j0 + r;
+      Ax[r][kk] = gi < N ? Xc[static_cast<size_t>(gi) * Tp + k0 + kk] : 0.0;
+      Am[r][kk] = gi < N ? Mc[static_cast<size_t>(gi) * Tp + k0 + kk] : 0.0;
+      Bx[r][kk] = gj < N ? Xc[static_cast<size_t>(gj) * Tp + k0 + kk] : 0.0;
+      Bm[r][kk] = gj < N ? Mc[static_cast<size_t>(gj) * Tp + k0 + kk] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) part[c][q] = 0.0;
+#pragma unroll 4
+    for (int kk = 0; kk < kScK; ++kk) {
+      const double ax0 = Ax[ty * 2][kk], ax1 = Ax[ty * 2 + 1][kk];
+      const double am0 = Am[ty * 2][kk], am1 = Am[ty * 2 + 1][kk];
+      const double bx0 = Bx[tx * 2][kk], bx1 = Bx[tx * 2 + 1][kk];
+      const double bm0 = Bm[tx * 2][kk], bm1 = Bm[tx * 2 + 1][kk];
+      const double axs[2] = {ax0, ax1}, ams[2] = {am0, am1}, bxs[2] = {bx0, bx1}, bms[2] = {bm0, bm1};
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          const int c = a * 2 + b;
+          const double jx = axs[a] * bms[b];
+          const double jy = ams[a] * bxs[b];
+          part[c][0] = fma(ams[a], bms[b], part[c][0]);
+          part[c][1] += jx;
+          part[c][2] += jy;
+          part[c][3] = fma(axs[a], bxs[b], part[c][3]);
+          part[c][4] = fma(axs[a], jx, part[c][4]);
+          part[c][5] = fma(bxs[b], jy, part[c][5]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) acc[c][q] += part[c][q];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int i = i0 + ty * 2 + a, j = j0 + tx * 2 + b;
+      if (i >= N || j >= N || i > j) continue;
+      const double* q = acc[a * 2 + b];
+      double r;
+      bool flag = false;
+      if (i == j) {
+        // diagonal: 1.0 iff the column's centred sum of squares is usable
+        const ColStat& s = st[i];
+        r = (s.count >= 2.0 && s.min != s.max && s.s2 > 0.0 && isfinite(s.s2)) ? 1.0 : dnan();
+      } else {
+        r = finalize_pair(q[0], q[1], q[2], q[3], q[4], q[5], st[i].mean, st[j].mean, flag);
+        if (!flag && q[0] >= 2.0) {
+          // an exact-constant column on the joint set has zero centred
+          // variance; the gate above catches it, min==max settles it
+        }
+      }
+      out[static_cast<size_t>(i) * N + j] = r;
+      out[static_cast<size_t>(j) * N + i] = r;
+      if (flag) {
+        const int slot = atomicAdd(fb_count, 1);
+        fb_list[slot] = i * N + j;  // N*N <= INT32_MAX
+      }
+    }
+  (void)full;
+}
+
+// Two-pass Pearson of one pair over its joint valid rows, serial in row
+// order (exact replica of the Kahan-mean two-pass reference).
+FCB_DEV double two_pass_serial(const double* xi, const double* mi, const double* xj, const double* mj, int T,
+                               size_t stride_x, size_t stride_m) {
+  double n = 0.0, mnx = kBigPos, mxx = -kBigPos, mny = kBigPos, mxy = -kBigPos;
+  Kahan kx, ky;
+  for (int t = 0; t < T; ++t) {
+    if (mi[t * stride_m] != 0.0 && mj[t * stride_m] != 0.0) {
+      const double x = xi[t * stride_x], y = xj[t * stride_x];
+      n += 1.0;
+      kx.add(x);
+      ky.add(y);
+      mnx = fmin(mnx, x);
+      mxx = fmax(mxx, x);
+      mny = fmin(mny, y);
+      mxy = fmax(mxy, y);
+    }
+  }
+  if (n < 2.0) return dnan();
+  if (mnx == mxx || mny == mxy) return dnan();
+  const double mx = kx.s / n, my = ky.s / n;
+  double sxx, syy, sxy;
+  if (T > kTwoPassKahanT) {
+    Kahan a, b, c;
+    for (int t = 0; t < T; ++t)
+      if (mi[t * stride_m] != 0.0 && mj[t * stride_m] != 0.0) {
+        const double dx = xi[t * stride_x] - mx, dy = xj[t * stride_x] - my;
+        a.add(dx * dx);
+        b.add(dy * dy);
+        c.add(dx * dy);
+      }
+    sxx = a.s - a.c;
+    syy = b.s - b.c;
+    sxy = c.s - c.c;
+  } else {
+    sxx = syy = sxy = 0.0;
+    for (int t = 0; t < T; ++t)
+      if (mi[t * stride_m] != 0.0 && mj[t * stride_m] != 0.0) {
+        const double dx = xi[t * stride_x] - mx, dy = xj[t * stride_x] - my;
+        sxx += dx * dx;
+        syy += dy * dy;
+        sxy += dx * dy;
+      }
+  }
+  return safe_pearson(sxy, sxx, syy);
+}
+
+__global__ void k_sc_fallback(const double* __restrict__ Xraw, const double* __restrict__ Mc, int T, int N, int Tp,
+                              const int* __restrict__ fb_list, const int* __restrict__ fb_count,
+                              double* __restrict__ out) {
+  const int cnt = *fb_count;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+    const int cell = fb_list[k];
+    const int i = cell / N, j = cell % N;
+    const double r = two_pass_serial(Xraw + static_cast<size_t>(i) * Tp, Mc + static_cast<size_t>(i) * Tp,
+                                     Xraw + static_cast<size_t>(j) * Tp, Mc + static_cast<size_t>(j) * Tp, T, 1, 1);
+    out[static_cast<size_t>(i) * N + j] = r;
+    out[static_cast<size_t>(j) * N + i] = r;
+  }
+}
+
+cudaError_t launch_stock_corr_prep(const void* X, int dtype, const uint8_t* mask, int T, int N, int Tp,
+                                   double* Xraw, double* Xc, double* Mc, ColStat* st, double* summary,
+                                   cudaStream_t s) {
+  dim3 grid((Tp + 31) / 32, (N + 31) / 32), block(32, 8);
+  if (dtype == 0)
+    k_sc_transpose<float><<<grid, block, 0, s>>>(static_cast<const float*>(X), mask, T, N, Tp, Xraw, Mc);
+  else
+    k_sc_transpose<double><<<grid, block, 0, s>>>(static_cast<const double*>(X), mask, T, N, Tp, Xraw, Mc);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_sc_colstats<<<(N * 32 + 255) / 256, 256, 0, s>>>(Xraw, Mc, T, N, Tp, Xc, st);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_sc_summary<<<1, 1024, 0, s>>>(st, N, T, summary);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const double* Mc, const ColStat* st, int T,
+                                   int N, int Tp, double* out, int* fb_list, int* fb_count, cudaStream_t s) {
+  const int nt = (N + kScTile - 1) / kScTile;
+  const long long tiles = static_cast<long long>(nt) * (nt + 1) / 2;
+  k_sc_gram<<<static_cast<unsigned>(tiles), 256, 0, s>>>(Xc, Mc, st, N, Tp, nt, out, fb_list, fb_count, 0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // grid-stride over the device-side fallback count (no host round trip)
+  k_sc_fallback<<<148 * 4, 128, 0, s>>>(Xraw, Mc, T, N, Tp, fb_list, fb_count, out);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// factor_corr: rows r = t*N+i of a (T,N,F) panel, F <= 128 columns
+// ---------------------------------------------------------------------------
+
+// Per-block column partials over a contiguous row range: count, Kahan sum,
+// min, max.  Rows are visited in increasing order within each thread's
+// strided slice; partials are merged in a fixed order by k_fc_colfinal.
+template <typename TIN>
+__global__ void k_fc_colpart(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
+                             long long rows_per_block, FcColPart* __restrict__ part) {
+  const long long r0 = blockIdx.x * rows_per_block;
+  const long long r1 = min(R, r0 + rows_per_block);
+  for (int f = threadIdx.y; f < F; f += blockDim.y) {
+    Kahan k;
+    double cnt = 0.0, mn = kBigPos, mx = -kBigPos;
+    for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      const double x = static_cast<double>(X[r * F + f]);
+      if (finite_f64(x) && (mask == nullptr || mask[r] != 0)) {
+        cnt += 1.0;
+        k.add(x);
+        mn = fmin(mn, x);
+        mx = fmax(mx, x);
+      }
+    }
+    // fixed-order warp merge (lanes are threadIdx.x within one warp row)
+    for (int o = 1; o < 32; o <<= 1) {
+      const double os = __shfl_down_sync(kFull, k.s, o), oc = __shfl_down_sync(kFull, k.c, o);
+      const double on = __shfl_down_sync(kFull, cnt, o);
+      const double omn = __shfl_down_sync(kFull, mn, o), omx = __shfl_down_sync(kFull, mx, o);
+      if ((threadIdx.x & (2 * o - 1)) == 0) {
+        Kahan kk;
+        kk.s = os;
+        kk.c = oc;
+        k.merge(kk);
+        cnt += on;
+        mn = fmin(mn, omn);
+        mx = fmax(mx, omx);
+      }
+    }
+    if (threadIdx.x == 0) {
+      FcColPart p;
+      p.count = cnt;
+      p.s = k.s;
+      p.c = k.c;
+      p.min = mn;
+      p.max = mx;
+      part[static_cast<size_t>(blockIdx.x) * F + f] = p;
+    }
+  }
+}
+
+__global__ void k_fc_colfinal(const FcColPart* __restrict__ part, int nblk, int F, FcColStat* __restrict__ st) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  Kahan k;
+  double cnt = 0.0, mn = kBigPos, mx = -kBigPos;
+  for (int b = 0; b < nblk; ++b) {
+    const FcColPart& p = part[static_cast<size_t>(b) * F + f];
+    Kahan o;
+    o.s = p.s;
+    o.c = p.c;
+    k.merge(o);
+    cnt += p.count;
+    mn = fmin(mn, p.min);
+    mx = fmax(mx, p.max);
+  }
+  FcColStat s;
+  s.count = cnt;
+  s.mean = cnt > 0.0 ? k.s / cnt : 0.0;
+  s.min = mn;
+  s.max = mx;
+  st[f] = s;
+}
+
+// Gram partials over a row range.  Products p: 0 n=(m,m), 1 sx=(x',m),
+// 2 sx2=(x'^2,m), 3 sxy=(x',x').  Each thread owns a 4x4 (f,g) tile of one
+// product and a slice of the staged rows; slices are summed in shared memory
+// in a fixed order at the end of the block.
+constexpr int kFcRowsChunk = 32;
+
+template <typename TIN>
+__global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                 long long R, int F, int Fp, long long rows_per_block,
+                                                 const FcColStat* __restrict__ st, int tasks_total,
+                                                 int tasks_per_block, double* __restrict__ part) {
+  extern __shared__ __align__(16) double fsm[];
+  double* sx = fsm;                                  // [chunk][Fp] centred values
+  double* sm = sx + kFcRowsChunk * Fp;               // [chunk][Fp] validity
+  double* sq = sm + kFcRowsChunk * Fp;               // [chunk][Fp] squares
+  double* red = sq + kFcRowsChunk * Fp;              // [slices][tasks_per_block][16]
+  const int tb = Fp / 4;
+  const int task0 = blockIdx.y * tasks_per_block;
+  const int ntask = min(tasks_per_block, tasks_total - task0);
+  const int slices = 256 / tasks_per_block;
+  const int my_task = threadIdx.x % tasks_per_block;
+  const int my_slice = threadIdx.x / tasks_per_block;
+  const bool active = (my_slice < slices) && (my_task < ntask);
+  int p = 0, fa = 0, ga = 0;
+  if (active) {
+    const int tk = task0 + my_task;
+    p = tk / (tb * tb);
+    const int rem = tk % (tb * tb);
+    fa = (rem / tb) * 4;
+    ga = (rem % tb) * 4;
+  }
+  double acc[16], prt[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+  const long long r0 = blockIdx.x * rows_per_block;
+  const long long r1 = min(R, r0 + rows_per_block);
+  for (long long c0 = r0; c0 < r1; c0 += kFcRowsChunk) {
+    const int nr = static_cast<int>(min(static_cast<long long>(kFcRowsChunk), r1 - c0));
+    for (int e = threadIdx.x; e < kFcRowsChunk * Fp; e += 256) {
+      const int rr = e / Fp, f = e % Fp;
+      double v = 0.0, mv = 0.0;
+      if (rr < nr && f < F) {
+        const long long r = c0 + rr;
+        const double x = static_cast<double>(X[r * F + f]);
+        if (finite_f64(x) && (mask == nullptr || mask[r] != 0)) {
+          v = x - st[f].mean;
+          mv = 1.0;
+        }
+      }
+      sx[e] = v;
+      sm[e] = mv;
+      sq[e] = v * v;
+    }
+    __syncthreads();
+    if (active) {
+      const double* A = (p == 0) ? sm : (p == 1 ? sx : (p == 2 ? sq : sx));
+      const double* B = (p == 3) ? sx : sm;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) prt[q] = 0.0;
+      for (int rr = my_slice; rr < nr; rr += slices) {
+        const double* ar = A + rr * Fp + fa;
+        const double* br = B + rr * Fp + ga;
+        const double a0 = ar[0], a1 = ar[1], a2 = ar[2], a3 = ar[3];
+        const double b0 = br[0], b1 = br[1], b2 = br[2], b3 = br[3];
+        const double av[4] = {a0, a1, a2, a3}, bv[4] = {b0, b1, b2, b3};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) prt[u * 4 + v] = fma(av[u], bv[v], prt[u * 4 + v]);
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc[q] += prt[q];
+    }
+    __syncthreads();
+  }
+  // reduce slices in fixed order
+  if (active) {
+    double* dst = red + (static_cast<size_t>(my_slice) * tasks_per_block + my_task) * 16;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) dst[q] = acc[q];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < ntask * 16; e += 256) {
+    const int tk = e / 16, q = e % 16;
+    double s = 0.0;
+    for (int sl = 0; sl < slices; ++sl) s += red[(static_cast<size_t>(sl) * tasks_per_block + tk) * 16 + q];
+    const int gt = task0 + tk;
+    const int pp = gt / (tb * tb);
+    const int rem = gt % (tb * tb);
+    const int f = (rem / tb) * 4 + q / 4, g = (rem % tb) * 4 + q % 4;
+    part[((static_cast<size_t>(blockIdx.x) * 4 + pp) * Fp + f) * Fp + g] = s;
+  }
+}
+
+// Sum the per-block Gram partials in block order, finalize each pair.
+__global__ void k_fc_final(const double* __restrict__ part, int nblk, int F, int Fp,
+                           const FcColStat* __restrict__ st, double* __restrict__ out, int* __restrict__ fb_list,
+                           int* __restrict__ fb_count, uint8_t* __restrict__ flags) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= F * F) return;
+  const int i = e / F, j = e % F;
+  if (i > j) return;
+  double q[6] = {0, 0, 0, 0, 0, 0};
+  // q: n, sx (x'_i m_j), sy (m_i x'_j), sxy, sx2 (x'^2_i m_j), sy2 (m_i x'^2_j)
+  for (int b = 0; b < nblk; ++b) {
+    const double* P = part + static_cast<size_t>(b) * 4 * Fp * Fp;
+    q[0] += P[(0 * Fp + i) * Fp + j];
+    q[1] += P[(1 * Fp + i) * Fp + j];
+    q[2] += P[(1 * Fp + j) * Fp + i];
+    q[3] += P[(3 * Fp + i) * Fp + j];
+    q[4] += P[(2 * Fp + i) * Fp + j];
+    q[5] += P[(2 * Fp + j) * Fp + i];
+  }
+  double r;
+  bool flag = false;
+  if (i == j) {
+    const FcColStat& s = st[i];
+    const double v = q[4] - q[1] * q[1] / fmax(q[0], 1.0);
+    r = (s.count >= 2.0 && s.min != s.max && v > 0.0 && isfinite(v)) ? 1.0 : dnan();
+  } else {
+    r = finalize_pair(q[0], q[1], q[2], q[3], q[4], q[5], st[i].mean, st[j].mean, flag);
+  }
+  out[i * F + j] = r;
+  out[j * F + i] = r;
+  if (flags != nullptr) flags[i * F + j] = flag ? 1 : 0;
+  if (flag) {
+    const int slot = atomicAdd(fb_count, 1);
+    fb_list[slot] = e;
+  }
+}
+
+// One block per flagged pair: two-pass over the pooled joint rows.  Small
+// pools run serially in row order (bit-compatible with the serial-Kahan
+// reference); large pools use per-thread Kahan partials merged in a fixed
+// tree (the reference's kahan_reduce kernels, src/factor_corr.cu:188-322).
+template <typename TIN>
+__global__ void k_fc_fallback(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
+                              const int* __restrict__ fb_list, const int* __restrict__ fb_count,
+                              double* __restrict__ out) {
+  if (static_cast<int>(blockIdx.x) >= *fb_count) return;
+  const int e = fb_list[blockIdx.x];
+  const int i = e / F, j = e % F;
+  __shared__ double sh[6][256];
+  __shared__ double res[8];
+  const bool serial = R < 4096;
+  const int nth = serial ? 1 : blockDim.x;
+  const int tid = threadIdx.x;
+  if (tid >= nth) {
+    // idle threads still take part in the barriers below
+  }
+  auto valid = [&](long long r, double& x, double& y) {
+    x = static_cast<double>(X[r * F + i]);
+    y = static_cast<double>(X[r * F + j]);
+    return finite_f64(x) && finite_f64(y) && (mask == nullptr || mask[r] != 0);
+  };
+  Kahan kx, ky;
+  double n = 0.0, mnx = kBigPos, mxx = -kBigPos, mny = kBigPos, mxy = -kBigPos;
+  if (tid < nth) {
+    for (long long r = tid; r < R; r += nth) {
+      double x, y;
+      if (valid(r, x, y)) {
+        n += 1.0;
+        kx.add(x);
+        ky.add(y);
+        mnx = fmin(mnx, x);
+        mxx = fmax(mxx, x);
+        mny = fmin(mny, y);
+        mxy = fmax(mxy, y);
+      }
+    }
+  }
+  sh[0][tid] = kx.s; sh[1][tid] = kx.c; sh[2][tid] = ky.s; sh[3][tid] = ky.c; sh[4][tid] = n;
+  __syncthreads();
+  // fixed binary tree merge (thread order)
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (tid < s && tid + s < nth) {
+      Kahan a, b, c, d;
+      a.s = sh[0][tid]; a.c = sh[1][tid]; b.s = sh[0][tid + s]; b.c = sh[1][tid + s];
+      c.s = sh[2][tid]; c.c = sh[3][tid]; d.s = sh[2][tid + s]; d.c = sh[3][tid + s];
+      a.merge(b);
+      c.merge(d);
+      sh[0][tid] = a.s; sh[1][tid] = a.c; sh[2][tid] = c.s; sh[3][tid] = c.c;
+      sh[4][tid] += sh[4][tid + s];
+    }
+    __syncthreads();
+  }
+  // min / max
+  double v0 = mnx, v1 = mxx, v2 = mny, v3 = mxy;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v0 = fmin(v0, __shfl_xor_sync(kFull, v0, o));
+    v1 = fmax(v1, __shfl_xor_sync(kFull, v1, o));
+    v2 = fmin(v2, __shfl_xor_sync(kFull, v2, o));
+    v3 = fmax(v3, __shfl_xor_sync(kFull, v3, o));
+  }
+  __shared__ double mm[4][8];
+  if ((tid & 31) == 0) {
+    mm[0][tid >> 5] = v0; mm[1][tid >> 5] = v1; mm[2][tid >> 5] = v2; mm[3][tid >> 5] = v3;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < static_cast<int>(blockDim.x / 32); ++w) {
+      v0 = fmin(v0, mm[0][w]); v1 = fmax(v1, mm[1][w]); v2 = fmin(v2, mm[2][w]); v3 = fmax(v3, mm[3][w]);
+    }
+    const double nn = sh[4][0];
+    res[0] = nn;
+    res[1] = nn > 0 ? sh[0][0] / nn : 0.0;
+    res[2] = nn > 0 ? sh[2][0] / nn : 0.0;
+    res[3] = (nn < 2.0 || v0 == v1 || v2 == v3) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const double nn = res[0], mx = res[1], my = res[2];
+  if (res[3] != 0.0) {
+    if (tid == 0) {
+      out[i * F + j] = dnan();
+      out[j * F + i] = dnan();
+    }
+    return;
+  }
+  Kahan a, b, c;
+  if (tid < nth) {
+    for (long long r = tid; r < R; r += nth) {
+      double x, y;
+      if (valid(r, x, y)) {
+        const double dx = x - mx, dy = y - my;
+        if (serial && R <= kTwoPassKahanT) {
+          a.s += dx * dx;
+          b.s += dy * dy;
+          c.s += dx * dy;
+        } else {
+          a.add(dx * dx);
+          b.add(dy * dy);
+          c.add(dx * dy);
+        }
+      }
+    }
+  }
+  sh[0][tid] = a.s; sh[1][tid] = a.c; sh[2][tid] = b.s; sh[3][tid] = b.c; sh[4][tid] = c.s; sh[5][tid] = c.c;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (tid < s && tid + s < nth) {
+      for (int q = 0; q < 3; ++q) {
+        Kahan u, v;
+        u.s = sh[2 * q][tid]; u.c = sh[2 * q + 1][tid]; v.s = sh[2 * q][tid + s]; v.c = sh[2 * q + 1][tid + s];
+        u.merge(v);
+        sh[2 * q][tid] = u.s;
+        sh[2 * q + 1][tid] = u.c;
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const double r = safe_pearson(sh[4][0] - sh[5][0], sh[0][0] - sh[1][0], sh[2][0] - sh[3][0]);
+    (void)nn;
+    out[i * F + j] = r;
+    out[j * F + i] = r;
+  }
+}
+
+size_t fc_gram_smem(int Fp, int tasks_per_block) {
+  const int slices = 256 / tasks_per_block;
+  return (3 * static_cast<size_t>(kFcRowsChunk) * Fp + static_cast<size_t>(slices) * tasks_per_block * 16) *
+         sizeof(double);
+}
+
+cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
+                               double* out, uint8_t* flags, cudaStream_t s) {
+  const int Fp = (F + 3) / 4 * 4;
+  const int tb = Fp / 4;
+  const int tasks_total = 4 * tb * tb;
+  const int tasks_per_block = tasks_total <= 256 ? tasks_total : 256;
+  const int ytiles = (tasks_total + tasks_per_block - 1) / tasks_per_block;
+  const long long rpb_cols = (R + w.nblk_cols - 1) / w.nblk_cols;
+  const long long rpb_gram = (R + w.nblk_gram - 1) / w.nblk_gram;
+  dim3 cb(32, 8);
+  if (dtype == 0)
+    k_fc_colpart<float><<<w.nblk_cols, cb, 0, s>>>(static_cast<const float*>(X), mask, R, F, rpb_cols, w.colpart);
+  else
+    k_fc_colpart<double><<<w.nblk_cols, cb, 0, s>>>(static_cast<const double*>(X), mask, R, F, rpb_cols, w.colpart);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_fc_colfinal<<<(F + 127) / 128, 128, 0, s>>>(w.colpart, w.nblk_cols, F, w.colstat);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const size_t smem = fc_gram_smem(Fp, tasks_per_block);
+  dim3 gg(w.nblk_gram, ytiles);
+  if (dtype == 0) {
+    e = cudaFuncSetAttribute(k_fc_gram<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    k_fc_gram<float><<<gg, 256, smem, s>>>(static_cast<const float*>(X), mask, R, F, Fp, rpb_gram, w.colstat,
+                                           tasks_total, tasks_per_block, w.gram);
+  } else {
+    e = cudaFuncSetAttribute(k_fc_gram<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    k_fc_gram<double><<<gg, 256, smem, s>>>(static_cast<const double*>(X), mask, R, F, Fp, rpb_gram, w.colstat,
+                                            tasks_total, tasks_per_block, w.gram);
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(w.fb_count, 0, sizeof(int), s)) != cudaSuccess) return e;
+  k_fc_final<<<(F * F + 255) / 256, 256, 0, s>>>(w.gram, w.nblk_gram, F, Fp, w.colstat, out, w.fb_list, w.fb_count,
+                                                 flags);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const int maxpairs = F * (F - 1) / 2 > 0 ? F * (F - 1) / 2 : 1;
+  if (dtype == 0)
+    k_fc_fallback<float><<<maxpairs, 256, 0, s>>>(static_cast<const float*>(X), mask, R, F, w.fb_list, w.fb_count,
+                                                  out);
+  else
+    k_fc_fallback<double><<<maxpairs, 256, 0, s>>>(static_cast<const double*>(X), mask, R, F, w.fb_list,
+                                                   w.fb_count, out);
+  return cudaGetLastError();
+}
+
+}  // namespace fcb

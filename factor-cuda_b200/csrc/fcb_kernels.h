@@ -1,0 +1,72 @@
+// fcb_kernels.h -- internal launch interface between the kernel translation
+// units and the C-ABI host drivers (capi.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fcb {
+
+// Largest cross-section the shared-memory rank kernels take (u16 column ids,
+// 1024 threads x 16 items).  Larger N goes through the global-memory path.
+constexpr int kSmemRankCap = 16384;
+constexpr size_t kMaxSmemPerBlock = 227 * 1024;
+
+struct ScanOut {
+  float* out[4];  // group g output panel (T,N) or nullptr when the group is inactive
+};
+
+template <typename TF, typename TR>
+struct RankIcArgs {
+  const TF* X;              // (F,T,N) factor panels
+  const TR* R;              // (T,N) forward returns
+  const uint8_t* fmask;     // (T,N) factor mask or nullptr
+  const uint8_t* rmask;     // (T,N) forward-return mask or nullptr
+  int F, T, N, min_valid;
+  float* ranks_out;         // (F,T,N) cs_rank ranks (valid = finite(f) & fmask) or nullptr
+  double* ic_out;           // (F,T)
+  double* rank_f_out;       // (F,T,N) joint-set ranks, 0 elsewhere, or nullptr
+  double* rank_r_out;       // (F,T,N) joint-set ranks of the returns, or nullptr
+};
+
+struct ColStat {  // one stock_corr column
+  double count, mean, min, max, min_abs, max_abs, s2, s1;
+};
+struct FcColPart {
+  double count, s, c, min, max;
+};
+struct FcColStat {
+  double count, mean, min, max;
+};
+struct FcWork {
+  int nblk_cols, nblk_gram;
+  FcColPart* colpart;  // [nblk_cols][F]
+  FcColStat* colstat;  // [F]
+  double* gram;        // [nblk_gram][4][Fp][Fp]
+  int* fb_list;        // [F*F]
+  int* fb_count;       // [1]
+};
+
+// rank_kernels.cu
+size_t cs_rank_smem(int N);
+cudaError_t launch_cs_rank(const float* X, const uint8_t* mask, int T, int N, int desc, float* out,
+                           int* status, cudaStream_t st);
+cudaError_t launch_param_scan(const float* X, const uint8_t* mask, int T, int N, ScanOut outs, int* status,
+                              cudaStream_t st);
+template <typename TF, typename TR>
+size_t rank_ic_smem(int N);
+template <typename TF, typename TR>
+cudaError_t launch_rank_ic(const RankIcArgs<TF, TR>& a, int* status, cudaStream_t st);
+
+// corr_kernels.cu
+cudaError_t launch_stock_corr_prep(const void* X, int dtype, const uint8_t* mask, int T, int N, int Tp,
+                                   double* Xraw, double* Xc, double* Mc, ColStat* st, double* summary,
+                                   cudaStream_t s);
+cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const double* Mc, const ColStat* st, int T,
+                                   int N, int Tp, double* out, int* fb_list, int* fb_count, cudaStream_t s);
+size_t fc_gram_smem(int Fp, int tasks_per_block);
+cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
+                               double* out, uint8_t* flags, cudaStream_t s);
+
+}  // namespace fcb

@@ -1,0 +1,548 @@
+// rank_kernels.cu -- per-date in-shared-memory rank kernels for sm_100a.
+//
+//  k_cs_rank      one CTA per date: stage the row (bulk copy), compact the valid
+//                 cells, radix-sort (key, column) in shared memory, scatter
+//                 ordinal ranks, store the row.  Semantics of the reference's
+//                 cs_rank_gpu (src/cross_sectional_rank.cu:228-372).
+//  k_param_scan   one sort per date serves all four parameter_scan groups
+//                 (asc/desc x masked/unmasked): masked ranks are prefix counts
+//                 of mask flags in sorted order, descending ranks come from the
+//                 tie-group bounds of the ascending order.  Replaces four full
+//                 rank pipelines (src/cross_sectional_rank.cu:401-664).
+//  k_rank_ic      one CTA per date, looping over F factor panels: the forward
+//                 returns are sorted once per date, each factor is sorted once;
+//                 cs_rank ranks (own valid set) and the joint-set ranks of the
+//                 Spearman IC come from prefix counts over the two sorted
+//                 orders; the IC is evaluated in exact integer arithmetic
+//                 (sum r_f*r_r in int64) with one f64 finalize.  Semantics of
+//                 rolling_ic_gpu (src/rolling_ic.cu:306-540) / np_rolling_ic
+//                 (fc/_cpu_core.py:271-293).
+#include "block_sort.cuh"
+#include "fcb_kernels.h"
+
+namespace fcb {
+
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// Exclusive max-scan of one int per thread (in thread order); identity -1.
+FCB_DEV int block_exclusive_max(int v, int* scratch) {
+  int inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int u = __shfl_up_sync(kFull, inc, o);
+    if (lane_id() >= static_cast<unsigned>(o)) inc = max(inc, u);
+  }
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane_id() == 31) scratch[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    int s = (lane_id() < static_cast<unsigned>(nw)) ? scratch[lane_id()] : -1;
+    int si = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int u = __shfl_up_sync(kFull, si, o);
+      if (lane_id() >= static_cast<unsigned>(o)) si = max(si, u);
+    }
+    int ex = __shfl_up_sync(kFull, si, 1);
+    if (lane_id() == 0) ex = -1;
+    if (lane_id() < static_cast<unsigned>(nw)) scratch[lane_id()] = ex;
+  }
+  __syncthreads();
+  int excl_lane = __shfl_up_sync(kFull, inc, 1);
+  if (lane_id() == 0) excl_lane = -1;
+  int res = max(scratch[w], excl_lane);
+  __syncthreads();
+  return res;
+}
+
+// Tie-group start per sorted position: S[p] = largest q <= p with
+// q == 0 || key[q] != key[q-1].  Optionally GE[S[p]] = one past the group end.
+template <typename K>
+FCB_DEV void tie_groups(const K* keys, int m, uint16_t* S, uint16_t* GE, int* scratch) {
+  const int per = (m + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per, e = min(m, b + per);
+  int last = -1;
+  for (int p = b; p < e; ++p)
+    if (p == 0 || keys[p] != keys[p - 1]) last = p;
+  int carry = block_exclusive_max(last, scratch);
+  for (int p = b; p < e; ++p) {
+    if (p == 0 || keys[p] != keys[p - 1]) carry = p;
+    S[p] = static_cast<uint16_t>(carry);
+  }
+  __syncthreads();
+  if (GE != nullptr) {
+    for (int p = b; p < e; ++p)
+      if (p == m - 1 || keys[p] != keys[p + 1]) GE[S[p]] = static_cast<uint16_t>(p + 1);
+    __syncthreads();
+  }
+}
+
+// Blocked exclusive prefix count of pred(p) over p in [0, m): returns the
+// count before this thread's chunk [b, e) and the total.
+template <typename Pred>
+FCB_DEV uint32_t chunk_prefix(int m, Pred pred, int& b, int& e, uint32_t* scan, uint32_t& total) {
+  const int per = (m + blockDim.x - 1) / blockDim.x;
+  b = threadIdx.x * per;
+  e = min(m, b + per);
+  uint32_t c = 0;
+  for (int p = b; p < e; ++p) c += pred(p) ? 1u : 0u;
+  return block_exclusive_sum(c, scan, total);
+}
+
+FCB_DEV void store_row_f32(float* __restrict__ dst, const float* __restrict__ src, int n) {
+  // dst and src share the same 16-byte phase whenever N % 4 == 0 and the
+  // panel is 16-aligned; fall back to scalar stores otherwise.
+  const uintptr_t d = reinterpret_cast<uintptr_t>(dst), s = reinterpret_cast<uintptr_t>(src);
+  if (((d ^ s) & 15u) == 0) {
+    const int head = static_cast<int>(((16 - (d & 15u)) & 15u) / 4);
+    const int h = min(head, n);
+    for (int i = threadIdx.x; i < h; i += blockDim.x) dst[i] = src[i];
+    const int nv = (n - h) / 4;
+    const float4* s4 = reinterpret_cast<const float4*>(src + h);
+    float4* d4 = reinterpret_cast<float4*>(dst + h);
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) d4[i] = s4[i];
+    for (int i = h + nv * 4 + threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// cs_rank
+// ---------------------------------------------------------------------------
+struct CsRankLayout {
+  size_t bars, scratch, k0, k1, i0, i1, total;
+  __host__ __device__ CsRankLayout(int n, size_t sort_scratch) {
+    size_t o = 0;
+    bars = o; o += 64;
+    scratch = o; o = align16(o + sort_scratch);
+    k0 = o; o = align16(o + size_t(n) * 4 + 16);
+    k1 = o; o = align16(o + size_t(n) * 4 + 16);
+    i0 = o; o = align16(o + size_t(n) * 2 + 16);
+    i1 = o; o = align16(o + size_t(n) * 2 + 16);
+    total = o;
+  }
+};
+
+template <int NT, int MAXIPT>
+__global__ void __launch_bounds__(NT, 2048 / NT) k_cs_rank(const float* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                int N, int desc, float* __restrict__ out, int* status) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  const CsRankLayout L(N, SortScratch<NT>::bytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L.bars);
+  uint32_t* scan = reinterpret_cast<uint32_t*>(sm + L.scratch + SortScratch<NT>::hist_bytes +
+                                               SortScratch<NT>::base_bytes);
+  const size_t row = static_cast<size_t>(blockIdx.x) * N;
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t ph0 = 0, ph1 = 0;
+  bool a0 = false, a1 = false;
+  const float* x = stage_issue(sm + L.k1, X + row, N, &bars[0], a0);
+  const uint8_t* mk = nullptr;
+  if (mask != nullptr) mk = stage_issue(sm + L.i1, mask + row, N, &bars[1], a1);
+  bool ok = stage_wait(&bars[0], ph0, a0);
+  ok = stage_wait(&bars[1], ph1, a1) && ok;
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(status, 1);
+    return;
+  }
+  uint32_t* k0 = reinterpret_cast<uint32_t*>(sm + L.k0);
+  uint32_t* k1 = reinterpret_cast<uint32_t*>(sm + L.k1);
+  uint16_t* i0 = reinterpret_cast<uint16_t*>(sm + L.i0);
+  uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
+  const int m = compact_keys<uint32_t>(
+      N, [&](int i) { return finite_f32(x[i]) && (mk == nullptr || mk[i] != 0); },
+      [&](int i) { return key_f32(desc ? -x[i] : x[i]); }, k0, i0, scan);
+  uint32_t* ks;
+  uint16_t* is;
+  block_radix_sort<NT, MAXIPT, uint32_t>(k0, i0, k1, i1, m, sm + L.scratch, &ks, &is);
+  float* rbuf = reinterpret_cast<float*>(ks == k0 ? k1 : k0);
+  const float qnan = __uint_as_float(kQuietNanBits);
+  for (int i = threadIdx.x; i < N; i += NT) rbuf[i] = qnan;
+  __syncthreads();
+  for (int p = threadIdx.x; p < m; p += NT) rbuf[is[p]] = static_cast<float>(p + 1);
+  __syncthreads();
+  store_row_f32(out + row, rbuf, N);
+}
+
+// ---------------------------------------------------------------------------
+// parameter_scan: one ascending sort of the finite cells, four groups
+// ---------------------------------------------------------------------------
+struct ScanLayout {
+  size_t bars, scratch, k0, k1, i0, i1, mf, total;
+  __host__ __device__ ScanLayout(int n, size_t sort_scratch) {
+    size_t o = 0;
+    bars = o; o += 64;
+    scratch = o; o = align16(o + sort_scratch);
+    k0 = o; o = align16(o + size_t(n) * 4 + 16);
+    k1 = o; o = align16(o + size_t(n) * 4 + 16);
+    i0 = o; o = align16(o + size_t(n) * 2 + 16);
+    i1 = o; o = align16(o + size_t(n) * 2 + 16);
+    mf = o; o = align16(o + size_t(n) + 16);
+    total = o;
+  }
+};
+
+template <int NT, int MAXIPT>
+__global__ void __launch_bounds__(NT, 2048 / NT) k_param_scan(const float* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                   int N, ScanOut outs, int* status) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  const ScanLayout L(N, SortScratch<NT>::bytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L.bars);
+  uint32_t* scan = reinterpret_cast<uint32_t*>(sm + L.scratch + SortScratch<NT>::hist_bytes +
+                                               SortScratch<NT>::base_bytes);
+  const size_t row = static_cast<size_t>(blockIdx.x) * N;
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t ph0 = 0, ph1 = 0;
+  bool a0 = false, a1 = false;
+  const float* x = stage_issue(sm + L.k1, X + row, N, &bars[0], a0);
+  const uint8_t* mk = nullptr;
+  if (mask != nullptr) mk = stage_issue(sm + L.mf, mask + row, N, &bars[1], a1);
+  bool ok = stage_wait(&bars[0], ph0, a0);
+  ok = stage_wait(&bars[1], ph1, a1) && ok;
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(status, 1);
+    return;
+  }
+  uint32_t* k0 = reinterpret_cast<uint32_t*>(sm + L.k0);
+  uint32_t* k1 = reinterpret_cast<uint32_t*>(sm + L.k1);
+  uint16_t* i0 = reinterpret_cast<uint16_t*>(sm + L.i0);
+  uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
+  const int m = compact_keys<uint32_t>(
+      N, [&](int i) { return finite_f32(x[i]); }, [&](int i) { return key_f32(x[i]); }, k0, i0, scan);
+  uint32_t* ks;
+  uint16_t* is;
+  block_radix_sort<NT, MAXIPT, uint32_t>(k0, i0, k1, i1, m, sm + L.scratch, &ks, &is);
+  // free buffers: the other key buffer (4n+16 B) and the other index buffer
+  uint8_t* kfree = reinterpret_cast<uint8_t*>(ks == k0 ? k1 : k0);
+  uint16_t* S = (is == i0) ? i1 : i0;                                   // 2n
+  uint16_t* C = reinterpret_cast<uint16_t*>(kfree);                     // 2(n+1)
+  uint16_t* GE = reinterpret_cast<uint16_t*>(kfree) + (N + 1);          // 2n  (fits 4n+16)
+  const bool need_desc = outs.out[2] != nullptr || outs.out[3] != nullptr;
+  const bool need_mask = outs.out[0] != nullptr || outs.out[2] != nullptr;
+  if (need_desc) tie_groups(ks, m, S, GE, reinterpret_cast<int*>(scan));
+  uint32_t mtot = static_cast<uint32_t>(m);
+  if (need_mask) {
+    int b, e;
+    uint32_t c = chunk_prefix(m, [&](int p) { return mk == nullptr || mk[is[p]] != 0; }, b, e, scan, mtot);
+    for (int p = b; p < e; ++p) {
+      C[p] = static_cast<uint16_t>(c);
+      c += (mk == nullptr || mk[is[p]] != 0) ? 1u : 0u;
+    }
+    if (threadIdx.x == 0) C[m] = static_cast<uint16_t>(mtot);
+    __syncthreads();
+  }
+  // ranks buffer aliases the sorted keys (no longer needed once S is built)
+  float* rbuf = reinterpret_cast<float*>(ks);
+  const float qnan = __uint_as_float(kQuietNanBits);
+  for (int g = 0; g < 4; ++g) {
+    if (outs.out[g] == nullptr) continue;
+    for (int i = threadIdx.x; i < N; i += NT) rbuf[i] = qnan;
+    __syncthreads();
+    for (int p = threadIdx.x; p < m; p += NT) {
+      const int i = is[p];
+      const bool mv = (mk == nullptr || mk[i] != 0);
+      switch (g) {
+        case 0:
+          if (mv) rbuf[i] = static_cast<float>(C[p] + 1);
+          break;
+        case 1:
+          rbuf[i] = static_cast<float>(p + 1);
+          break;
+        case 2:
+          if (mv) {
+            const int s = S[p], e = GE[s];
+            rbuf[i] = static_cast<float>(static_cast<int>(mtot) - C[e] + (C[p] - C[s]) + 1);
+          }
+          break;
+        default: {
+          const int s = S[p], e = GE[s];
+          rbuf[i] = static_cast<float>(m - e + (p - s) + 1);
+        }
+      }
+    }
+    __syncthreads();
+    store_row_f32(outs.out[g] + row, rbuf, N);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// rank + IC over F factor panels sharing one forward-return panel
+// ---------------------------------------------------------------------------
+struct RankIcLayout {
+  size_t bars, scratch, k0, k1, i0, i1, flags, ir, gr, rr, total;
+  __host__ __device__ RankIcLayout(int n, int ksz, size_t sort_scratch) {
+    size_t o = 0;
+    bars = o; o += 64;
+    scratch = o; o = align16(o + sort_scratch);
+    k0 = o; o = align16(o + size_t(n) * ksz + 16);
+    k1 = o; o = align16(o + size_t(n) * ksz + 16);
+    i0 = o; o = align16(o + size_t(n) * 2 + 16);
+    i1 = o; o = align16(o + size_t(n) * 2 + 16);
+    flags = o; o = align16(o + size_t(n) + 16);
+    ir = o; o = align16(o + size_t(n) * 2);
+    gr = o; o = align16(o + size_t(n) * 2);
+    rr = o; o = align16(o + size_t(n) * 2);
+    total = o;
+  }
+};
+
+// IC from the exact integer sums (see k_rank_ic header comment).
+FCB_DEV double spearman_from_sum(long long m, long long sum_rr) {
+  const long long s4 = 4 * sum_rr - m * (m + 1) * (m + 1);  // 4*sxy
+  const long long q4 = m * (m * m - 1) / 3;                // 4*sxx == 4*syy
+  const double sxy = static_cast<double>(s4) * 0.25;
+  const double sxx = static_cast<double>(q4) * 0.25;
+  return (sxy / sqrt(sxx)) / sqrt(sxx);
+}
+
+template <int NT, int MAXIPT, typename TF, typename TR>
+__global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(RankIcArgs<TF, TR> a, int* status) {
+  using KF = typename KeyOf<TF>::type;
+  using KR = typename KeyOf<TR>::type;
+  constexpr int KSZ = (sizeof(KF) > sizeof(KR)) ? int(sizeof(KF)) : int(sizeof(KR));
+  extern __shared__ __align__(16) uint8_t sm[];
+  const int N = a.N, T = a.T;
+  const RankIcLayout L(N, KSZ, SortScratch<NT>::bytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L.bars);
+  uint32_t* scan = reinterpret_cast<uint32_t*>(sm + L.scratch + SortScratch<NT>::hist_bytes +
+                                               SortScratch<NT>::base_bytes);
+  unsigned long long* scan64 = reinterpret_cast<unsigned long long*>(scan);
+  const int t = blockIdx.x;
+  const size_t row = static_cast<size_t>(t) * N;
+  uint8_t* flags = sm + L.flags;
+  uint16_t* IR = reinterpret_cast<uint16_t*>(sm + L.ir);
+  uint16_t* GR = reinterpret_cast<uint16_t*>(sm + L.gr);
+  uint16_t* RR = reinterpret_cast<uint16_t*>(sm + L.rr);
+  uint16_t* i0 = reinterpret_cast<uint16_t*>(sm + L.i0);
+  uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
+
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < 4; ++b) mbar_init(&bars[b], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t ph[4] = {0, 0, 0, 0};
+  bool arm[4] = {false, false, false, false};
+
+  // ---- stage forward returns and both masks; flags bit0 = return valid, bit1 = factor mask
+  const TR* r = stage_issue(sm + L.k1, a.R + row, N, &bars[0], arm[0]);
+  const uint8_t* rm = nullptr;
+  const uint8_t* fm = nullptr;
+  if (a.rmask != nullptr) rm = stage_issue(sm + L.i1, a.rmask + row, N, &bars[1], arm[1]);
+  if (a.fmask != nullptr) fm = stage_issue(sm + L.i0, a.fmask + row, N, &bars[2], arm[2]);
+  bool ok = stage_wait(&bars[0], ph[0], arm[0]);
+  ok = stage_wait(&bars[1], ph[1], arm[1]) && ok;
+  ok = stage_wait(&bars[2], ph[2], arm[2]) && ok;
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(status, 1);
+    return;
+  }
+  for (int i = threadIdx.x; i < N; i += NT) {
+    const bool rv = KeyOf<TR>::finite(r[i]) && (rm == nullptr || rm[i] != 0);
+    const bool fv = (fm == nullptr) || fm[i] != 0;
+    flags[i] = static_cast<uint8_t>((rv ? 1u : 0u) | (fv ? 2u : 0u));
+  }
+  __syncthreads();
+
+  // ---- sort the forward returns once per date
+  KR* kr0 = reinterpret_cast<KR*>(sm + L.k0);
+  KR* kr1 = reinterpret_cast<KR*>(sm + L.k1);
+  const int mr = compact_keys<KR>(
+      N, [&](int i) { return (flags[i] & 1u) != 0; }, [&](int i) { return KeyOf<TR>::key(r[i]); }, kr0, i0,
+      scan);
+  KR* krs;
+  uint16_t* irs;
+  block_radix_sort<NT, MAXIPT, KR>(kr0, i0, kr1, i1, mr, sm + L.scratch, &krs, &irs);
+  for (int p = threadIdx.x; p < mr; p += NT) IR[p] = irs[p];
+  tie_groups(krs, mr, GR, static_cast<uint16_t*>(nullptr), reinterpret_cast<int*>(scan));
+
+  // ---- per factor
+  for (int f = 0; f < a.F; ++f) {
+    const size_t frow = (static_cast<size_t>(f) * T + t) * N;
+    const TF* x = stage_issue(sm + L.k1, a.X + frow, N, &bars[3], arm[3]);
+    ok = stage_wait(&bars[3], ph[3], arm[3]);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicExch(status, 1);
+      return;
+    }
+    for (int i = threadIdx.x; i < N; i += NT)
+      flags[i] = static_cast<uint8_t>((flags[i] & 3u) | (KeyOf<TF>::finite(x[i]) ? 4u : 0u));
+    __syncthreads();
+    KF* kf0 = reinterpret_cast<KF*>(sm + L.k0);
+    KF* kf1 = reinterpret_cast<KF*>(sm + L.k1);
+    const int mf = compact_keys<KF>(
+        N, [&](int i) { return (flags[i] & 6u) == 6u; }, [&](int i) { return KeyOf<TF>::key(x[i]); }, kf0, i0,
+        scan);
+    KF* kfs;
+    uint16_t* ifs;
+    block_radix_sort<NT, MAXIPT, KF>(kf0, i0, kf1, i1, mf, sm + L.scratch, &kfs, &ifs);
+
+    // returns side: joint ranks in return order, first/last joint position
+    int b, e;
+    uint32_t mj;
+    uint32_t c = chunk_prefix(mr, [&](int p) { return flags[IR[p]] == 7u; }, b, e, scan, mj);
+    int rfirst = 0x7fffffff, rlast = -1;
+    for (int p = b; p < e; ++p) {
+      const int i = IR[p];
+      if (flags[i] == 7u) {
+        RR[i] = static_cast<uint16_t>(++c);
+        rfirst = min(rfirst, p);
+        rlast = max(rlast, p);
+      }
+    }
+    rfirst = block_min_int(rfirst, reinterpret_cast<int*>(scan));
+    rlast = block_max_int(rlast, reinterpret_cast<int*>(scan));
+
+    // factor side: cs ranks, joint ranks, sum of rank products
+    float* rbuf = reinterpret_cast<float*>(kfs == kf0 ? kf1 : kf0);
+    const bool want_ranks = a.ranks_out != nullptr;
+    if (want_ranks) {
+      const float qnan = __uint_as_float(kQuietNanBits);
+      for (int i = threadIdx.x; i < N; i += NT) rbuf[i] = qnan;
+    }
+    if (a.rank_f_out != nullptr) {
+      for (int i = threadIdx.x; i < N; i += NT) {
+        a.rank_f_out[frow + i] = 0.0;
+        a.rank_r_out[frow + i] = 0.0;
+      }
+    }
+    __syncthreads();
+    uint32_t mj2;
+    uint32_t cf = chunk_prefix(mf, [&](int p) { return flags[ifs[p]] == 7u; }, b, e, scan, mj2);
+    long long sum = 0;
+    int ffirst = 0x7fffffff, flast = -1;
+    for (int p = b; p < e; ++p) {
+      const int i = ifs[p];
+      if (want_ranks) rbuf[i] = static_cast<float>(p + 1);
+      if (flags[i] == 7u) {
+        ++cf;
+        sum += static_cast<long long>(cf) * RR[i];
+        ffirst = min(ffirst, p);
+        flast = max(flast, p);
+        if (a.rank_f_out != nullptr) {
+          a.rank_f_out[frow + i] = static_cast<double>(cf);
+          a.rank_r_out[frow + i] = static_cast<double>(RR[i]);
+        }
+      }
+    }
+    sum = block_sum<unsigned long long>(static_cast<unsigned long long>(sum), scan64);
+    ffirst = block_min_int(ffirst, reinterpret_cast<int*>(scan));
+    flast = block_max_int(flast, reinterpret_cast<int*>(scan));
+    if (threadIdx.x == 0) {
+      double ic = __longlong_as_double(0x7ff8000000000000ll);
+      const long long m = static_cast<long long>(mj);
+      if (m >= a.min_valid && m >= 2) {
+        const bool fconst = kfs[ffirst] == kfs[flast];
+        const bool rconst = GR[rfirst] == GR[rlast];
+        if (!fconst && !rconst) ic = spearman_from_sum(m, sum);
+      }
+      a.ic_out[static_cast<size_t>(f) * T + t] = ic;
+    }
+    __syncthreads();
+    if (want_ranks) store_row_f32(a.ranks_out + frow, rbuf, N);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+template <int NT>
+constexpr int cap_of() { return NT * 16; }
+
+static int pick_nt(int n) { return n <= 4096 ? 256 : (n <= 8192 ? 512 : 1024); }
+
+size_t cs_rank_smem(int N) {
+  return CsRankLayout(N, SortScratch<1024>::bytes).total;
+}
+
+template <int NT>
+static cudaError_t launch_cs_rank_nt(const float* X, const uint8_t* mask, int T, int N, int desc, float* out,
+                                     int* status, cudaStream_t st) {
+  const size_t smem = CsRankLayout(N, SortScratch<NT>::bytes).total;
+  cudaError_t e = cudaFuncSetAttribute(k_cs_rank<NT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  k_cs_rank<NT, 16><<<T, NT, smem, st>>>(X, mask, N, desc, out, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cs_rank(const float* X, const uint8_t* mask, int T, int N, int desc, float* out,
+                           int* status, cudaStream_t st) {
+  if (N > kSmemRankCap) return cudaErrorInvalidValue;
+  switch (pick_nt(N)) {
+    case 256: return launch_cs_rank_nt<256>(X, mask, T, N, desc, out, status, st);
+    case 512: return launch_cs_rank_nt<512>(X, mask, T, N, desc, out, status, st);
+    default: return launch_cs_rank_nt<1024>(X, mask, T, N, desc, out, status, st);
+  }
+}
+
+template <int NT>
+static cudaError_t launch_scan_nt(const float* X, const uint8_t* mask, int T, int N, ScanOut outs, int* status,
+                                  cudaStream_t st) {
+  const size_t smem = ScanLayout(N, SortScratch<NT>::bytes).total;
+  cudaError_t e = cudaFuncSetAttribute(k_param_scan<NT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  k_param_scan<NT, 16><<<T, NT, smem, st>>>(X, mask, N, outs, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_param_scan(const float* X, const uint8_t* mask, int T, int N, ScanOut outs, int* status,
+                              cudaStream_t st) {
+  if (N > kSmemRankCap) return cudaErrorInvalidValue;
+  switch (pick_nt(N)) {
+    case 256: return launch_scan_nt<256>(X, mask, T, N, outs, status, st);
+    case 512: return launch_scan_nt<512>(X, mask, T, N, outs, status, st);
+    default: return launch_scan_nt<1024>(X, mask, T, N, outs, status, st);
+  }
+}
+
+template <typename TF, typename TR>
+size_t rank_ic_smem(int N) {
+  constexpr int KSZ = (sizeof(TF) > sizeof(TR)) ? int(sizeof(TF)) : int(sizeof(TR));
+  return RankIcLayout(N, KSZ, SortScratch<1024>::bytes).total;
+}
+template size_t rank_ic_smem<float, float>(int);
+template size_t rank_ic_smem<float, double>(int);
+template size_t rank_ic_smem<double, float>(int);
+template size_t rank_ic_smem<double, double>(int);
+
+template <int NT, typename TF, typename TR>
+static cudaError_t launch_rank_ic_nt(const RankIcArgs<TF, TR>& a, int* status, cudaStream_t st) {
+  constexpr int KSZ = (sizeof(TF) > sizeof(TR)) ? int(sizeof(TF)) : int(sizeof(TR));
+  const size_t smem = RankIcLayout(a.N, KSZ, SortScratch<NT>::bytes).total;
+  if (smem > kMaxSmemPerBlock) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_rank_ic<NT, 16, TF, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  k_rank_ic<NT, 16, TF, TR><<<a.T, NT, smem, st>>>(a, status);
+  return cudaGetLastError();
+}
+
+template <typename TF, typename TR>
+cudaError_t launch_rank_ic(const RankIcArgs<TF, TR>& a, int* status, cudaStream_t st) {
+  if (a.N > kSmemRankCap) return cudaErrorInvalidValue;
+  switch (pick_nt(a.N)) {
+    case 256: return launch_rank_ic_nt<256>(a, status, st);
+    case 512: return launch_rank_ic_nt<512>(a, status, st);
+    default: return launch_rank_ic_nt<1024>(a, status, st);
+  }
+}
+template cudaError_t launch_rank_ic<float, float>(const RankIcArgs<float, float>&, int*, cudaStream_t);
+template cudaError_t launch_rank_ic<float, double>(const RankIcArgs<float, double>&, int*, cudaStream_t);
+template cudaError_t launch_rank_ic<double, float>(const RankIcArgs<double, float>&, int*, cudaStream_t);
+template cudaError_t launch_rank_ic<double, double>(const RankIcArgs<double, double>&, int*, cudaStream_t);
+
+}  // namespace fcb

@@ -1,0 +1,418 @@
+"""fcb200 -- B200-native cross-sectional analysis path with factor-cuda's ``fc.*`` API.
+
+Public functions mirror the reference adapter (``fc/__init__.py:5-29``):
+``cross_sectional_rank``, ``factor_plane``, ``parameter_scan``, ``rolling_ic``,
+``factor_corr``, ``stock_corr`` and ``clear_workspaces``, with the same
+argument names, validation (dtype whitelist, strict-bool masks, f64->f32
+downcast for the rank ops, ``min_valid`` int >= 2), error classes and output
+containers (numpy in -> numpy out, torch in -> torch out on the input device).
+
+Every compute call goes to the CUDA path through the drop-in pybind11 modules
+``factor_cuda_pybind`` / ``factor_corr_pybind`` over ``libfcb200.so``.  There is
+no CPU backend: ``backend='cpu'`` / ``device='cpu'`` raise, and a missing GPU or
+build raises ``RuntimeError``.  (The reference's own adapter keeps its CPU
+oracle; use it unchanged with these modules for a CPU fallback.)
+
+Extensions beyond the reference API: ``rank_ic_panel`` (F factors against one
+forward-return panel in one call), ``workspace_stats``.
+"""
+from __future__ import annotations
+
+import threading
+import time
+from contextlib import contextmanager
+
+import numpy as np
+
+from . import _native as nat
+
+try:  # optional, only to accept / return torch tensors
+    import torch as _torch
+except Exception:  # pragma: no cover
+    _torch = None
+
+__version__ = "1.0.0"
+__all__ = ["cross_sectional_rank", "factor_plane", "factor_corr", "stock_corr", "rolling_ic",
+           "parameter_scan", "rank_ic_panel", "clear_workspaces", "__version__"]
+
+_WHITELIST = (np.float32, np.float64)
+DOMAIN_MSG = ("correlation domain violation: max|x| > 1e150 or a nonzero |x| < 1e-150 "
+              "on a valid cell")
+
+
+# ---------------------------------------------------------------------------
+# container / validation helpers (reference fc/_util.py:79-197)
+# ---------------------------------------------------------------------------
+def _dtype_ok(dt, dtypes):
+    if _torch is not None and isinstance(dt, _torch.dtype):
+        allowed = {"f32": (_torch.float32,), "f64": (_torch.float64,)}.get(
+            dtypes, (_torch.float32, _torch.float64))
+        return dt in allowed
+    allowed = {"f32": (np.float32,), "f64": (np.float64,)}.get(dtypes, _WHITELIST)
+    return dt in allowed
+
+
+def _to_numpy(x, *, name, ndim, dtypes="f32f64", downcast_to=None):
+    kind, device = "numpy", "cpu"
+    if isinstance(x, np.ndarray):
+        if not _dtype_ok(x.dtype, dtypes):
+            raise ValueError(f"{name} dtype {x.dtype} not in whitelist {{float32,float64}}")
+        arr = np.ascontiguousarray(x)
+    elif _torch is not None and isinstance(x, _torch.Tensor):
+        kind = "torch"
+        device = "cpu" if not x.is_cuda else f"cuda:{x.device.index}"
+        x = x.detach()
+        if not _dtype_ok(x.dtype, dtypes):
+            raise ValueError(f"{name} dtype {x.dtype} not in whitelist {{float32,float64}}")
+        arr = x.contiguous().cpu().numpy()
+    else:
+        if _torch is None:
+            raise TypeError(f"{name} must be a numpy array or torch.Tensor")
+        try:
+            t = _torch.utils.dlpack.from_dlpack(x)
+        except (RuntimeError, TypeError, AttributeError):
+            if type(x).__name__ == "PyCapsule":
+                raise ValueError(f"{name}: DLPack capsule already consumed") from None
+            raise TypeError(f"{name} must be a numpy array, torch.Tensor, or DLPack capsule") from None
+        kind = "dlpack"
+        device = "cpu" if not t.is_cuda else f"cuda:{t.device.index}"
+        if not _dtype_ok(t.dtype, dtypes):
+            raise ValueError(f"{name} dtype {t.dtype} not in whitelist {{float32,float64}}")
+        arr = t.detach().contiguous().cpu().numpy()
+    ok = arr.ndim == ndim if isinstance(ndim, int) else arr.ndim in ndim
+    if not ok:
+        raise ValueError(f"{name} must be {ndim}-D, got ndim={arr.ndim}")
+    if downcast_to == "float32" and arr.dtype == np.float64:
+        arr = arr.astype(np.float32)  # IEEE round-to-nearest-even
+    return kind, device, np.ascontiguousarray(arr)
+
+
+def _check_mask(mask, *, name, T, N, allow_none=True):
+    if mask is None:
+        if allow_none:
+            return None
+        raise ValueError(f"{name} is required")
+    if isinstance(mask, np.ndarray):
+        if mask.dtype != np.bool_:
+            raise ValueError(f"{name} must be bool, got {mask.dtype}")
+        arr = np.ascontiguousarray(mask)
+    elif _torch is not None and isinstance(mask, _torch.Tensor):
+        if mask.dtype != _torch.bool:
+            raise ValueError(f"{name} must be bool, got {mask.dtype}")
+        arr = mask.detach().cpu().numpy()
+    else:
+        raise TypeError(f"{name} must be a bool numpy array or torch.Tensor")
+    if arr.shape != (T, N):
+        raise ValueError(f"{name} shape must be (T,N) matching input, got {arr.shape}")
+    return arr
+
+
+def _mask_device(mask, device, name):
+    if mask is None:
+        return
+    md = "cpu"
+    if _torch is not None and isinstance(mask, _torch.Tensor) and mask.is_cuda:
+        md = f"cuda:{mask.device.index}"
+    if md != device:
+        raise ValueError(f"{name} must be on the same device as values ({device}), got {md}")
+
+
+def _require_cuda(context):
+    if nat.device_count() < 1:
+        raise RuntimeError(f"CUDA unavailable: {context} runs on the GPU only in fcb200")
+
+
+def _sync_entry(device):
+    if _torch is not None and device.startswith("cuda") and _torch.cuda.is_available():
+        _torch.cuda.current_stream(int(device.split(":")[1])).synchronize()
+
+
+def _make_output(res, kind, device):
+    if kind == "numpy":
+        return res
+    return _torch.as_tensor(res, device=_torch.device(device if device != "cpu" else "cpu"))
+
+
+def _domain_check(arr, mask):
+    """max|x| <= 1e150 and min nonzero |x| >= 1e-150 over valid cells; f32
+    panels always satisfy it (fc/correlation.py:16-49)."""
+    if arr.dtype == np.float32:
+        return
+    if arr.ndim == 3:
+        T, N, F = arr.shape
+        flat = arr.reshape(T * N, F)
+        valid = np.isfinite(flat)
+        if mask is not None:
+            valid &= mask.reshape(T * N, 1)
+    else:
+        flat = arr
+        valid = np.isfinite(flat)
+        if mask is not None:
+            valid &= mask
+    xv = np.abs(flat[valid])
+    if xv.size == 0:
+        return
+    if xv.max() > 1e150:
+        raise ValueError(DOMAIN_MSG)
+    nz = xv[xv != 0.0]
+    if nz.size and nz.min() < 1e-150:
+        raise ValueError(DOMAIN_MSG)
+
+
+# ---------------------------------------------------------------------------
+# per-shape workspace cache (reference fc/_workspace.py:42-133)
+# ---------------------------------------------------------------------------
+class _WorkspaceCache:
+    _all: list = []
+
+    def __init__(self, factory):
+        self._factory = factory
+        self._items = {}
+        self._guard = threading.Lock()
+        _WorkspaceCache._all.append(self)
+
+    @contextmanager
+    def use(self, key):
+        with self._guard:
+            item = self._items.get(key)
+            if item is None:
+                item = (self._factory(), threading.Lock())
+                self._items[key] = item
+            ws, lock = item
+            lock.acquire()
+        try:
+            yield ws
+        finally:
+            lock.release()
+
+    def clear(self):
+        with self._guard:
+            items = list(self._items.values())
+            self._items = {}
+        for ws, lock in items:
+            with lock:
+                ws.clear()
+
+
+_RANK_CACHE = _WorkspaceCache(lambda: nat.fcb().CsRankWorkspace())
+_SCAN_CACHE = _WorkspaceCache(lambda: nat.fcb().CsRankWorkspace())
+_ROLL_CACHE = _WorkspaceCache(lambda: nat.fcb().RollingIcWorkspace())
+
+
+def clear_workspaces():
+    """Release every cached device workspace (idempotent)."""
+    for c in _WorkspaceCache._all:
+        c.clear()
+
+
+# ---------------------------------------------------------------------------
+# operators
+# ---------------------------------------------------------------------------
+def cross_sectional_rank(values, mask=None, descending=False):
+    """Stable ordinal rank 1..K per date; invalid cells NaN (0x7fc00000).
+    Reference: fc/cross_sectional_rank.py:19-35."""
+    if type(descending) is not bool:
+        raise ValueError("descending must be a bool (type(x) is bool), got "
+                         f"{type(descending).__name__}")
+    kind, device, x = _to_numpy(values, name="values", ndim=2, downcast_to="float32")
+    T, N = x.shape
+    _require_cuda("cross_sectional_rank")
+    _mask_device(mask, device, "mask")
+    m = _check_mask(mask, name="mask", T=T, N=N)
+    _sync_entry(device)
+    with _RANK_CACHE.use((T, N)) as ws:
+        res = nat.fcb().cs_rank_f32(x, m, descending, workspace=ws)
+    return _make_output(res, kind, device)
+
+
+def factor_plane(factors, f):
+    """Factor f of a (T,N,F) panel as a fresh (T,N) array
+    (fc/cross_sectional_rank.py:38-54)."""
+    if not isinstance(f, int) or isinstance(f, bool):
+        raise ValueError(f"f must be an integer, got {type(f).__name__}")
+    kind, device, arr = _to_numpy(factors, name="factors", ndim=(2, 3))
+    if arr.ndim == 2:
+        if f != 0:
+            raise ValueError("ndim=2 input requires f == 0")
+        plane = np.array(arr, copy=True)
+    else:
+        if not (0 <= f < arr.shape[2]):
+            raise ValueError(f"f={f} out of range [0,F={arr.shape[2]})")
+        plane = np.ascontiguousarray(arr[..., f])
+    return _make_output(plane, kind, device)
+
+
+_AXES = ("direction", "mask_mode")
+_DIR = ("ascending", "descending")
+_MM = ("masked", "unmasked")
+_BINDING_INDEX = {"ascending": {"masked": 0, "unmasked": 1},
+                  "descending": {"masked": 2, "unmasked": 3}}
+
+
+def _normalize_axes(axes):
+    if not isinstance(axes, (list, tuple)) or not all(
+            isinstance(a, (list, tuple)) and len(a) == 2 for a in axes):
+        raise ValueError("axes must be a list of (axis_name, values_list) tuples")
+    user, seen = {}, set()
+    for name, vals in axes:
+        if name not in _AXES:
+            raise ValueError(f"unknown scan axis {name!r}; allowed: direction, mask_mode")
+        if name in seen:
+            raise ValueError(f"duplicate axis {name!r}")
+        seen.add(name)
+        if not isinstance(vals, (list, tuple)) or len(vals) == 0:
+            raise ValueError(f"axis {name!r} values must be non-empty")
+        if len(set(vals)) != len(vals):
+            raise ValueError(f"axis {name!r} contains duplicate values")
+        if name == "direction" and not set(vals) <= set(_DIR):
+            raise ValueError(f"direction values must be in {_DIR}")
+        if name == "mask_mode" and not set(vals) <= set(_MM):
+            raise ValueError(f"mask_mode values must be in {_MM}")
+        user[name] = list(vals)
+    eff = {"direction": user.get("direction", ["ascending"]),
+           "mask_mode": user.get("mask_mode", ["masked"])}
+    return eff, [(d, m) for d in eff["direction"] for m in eff["mask_mode"]]
+
+
+def parameter_scan(axes, X, mask=None):
+    """direction x mask_mode rank scan; results always host numpy
+    (fc/parameter_scan.py:62-132).  The active groups come from one fused pass."""
+    effective, combos = _normalize_axes(axes)
+    _, device, x = _to_numpy(X, name="X", ndim=2, downcast_to="float32")
+    T, N = x.shape
+    _require_cuda("parameter_scan")
+    if N > (1 << 24):
+        raise ValueError("N > 2^24 (rank precision cap)")
+    any_masked = any(mm == "masked" for _, mm in combos)
+    m = (_check_mask(mask, name="mask", T=T, N=N, allow_none=False) if any_masked
+         else np.ones((T, N), dtype=np.bool_))
+    active = [0, 0, 0, 0]
+    for d, mm in combos:
+        active[_BINDING_INDEX[d][mm]] = 1
+    _sync_entry(device)
+    t0 = time.perf_counter()
+    with _SCAN_CACHE.use((T, N)) as ws:
+        r = nat.fcb().parameter_scan_f32(x, m, return_timing=True, active_groups=active, workspace=ws)
+    elapsed_ms = (time.perf_counter() - t0) * 1e3
+    groups = []
+    for gi, (d, mm) in enumerate(combos):
+        g = _BINDING_INDEX[d][mm]
+        st = r["group_status"][g]
+        if st == 0:
+            groups.append({"group_index": gi, "axis_values": {"direction": d, "mask_mode": mm},
+                           "result": r["groups"][g], "status": "ok", "error": None,
+                           "error_stage": None, "time_ms": r["time_ms"][g],
+                           "time_gpu_ms": r["time_gpu_ms"][g]})
+        elif st in (9, 701):
+            groups.append({"group_index": gi, "axis_values": {"direction": d, "mask_mode": mm},
+                           "result": None, "status": "failed",
+                           "error": f"group-level CUDA error {st}", "error_stage": "launch",
+                           "time_ms": 0.0, "time_gpu_ms": 0.0})
+        else:
+            raise RuntimeError(f"non-whitelist CUDA status {st} for group {g} "
+                               "(must be scan-level, not group-failed)")
+    ok = [g for g in groups if g["status"] == "ok"]
+    return {"spec": effective, "groups": groups,
+            "summary": {"total_groups": len(combos),
+                        "n_failed": sum(1 for g in groups if g["status"] == "failed"),
+                        "total_time_ms": sum(g["time_ms"] for g in ok),
+                        "total_time_gpu_ms": sum(g["time_gpu_ms"] for g in ok),
+                        "elapsed_ms": elapsed_ms}}
+
+
+def rolling_ic(factor, forward_returns, factor_mask=None, fwd_mask=None, min_valid=30, device=None):
+    """Daily Spearman IC (T,) f64 (fc/rolling_ic.py:16-57); GPU only."""
+    if device not in (None, "cpu", "cuda"):
+        raise ValueError(f"device must be None, 'cpu', or 'cuda', got {device!r}")
+    if not isinstance(min_valid, int) or isinstance(min_valid, bool):
+        raise ValueError("min_valid must be an integer (bool rejected)")
+    if min_valid < 2:
+        raise ValueError("min_valid must be >= 2")
+    kf, df, f = _to_numpy(factor, name="factor", ndim=2)
+    kr, dr, r = _to_numpy(forward_returns, name="forward_returns", ndim=2)
+    T, N = f.shape
+    if r.shape != (T, N):
+        raise ValueError(f"factor and forward_returns shapes must match (T,N), got {f.shape} vs {r.shape}")
+    _mask_device(factor_mask, df, "factor_mask")
+    _mask_device(fwd_mask, df, "fwd_mask")
+    fm = _check_mask(factor_mask, name="factor_mask", T=T, N=N)
+    rm = _check_mask(fwd_mask, name="fwd_mask", T=T, N=N)
+    if device == "cpu":
+        raise NotImplementedError("fcb200 has no CPU backend; use the reference adapter for device='cpu'")
+    _require_cuda("rolling_ic")
+    _sync_entry(df)
+    with _ROLL_CACHE.use((T, N)) as ws:
+        res = nat.fcb().rolling_ic_f64(f, r, fm, rm, min_valid, workspace=ws)
+    kind = "torch" if (kf == "torch" or kr == "torch") else "numpy"
+    if kind == "numpy":
+        return res
+    return _torch.as_tensor(res, device=_torch.device(df))
+
+
+def factor_corr(data, mask=None, names=None, backend="cuda"):
+    """(F,F) pooled pairwise-complete correlation (fc/correlation.py:52-72)."""
+    if backend not in ("cpu", "cuda"):
+        raise ValueError(f"backend must be 'cpu' or 'cuda', got {backend!r}")
+    kind, device, arr = _to_numpy(data, name="data", ndim=3)
+    T, N, F = arr.shape
+    if names is not None and len(names) != F:
+        raise ValueError(f"names length {len(names)} must equal F={F}")
+    if backend == "cpu":
+        raise NotImplementedError("fcb200 has no CPU backend; use the reference adapter for backend='cpu'")
+    _require_cuda("factor_corr backend='cuda'")
+    _mask_device(mask, device, "mask")
+    m = _check_mask(mask, name="mask", T=T, N=N)
+    if F > 128:
+        raise ValueError("F > 128 (factor pair grid cap)")
+    _domain_check(arr, m)
+    _sync_entry(device)
+    res = nat.fcp().factor_corr_f64(arr, m)
+    return res if kind == "numpy" else _make_output(res, kind, device)
+
+
+def stock_corr(data, mask=None, backend="cuda"):
+    """(N,N) pairwise-complete correlation over t (fc/correlation.py:75-93)."""
+    if backend not in ("cpu", "cuda"):
+        raise ValueError(f"backend must be 'cpu' or 'cuda', got {backend!r}")
+    kind, device, arr = _to_numpy(data, name="data", ndim=2)
+    T, N = arr.shape
+    if backend == "cpu":
+        raise NotImplementedError("fcb200 has no CPU backend; use the reference adapter for backend='cpu'")
+    _require_cuda("stock_corr backend='cuda'")
+    _mask_device(mask, device, "mask")
+    m = _check_mask(mask, name="mask", T=T, N=N)
+    if int(N) * N > (1 << 31) - 1:
+        raise ValueError("N*N exceeds INT32_MAX (output grid cap, N <= 46340)")
+    _domain_check(arr, m)
+    _sync_entry(device)
+    res = nat.fcb().stock_corr_f64(arr, m)
+    return res if kind == "numpy" else _make_output(res, kind, device)
+
+
+# ---------------------------------------------------------------------------
+# extensions
+# ---------------------------------------------------------------------------
+def rank_ic_panel(X, forward_returns, factor_mask=None, fwd_mask=None, min_valid=30,
+                  method="radix", return_ranks=True):
+    """cs_rank + rolling_ic of F factor panels X (F,T,N) f32 against one
+    forward-return panel (T,N) f32, in one streamed call.  Returns
+    ``(ranks (F,T,N) f32 | None, ic (F,T) f64)``; ranks follow
+    cross_sectional_rank(X[f], factor_mask), ic follows
+    rolling_ic(X[f], forward_returns, factor_mask, fwd_mask, min_valid)."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    R = np.ascontiguousarray(forward_returns, dtype=np.float32)
+    if X.ndim != 3 or R.shape != X.shape[1:]:
+        raise ValueError("X must be (F,T,N) and forward_returns (T,N)")
+    F, T, N = X.shape
+    if not isinstance(min_valid, int) or isinstance(min_valid, bool) or min_valid < 2:
+        raise ValueError("min_valid must be an integer >= 2")
+    meth = {"radix": 0, "learned": 1}[method]
+    fm = None if factor_mask is None else np.ascontiguousarray(factor_mask, dtype=np.uint8)
+    rm = None if fwd_mask is None else np.ascontiguousarray(fwd_mask, dtype=np.uint8)
+    _require_cuda("rank_ic_panel")
+    ranks = np.empty((F, T, N), np.float32) if return_ranks else None
+    ic = np.empty((F, T), np.float64)
+    rc = nat.lib().fcb_rank_ic_panel(nat.ptr(X), nat.ptr(R), nat.ptr(fm), nat.ptr(rm), F, T, N, min_valid,
+                                     nat.ptr(ranks), nat.ptr(ic), meth, None)
+    nat.check(rc, "rank_ic_panel")
+    return ranks, ic

@@ -1,0 +1,110 @@
+"""Loader for the native library and the drop-in binding modules.
+
+``lib()`` returns the ctypes handle of ``build/libfcb200.so`` with every C ABI
+prototype declared (include/fcb200.h).  ``fcb()`` / ``fcp()`` import the
+drop-in pybind11 modules ``factor_cuda_pybind`` / ``factor_corr_pybind`` from
+the same build directory (the reference adapter's ``fc/_util.py:200-219``
+loads modules of these names from its own ``build/``).
+
+There is no fallback: a missing build raises ``RuntimeError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import functools
+import importlib
+import pathlib
+import sys
+
+PKG = pathlib.Path(__file__).resolve().parent.parent
+BUILD = PKG / "build"
+LIB = BUILD / "libfcb200.so"
+
+FCB_DTYPE_F32 = 0
+FCB_DTYPE_F64 = 1
+FCB_GROUP_NOT_EXECUTED = -100
+FCB_ERR_DEVICE_WAIT = 100000
+
+_p = C.c_void_p
+_i = C.c_int
+_d = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes); the symbol table of include/fcb200.h
+PROTOTYPES = {
+    "fcb_workspace_create": (_p, []),
+    "fcb_workspace_clear": (None, [_p]),
+    "fcb_workspace_destroy": (None, [_p]),
+    "fcb_workspace_stats": (_i, [_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "fcb_version": (_i, []),
+    "fcb_device_count": (_i, []),
+    "fcb_status_string": (C.c_char_p, [_i]),
+    "fcb_host_alloc": (_p, [C.c_size_t]),
+    "fcb_host_free": (None, [_p]),
+    "fcb_cs_rank_f32": (_i, [_p, _p, _i, _i, _i, _p, _p]),
+    "fcb_parameter_scan_f32": (_i, [_p, _p, _i, _i, C.POINTER(_p), C.POINTER(_i), _d, C.POINTER(C.c_float),
+                                    C.POINTER(_i), _p]),
+    "fcb_rolling_ic": (_i, [_p, _i, _p, _i, _p, _p, _i, _i, _i, _p, _p, _p, _p]),
+    "fcb_factor_corr": (_i, [_p, _i, _p, _i, _i, _i, _p, _p]),
+    "fcb_stock_corr": (_i, [_p, _i, _p, _i, _i, _p, C.POINTER(_i), C.POINTER(_i)]),
+    "fcb_rank_ic_panel": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i, _p]),
+    "fcb_dev_rank_ic_panel": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i, _p]),
+    "fcb_dev_cs_rank_f32": (_i, [_p, _p, _i, _i, _i, _p, _p]),
+}
+
+
+@functools.lru_cache(maxsize=1)
+def lib():
+    if not LIB.exists():
+        raise RuntimeError(f"libfcb200.so not built ({LIB}); run python factor-cuda_b200/fcb_build.py")
+    h = C.CDLL(str(LIB))
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(h, name)
+        fn.restype = res
+        fn.argtypes = args
+    return h
+
+
+def _load_module(name: str):
+    b = str(BUILD)
+    if b not in sys.path:
+        sys.path.insert(0, b)
+    try:
+        return importlib.import_module(name)
+    except ImportError as e:
+        raise RuntimeError(f"binding {name} not found in {BUILD}; run python factor-cuda_b200/fcb_build.py") from e
+
+
+@functools.lru_cache(maxsize=1)
+def fcb():
+    return _load_module("factor_cuda_pybind")
+
+
+@functools.lru_cache(maxsize=1)
+def fcp():
+    return _load_module("factor_corr_pybind")
+
+
+def device_count() -> int:
+    return int(lib().fcb_device_count())
+
+
+def status_string(rc: int) -> str:
+    return lib().fcb_status_string(int(rc)).decode()
+
+
+def check(rc: int, what: str) -> None:
+    """Map a C ABI status to the reference's exception classes."""
+    if rc == 0:
+        return
+    if rc < 0:
+        raise ValueError(f"{what}: contract error {rc} ({status_string(rc)})")
+    raise RuntimeError(f"{what}: error {rc} ({status_string(rc)})")
+
+
+def ptr(a) -> int | None:
+    """Raw data pointer of a numpy array or a torch tensor (None passes through)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return int(a.data_ptr())
+    return int(a.ctypes.data)

@@ -1,0 +1,150 @@
+/* fcb200.h -- C ABI of the B200-native cross-sectional analysis path.
+ *
+ * libfcb200.so exports plain C entry points (host pointers + sizes, no torch
+ * or pybind types).  Each replaces one native interface of factor-cuda
+ * (reference file:line given beside it) with the same argument meaning,
+ * preconditions and status codes, so the reference's pybind11 layer -- or the
+ * drop-in modules factor_cuda_pybind / factor_corr_pybind built on this ABI --
+ * can bind it directly.
+ *
+ * Status convention (reference src/factor_cuda_pybind.cpp:117-123):
+ *   0            success
+ *   negative     contract error (caller maps to ValueError)
+ *   positive     cudaError_t of the failing CUDA call (RuntimeError)
+ * FCB_ERR_DEVICE_WAIT (a positive code outside the cudaError_t range used by
+ * these calls) reports a bounded device-side wait that gave up.
+ *
+ * Host entry points are synchronous: inputs are uploaded, kernels run and
+ * results are downloaded before they return.  Host buffers may be pageable or
+ * pinned (fcb_host_alloc); pinned buffers make the copies faster.
+ * Every entry point is safe to call from any host thread; calls that share a
+ * workspace must be serialised by the caller (as in the reference).
+ */
+#ifndef FCB200_H_
+#define FCB200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FCB_DTYPE_F32 0
+#define FCB_DTYPE_F64 1
+
+#define FCB_OK 0
+#define FCB_ERR_ARG (-1)      /* null pointer or a dimension < 1            */
+#define FCB_ERR_CAP2 (-2)     /* op-specific cap, see each entry point      */
+#define FCB_ERR_CAP3 (-3)     /* op-specific cap, see each entry point      */
+#define FCB_ERR_CAP4 (-4)     /* op-specific (domain / min_valid)           */
+#define FCB_ERR_UNSUPPORTED (-5) /* valid request this build cannot serve   */
+#define FCB_ERR_DEVICE_WAIT 100000 /* bounded device wait gave up           */
+
+/* parameter_scan group status (reference src/parameter_scan.cuh:35-71) */
+#define FCB_GROUP_NOT_EXECUTED (-100)
+
+/* Opaque cached-device-buffer workspace (reference cs_rank_workspace,
+ * src/cross_sectional_rank.cuh:38-58, and rolling_ic_workspace,
+ * src/rolling_ic.cuh:33-67).  Buffers grow on demand and are reused across
+ * calls; they are bound to the device current at allocation time and
+ * re-allocated on a device change.  Not thread-safe. */
+typedef struct fcb_workspace fcb_workspace;
+
+fcb_workspace* fcb_workspace_create(void);
+/* Release all device buffers (idempotent); the handle stays usable.
+ * Replaces cs_rank_workspace_clear (src/cross_sectional_rank.cuh:67). */
+void fcb_workspace_clear(fcb_workspace* ws);
+void fcb_workspace_destroy(fcb_workspace* ws);
+/* Allocation accounting: live and high-water device bytes held by the
+ * workspace (replaces MemTracker live/peak, src/mem_tracker.h:35-77). */
+int fcb_workspace_stats(const fcb_workspace* ws, uint64_t* live_bytes, uint64_t* peak_bytes,
+                        uint64_t* n_allocs);
+
+/* Library / device helpers. */
+int fcb_version(void);
+int fcb_device_count(void);
+const char* fcb_status_string(int status);
+/* Pinned host memory for fast transfers (cudaHostAlloc / cudaFreeHost). */
+void* fcb_host_alloc(size_t bytes);
+void fcb_host_free(void* p);
+
+/* ---------------------------------------------------------------- rank ---
+ * Stable ordinal cross-sectional rank of a (T,N) f32 panel.  Valid cell =
+ * finite && mask; ranks 1..K by ascending value (descending: of -x), ties by
+ * column; invalid cells get the quiet NaN 0x7fc00000.
+ * Replaces cs_rank_gpu (src/cross_sectional_rank.cuh:90-99).
+ * Returns -1 null/dim, -2 N > 2^24, -3 T*N > INT32_MAX. */
+int fcb_cs_rank_f32(const float* x, const uint8_t* mask, int T, int N, int descending, float* out,
+                    fcb_workspace* ws);
+
+/* G=4 parameter scan: out[g] for g = asc-masked, asc-unmasked, desc-masked,
+ * desc-unmasked (NULL allowed for inactive groups).  active[4] (NULL = all)
+ * selects groups; group_status[g] = 0 ok, -100 not executed, or the
+ * whitelisted cudaError_t (9 / 701) of a failed launch.  time_ms / time_gpu_ms
+ * (NULL = off) receive per-group host / device time; the four groups are
+ * produced by one fused pass whose time is split evenly over the active
+ * groups.  Replaces parameter_scan_gpu (src/parameter_scan.cuh:82-90). */
+int fcb_parameter_scan_f32(const float* x, const uint8_t* mask, int T, int N, float* const out[4],
+                           int group_status[4], double time_ms[4], float time_gpu_ms[4],
+                           const int active[4], fcb_workspace* ws);
+
+/* ----------------------------------------------------------- rolling_ic ---
+ * Daily Spearman IC between factor f and forward returns r, (T,) f64.
+ * Joint valid set = finite(f) & finite(r) & fmask & rmask; fewer than
+ * min_valid joint cells, or a constant side on the joint set -> NaN.  f and r
+ * are f32 or f64 (FCB_DTYPE_*) and are ranked at that dtype.  rank_f/rank_r
+ * (NULL = off) receive the (T,N) joint-set ranks as f64, 0 elsewhere.
+ * Replaces rolling_ic_gpu (src/rolling_ic.cuh:102-108).
+ * Returns -1 null/dim, -3 T*N > INT32_MAX, -4 min_valid < 2. */
+int fcb_rolling_ic(const void* f, int f_dtype, const void* r, int r_dtype, const uint8_t* fmask,
+                   const uint8_t* rmask, int T, int N, int min_valid, double* ic, double* rank_f,
+                   double* rank_r, fcb_workspace* ws);
+
+/* ---------------------------------------------------------- correlation ---
+ * (F,F) pooled pairwise-complete Pearson of a (T,N,F) panel over (t,i) rows,
+ * mask (T,N) broadcast to every factor.  x is f32 or f64.  fallback_out
+ * (NULL = off) receives F*F bytes, 1 where the pair was recomputed by the
+ * two-pass compensated fallback.
+ * Replaces factor_corr_gpu (src/factor_corr.cuh:46-49).
+ * Returns -1 null/dim, -2 T*N > INT32_MAX, -3 F > 128. */
+int fcb_factor_corr(const void* x, int dtype, const uint8_t* mask, int T, int N, int F, double* out,
+                    uint8_t* fallback_out);
+
+/* (N,N) pairwise-complete Pearson of a (T,N) panel over t.  selected_path
+ * (NULL = off): 0 fully valid panel, 1 masked panel; fallback_count: pairs
+ * recomputed by the two-pass fallback.
+ * Replaces stock_corr_gpu (src/stock_corr.cuh:66-68).
+ * Returns -1 null/dim, -2 T*N > INT32_MAX, -3 N*N > INT32_MAX,
+ * -4 domain (max|x| > 1e150 or a nonzero |x| < 1e-150 on a valid cell). */
+int fcb_stock_corr(const void* x, int dtype, const uint8_t* mask, int T, int N, double* out,
+                   int* selected_path, int* fallback_count);
+
+/* ------------------------------------------------------- batched panels ---
+ * Rank + IC over F factor panels sharing one forward-return panel (the
+ * reference pipeline's cs_rank -> rolling_ic stages, benchmarks/poc4_e2e_v1.py
+ * :80-101, fused).  x (F,T,N) f32, r (T,N) f32, fmask / rmask (T,N) or NULL.
+ * ranks (F,T,N) f32 (NULL = off) = cs_rank of each factor under fmask;
+ * ic (F,T) f64 = rolling_ic(factor, r, fmask, rmask, min_valid).
+ * method: 0 plain radix, 1 learned splitters (falls back to radix per date).
+ * Host pointers; the panel is streamed through the device in date chunks
+ * with copies overlapping the kernels.  No reference counterpart as one call. */
+int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* fmask, const uint8_t* rmask, int F,
+                      int T, int N, int min_valid, float* ranks, double* ic, int method,
+                      fcb_workspace* ws);
+
+/* Device-pointer variant (all pointers device-resident, stream = cudaStream_t
+ * or NULL for the legacy stream).  Asynchronous; no host synchronisation. */
+int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const uint8_t* d_fmask, const uint8_t* d_rmask,
+                          int F, int T, int N, int min_valid, float* d_ranks, double* d_ic, int method,
+                          void* stream);
+
+/* Device-pointer cs_rank (asynchronous on `stream`). */
+int fcb_dev_cs_rank_f32(const float* d_x, const uint8_t* d_mask, int T, int N, int descending, float* d_out,
+                        void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FCB200_H_ */
