@@ -216,6 +216,13 @@ def run_b200(args, rank, world):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev.index) as clk:
+        # keep the GPU loaded for ~1 s before the timed region so that the
+        # 200 ms clock samples bracket it (extra untimed warm-up steps)
+        t_pre = time.perf_counter()
+        while time.perf_counter() - t_pre < 1.0:
+            for _ in range(5):
+                step()
+            torch.cuda.synchronize(dev)
         e0.record(stream)
         for _ in range(args.steps):
             step()
