@@ -157,6 +157,7 @@ extern "C" const char* fcb_status_string(int s) {
     case FCB_ERR_CAP3: return "size cap exceeded (-3)";
     case FCB_ERR_CAP4: return "domain / min_valid contract violated (-4)";
     case FCB_ERR_UNSUPPORTED: return "request not supported by this build";
+    case FCB_ERR_NOALLOC_CAP: return "F above the no-allocation entry point's maximum (FCB_NOALLOC_MAX_F)";
     case FCB_ERR_DEVICE_WAIT: return "a bounded device-side wait gave up";
     default: return s > 0 ? cudaGetErrorString(static_cast<cudaError_t>(s)) : "contract error";
   }

@@ -49,6 +49,7 @@ PROTOTYPES = {
     "fcb_rank_ic_panel": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i, _p]),
     "fcb_dev_rank_ic_panel": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i, _p]),
     "fcb_dev_cs_rank_f32": (_i, [_p, _p, _i, _i, _i, _p, _p]),
+    "fcb_dev_factor_corr_noalloc": (_i, [_p, _i, _p, _i, _i, _i, _p, _p]),
 }
 
 

@@ -39,6 +39,7 @@ extern "C" {
 #define FCB_ERR_CAP3 (-3)     /* op-specific cap, see each entry point      */
 #define FCB_ERR_CAP4 (-4)     /* op-specific (domain / min_valid)           */
 #define FCB_ERR_UNSUPPORTED (-5) /* valid request this build cannot serve   */
+#define FCB_ERR_NOALLOC_CAP (-6) /* size above a no-allocation entry's maximum */
 #define FCB_ERR_DEVICE_WAIT 100000 /* bounded device wait gave up           */
 
 /* parameter_scan group status (reference src/parameter_scan.cuh:35-71) */
@@ -142,6 +143,27 @@ int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const uint8_t* d_f
 /* Device-pointer cs_rank (asynchronous on `stream`). */
 int fcb_dev_cs_rank_f32(const float* d_x, const uint8_t* d_mask, int T, int N, int descending, float* d_out,
                         void* stream);
+
+/* ------------------------------------------------ no-allocation variant ---
+ * No counterpart in the reference.  factor_corr for callers that cannot let a
+ * library allocate device memory: applications whose device memory belongs to
+ * a framework pool or a hard budget, and latency-sensitive loops that cannot
+ * take the device-wide synchronisation of cudaMalloc/cudaFree.  Same kernels
+ * and results (within 1e-12) as fcb_factor_corr, on caller-owned DEVICE
+ * buffers: d_x (T,N,F) f32/f64, d_mask (T,N) or NULL, d_out (F,F) f64;
+ * asynchronous on `stream` (NULL = legacy stream).
+ * All scratch lives in one fixed device array of about 2.6 MB inside the
+ * library, which every GPU that loads the library holds until exit; no
+ * cudaMalloc/cudaFree or allocating library routine is called.  F is limited
+ * to FCB_NOALLOC_MAX_F (larger F returns FCB_ERR_NOALLOC_CAP).  The first
+ * call on each device resolves the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  Every call shares the one array: calls that
+ * overlap on the GPU (concurrent streams or threads) race and must be
+ * serialised by the caller. */
+#define FCB_NOALLOC_MAX_F 32
+int fcb_dev_factor_corr_noalloc(const void* d_x, int dtype, const uint8_t* d_mask, int T, int N, int F,
+                                double* d_out, void* stream);
 
 #ifdef __cplusplus
 }
