@@ -201,10 +201,37 @@ def run_b200(args, rank, world):
     dic = torch.empty((F, T), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    def step():
+    def radix_step():
         rc = lib.fcb_dev_rank_ic_panel(dX.data_ptr(), dR.data_ptr(), dfm.data_ptr(), drm.data_ptr(), F, T, N,
-                                       MIN_VALID, dranks.data_ptr(), dic.data_ptr(), method, stream.cuda_stream)
+                                       MIN_VALID, dranks.data_ptr(), dic.data_ptr(), 0, stream.cuda_stream)
         nat.check(rc, "fcb_dev_rank_ic_panel")
+
+    learn = None
+    if method == 1:
+        import fcb200
+        # exact radix ranks of the earlier dates are the training labels
+        radix_step()
+        torch.cuda.synchronize(dev)
+        model = fcb200.CdfModel(F, seed=20261203)
+        tfit = min(T, 250)
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        model.fit(dX, dranks, T, N, 0, tfit, steps=1500, lr=3e-3, stream=stream.cuda_stream)
+        f1.record(stream)
+        torch.cuda.synchronize(dev)
+        dstats = torch.zeros((F, T, 4), dtype=torch.int32, device=dev)
+        learn = {"model": model, "fit_ms": f0.elapsed_time(f1), "train_dates": tfit, "stats": dstats}
+
+    def step():
+        if learn is None:
+            radix_step()
+            return
+        rc = lib.fcb_dev_rank_ic_panel_learned(dX.data_ptr(), dR.data_ptr(), dfm.data_ptr(), drm.data_ptr(), F, T,
+                                               N, MIN_VALID, dranks.data_ptr(), dic.data_ptr(),
+                                               learn["model"].handle, 64, learn["stats"].data_ptr(),
+                                               stream.cuda_stream)
+        nat.check(rc, "fcb_dev_rank_ic_panel_learned")
 
     for _ in range(args.warmup):
         step()
@@ -231,10 +258,37 @@ def run_b200(args, rank, world):
     ms = e0.elapsed_time(e1) / args.steps
     # parity spot check of the timed outputs against the oracle (a few dates)
     spot = check_spot(X, R, fm, rm, dranks, dic)
+    learned_info = None
+    if learn is not None:
+        st = learn["stats"].cpu().numpy()
+        codes = st[..., 0]
+        # bit-exactness of the whole learned output against the radix path
+        lr_ranks = dranks.clone()
+        lr_ic = dic.clone()
+        radix_step()
+        torch.cuda.synchronize(dev)
+        exact = bool(torch.equal(lr_ranks.view(torch.int32), dranks.view(torch.int32))) and \
+            bool(torch.equal(torch.nan_to_num(lr_ic, nan=7.0), torch.nan_to_num(dic, nan=7.0)))
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(args.steps):
+            radix_step()
+        e3.record(stream)
+        torch.cuda.synchronize(dev)
+        radix_ms = e2.elapsed_time(e3) / args.steps
+        learned_info = {"fit_ms": learn["fit_ms"], "train_dates": learn["train_dates"],
+                        "learned_fraction": float((codes == 1).mean()),
+                        "fallback_overflow": float((codes == 2).mean()),
+                        "fallback_judge": float((codes == 3).mean()),
+                        "fallback_scale": float((codes == 4).mean()),
+                        "mean_max_bucket": float(st[..., 1][codes == 1].mean()) if (codes == 1).any() else None,
+                        "bit_exact_vs_radix": exact, "radix_ms_per_step": radix_ms,
+                        "speedup_vs_radix": radix_ms / ms}
 
     # e2e: host entry point, pinned buffers, copies in the timed region
     if args.no_e2e:
-        return finish(args, world, X, R, fm, rm, ms, None, None, clk, spot, dev)
+        return finish(args, world, X, R, fm, rm, ms, None, None, clk, spot, dev, learned_info)
     hX = torch.from_numpy(X).pin_memory()
     hR = torch.from_numpy(R).pin_memory()
     hfm = torch.from_numpy(fm).pin_memory()
@@ -250,6 +304,15 @@ def run_b200(args, rank, world):
 
     for _ in range(max(1, args.warmup)):
         host_step()
+    if method == 1:
+        # let the workspace's background fit land before timing (bounded)
+        import ctypes as C
+        rdy, fits, lch = C.c_int(), C.c_int(), C.c_int()
+        for _ in range(5):
+            lib.fcb_workspace_learned_state(ws, C.byref(rdy), C.byref(fits), C.byref(lch))
+            if rdy.value:
+                break
+            host_step()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -259,10 +322,10 @@ def run_b200(args, rank, world):
     e2e_s = (time.perf_counter() - t0) / args.steps
     lib.fcb_workspace_destroy(ws)
     e2e_ok = bool(np.array_equal(hranks.numpy().view(np.uint32), dranks.cpu().numpy().view(np.uint32)))
-    return finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev)
+    return finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info)
 
 
-def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev):
+def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info=None):
     import torch
     F, T, N = X.shape
     ms_all, e2e_all = ms, (e2e_s if e2e_s is not None else 0.0)
@@ -296,6 +359,8 @@ def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev):
         "clocks": clk.summary(),
         "parity_spot_check": spot,
     }
+    if learned_info is not None:
+        res["learned"] = learned_info
     return res
 
 

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/fcb200.h"
+#include "cdf_model.h"
 #include "fcb_kernels.h"
 
 using namespace fcb;
@@ -25,17 +26,30 @@ enum Slot : int {
   S_X = 0, S_X2, S_MASK, S_MASK2, S_OUT, S_OUT1, S_OUT2, S_OUT3, S_STATUS, S_IC, S_RF, S_RR,
   S_SC_RAW, S_SC_C, S_SC_M, S_SC_ST, S_SC_SUM, S_FB_LIST, S_FB_CNT,
   S_FC_COLPART, S_FC_COLSTAT, S_FC_GRAM, S_FC_FLAGS,
-  // streamed panel: two chunk buffers each
-  S_PX0, S_PX1, S_PR0, S_PR1, S_PFM0, S_PFM1, S_PRM0, S_PRM1, S_PRK0, S_PRK1, S_PIC0, S_PIC1,
+  // streamed panel: three chunk buffers each (upload / compute / download in flight)
+  S_PX0, S_PX1, S_PX2, S_PR0, S_PR1, S_PR2, S_PFM0, S_PFM1, S_PFM2, S_PRM0, S_PRM1, S_PRM2,
+  S_PRK0, S_PRK1, S_PRK2, S_PIC0, S_PIC1, S_PIC2,
   S_COUNT
 };
 
+// Streams: 0 compute (and every single-shot entry point), 1 uploads,
+// 2 downloads, 3 background model refits.
 struct fcb_workspace {
+  static constexpr int kStreams = 4;
   int device = -1;
-  cudaStream_t stream[2] = {nullptr, nullptr};
+  cudaStream_t stream[kStreams] = {};
   void* ptr[S_COUNT] = {};
   size_t cap[S_COUNT] = {};
   uint64_t live = 0, peak = 0, nalloc = 0;
+  // learned-splitter state carried across calls
+  fcb_cdf_model* model = nullptr;
+  bool model_ready = false;   // model->table[model->cur] holds a fitted table
+  bool fit_inflight = false;  // a refit runs on stream 3
+  int fit_slot = 0;           // table slot the in-flight refit writes
+  int since_fit = 0;          // dates ranked since the last refit was scheduled
+  int fits = 0;               // refits scheduled
+  int learned_chunks = 0;     // chunks ranked by the learned kernel
+  cudaEvent_t ev_fit = nullptr;
 
   cudaError_t bind() {
     int dev = 0;
@@ -45,7 +59,7 @@ struct fcb_workspace {
       release();
       device = dev;
     }
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < kStreams; ++i)
       if (stream[i] == nullptr) {
         e = cudaStreamCreateWithFlags(&stream[i], cudaStreamNonBlocking);
         if (e != cudaSuccess) return e;
@@ -75,13 +89,32 @@ struct fcb_workspace {
     *out = static_cast<T*>(ptr[s]);
     return cudaSuccess;
   }
+  // Poll the background refit; when it has finished, the rank kernels switch
+  // to the freshly written table slot.
+  void poll_fit() {
+    if (fit_inflight && cudaEventQuery(ev_fit) == cudaSuccess) {
+      model->cur = fit_slot;
+      model_ready = true;
+      fit_inflight = false;
+    }
+  }
+  void drop_model() {
+    if (stream[3] != nullptr) cudaStreamSynchronize(stream[3]);
+    if (model != nullptr) fcb_cdf_model_destroy(model);
+    model = nullptr;
+    model_ready = fit_inflight = false;
+    since_fit = 0;
+  }
   void release() {
+    drop_model();
+    if (ev_fit != nullptr) cudaEventDestroy(ev_fit);
+    ev_fit = nullptr;
     for (int s = 0; s < S_COUNT; ++s) {
       if (ptr[s] != nullptr) cudaFree(ptr[s]);
       ptr[s] = nullptr;
       cap[s] = 0;
     }
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kStreams; ++i) {
       if (stream[i] != nullptr) cudaStreamDestroy(stream[i]);
       stream[i] = nullptr;
     }
@@ -138,6 +171,14 @@ extern "C" int fcb_workspace_stats(const fcb_workspace* ws, uint64_t* live, uint
   if (live) *live = ws->live;
   if (peak) *peak = ws->peak;
   if (n) *n = ws->nalloc;
+  return FCB_OK;
+}
+
+extern "C" int fcb_workspace_learned_state(const fcb_workspace* ws, int* ready, int* fits, int* learned_chunks) {
+  if (ws == nullptr) return FCB_ERR_ARG;
+  if (ready) *ready = ws->model_ready ? 1 : 0;
+  if (fits) *fits = ws->fits;
+  if (learned_chunks) *learned_chunks = ws->learned_chunks;
   return FCB_OK;
 }
 
@@ -385,7 +426,7 @@ static int panel_args_check(const void* x, const void* r, const double* ic, int 
   if (min_valid < 2) return FCB_ERR_CAP4;
   if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
   if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
-  if (method != 0) return FCB_ERR_UNSUPPORTED;
+  if (method != 0 && method != 1) return FCB_ERR_ARG;
   return FCB_OK;
 }
 
@@ -394,6 +435,7 @@ extern "C" int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const u
                                      double* d_ic, int method, void* stream) {
   const int chk = panel_args_check(d_x, d_r, d_ic, F, T, N, min_valid, method);
   if (chk != FCB_OK) return chk;
+  if (method != 0) return FCB_ERR_UNSUPPORTED;  // learned: fcb_dev_rank_ic_panel_learned (needs a model)
   static int* d_status = nullptr;
   static std::mutex mu;
   {
@@ -404,8 +446,17 @@ extern "C" int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const u
   return rc(launch_rank_ic<float, float>(a, d_status, static_cast<cudaStream_t>(stream)));
 }
 
-// Host panel: dates are streamed in chunks over two streams so that the
-// upload of chunk k+1 and the download of chunk k-1 overlap the kernel on k.
+// Host panel: dates are streamed in chunks through three buffer sets so that
+// the upload of chunk k+1, the kernel on chunk k and the download of chunk k-1
+// run concurrently (stream 1 uploads, stream 0 computes, stream 2 downloads,
+// ordered by events).
+// method 1 (learned splitters): the workspace keeps a CDF model across calls.
+// Until a fitted table exists, chunks are ranked by radix; after each chunk
+// whose date count since the last refit reaches 250 (and after the first
+// chunk of a fresh workspace), training samples are taken from that chunk's
+// exact ranks on the compute stream and the refit (Adam + tabulation into the
+// idle table slot) runs on stream 3 while ranking continues with the current
+// slot; the host switches slots once the refit's event has completed.
 extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* fmask, const uint8_t* rmask,
                                  int F, int T, int N, int min_valid, float* ranks, double* ic, int method,
                                  fcb_workspace* wsp) {
@@ -414,56 +465,120 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
   WsScope sc(wsp);
   fcb_workspace& ws = *sc.ws;
   FCB_TRY(ws.bind());
-  // chunk: about 32 MB of factor input per chunk, at least one date
+  constexpr int NB = 3;
+  constexpr int kRefreshDates = 250;
+  // chunk: about 24 MB of factor input per chunk, at least one date
   const size_t per_date = static_cast<size_t>(F) * N * 4;
-  int Tc = static_cast<int>((32ull << 20) / (per_date > 0 ? per_date : 1));
+  int Tc = static_cast<int>((24ull << 20) / (per_date > 0 ? per_date : 1));
   if (Tc < 1) Tc = 1;
   if (Tc > T) Tc = T;
   const int nchunk = (T + Tc - 1) / Tc;
-  float* dx[2];
-  float* dr[2];
-  uint8_t* dfm[2] = {nullptr, nullptr};
-  uint8_t* drm[2] = {nullptr, nullptr};
-  float* drk[2] = {nullptr, nullptr};
-  double* dic[2];
+  const bool learned = (method == 1);
+  const bool need_ranks = ranks != nullptr || learned;
+  float* dx[NB];
+  float* dr[NB];
+  uint8_t* dfm[NB] = {};
+  uint8_t* drm[NB] = {};
+  float* drk[NB] = {};
+  double* dic[NB];
   int* dst;
   const size_t cn = static_cast<size_t>(Tc) * N;
   FCB_TRY(ws.get(S_STATUS, 64, &dst));
-  for (int b = 0; b < 2; ++b) {
+  for (int b = 0; b < NB; ++b) {
     FCB_TRY(ws.get(static_cast<Slot>(S_PX0 + b), cn * F * 4, &dx[b]));
     FCB_TRY(ws.get(static_cast<Slot>(S_PR0 + b), cn * 4, &dr[b]));
     FCB_TRY(ws.get(static_cast<Slot>(S_PIC0 + b), static_cast<size_t>(F) * Tc * 8, &dic[b]));
     if (fmask) FCB_TRY(ws.get(static_cast<Slot>(S_PFM0 + b), cn, &dfm[b]));
     if (rmask) FCB_TRY(ws.get(static_cast<Slot>(S_PRM0 + b), cn, &drm[b]));
-    if (ranks) FCB_TRY(ws.get(static_cast<Slot>(S_PRK0 + b), cn * F * 4, &drk[b]));
+    if (need_ranks) FCB_TRY(ws.get(static_cast<Slot>(S_PRK0 + b), cn * F * 4, &drk[b]));
   }
-  FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), ws.stream[0]));
-  FCB_TRY(cudaStreamSynchronize(ws.stream[0]));
+  cudaEvent_t ev_in[NB] = {}, ev_comp[NB] = {}, ev_out[NB] = {}, ev_feat = nullptr;
+  struct Events {
+    cudaEvent_t* a;
+    cudaEvent_t* b;
+    cudaEvent_t* c;
+    cudaEvent_t& f;
+    ~Events() {
+      for (int i = 0; i < NB; ++i) {
+        if (a[i]) cudaEventDestroy(a[i]);
+        if (b[i]) cudaEventDestroy(b[i]);
+        if (c[i]) cudaEventDestroy(c[i]);
+      }
+      if (f) cudaEventDestroy(f);
+    }
+  } evguard{ev_in, ev_comp, ev_out, ev_feat};
+  for (int i = 0; i < NB; ++i) {
+    FCB_TRY(cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming));
+    FCB_TRY(cudaEventCreateWithFlags(&ev_comp[i], cudaEventDisableTiming));
+    FCB_TRY(cudaEventCreateWithFlags(&ev_out[i], cudaEventDisableTiming));
+  }
+  if (learned) {
+    if (ws.model != nullptr && ws.model->F != F) ws.drop_model();
+    if (ws.model == nullptr) {
+      ws.model = fcb_cdf_model_create(F, 20261203ull);
+      if (ws.model == nullptr) return rc(cudaErrorMemoryAllocation);
+    }
+    if (ws.ev_fit == nullptr) FCB_TRY(cudaEventCreateWithFlags(&ws.ev_fit, cudaEventDisableTiming));
+    FCB_TRY(cudaEventCreateWithFlags(&ev_feat, cudaEventDisableTiming));
+  }
+  cudaStream_t s_c = ws.stream[0], s_in = ws.stream[1], s_out = ws.stream[2], s_fit = ws.stream[3];
+  FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), s_c));
   for (int c = 0; c < nchunk; ++c) {
-    const int b = c & 1;
-    cudaStream_t s = ws.stream[b];
+    const int j = c % NB;
     const int t0 = c * Tc;
     const int tc = (t0 + Tc <= T) ? Tc : (T - t0);
     const size_t cnn = static_cast<size_t>(tc) * N;
+    if (c >= NB) FCB_TRY(cudaStreamWaitEvent(s_in, ev_out[j], 0));  // buffer set j drained
     for (int f = 0; f < F; ++f)
-      FCB_TRY(cudaMemcpyAsync(dx[b] + static_cast<size_t>(f) * tc * N,
-                              x + (static_cast<size_t>(f) * T + t0) * N, cnn * 4, cudaMemcpyHostToDevice, s));
-    FCB_TRY(cudaMemcpyAsync(dr[b], r + static_cast<size_t>(t0) * N, cnn * 4, cudaMemcpyHostToDevice, s));
-    if (fmask) FCB_TRY(cudaMemcpyAsync(dfm[b], fmask + static_cast<size_t>(t0) * N, cnn, cudaMemcpyHostToDevice, s));
-    if (rmask) FCB_TRY(cudaMemcpyAsync(drm[b], rmask + static_cast<size_t>(t0) * N, cnn, cudaMemcpyHostToDevice, s));
-    RankIcArgs<float, float> a{dx[b], dr[b], dfm[b], drm[b], F, tc, N, min_valid, drk[b], dic[b], nullptr, nullptr};
-    FCB_TRY(launch_rank_ic<float, float>(a, dst, s));
-    for (int f = 0; f < F; ++f) {
-      FCB_TRY(cudaMemcpyAsync(ic + static_cast<size_t>(f) * T + t0, dic[b] + static_cast<size_t>(f) * tc,
-                              static_cast<size_t>(tc) * 8, cudaMemcpyDeviceToHost, s));
-      if (ranks)
-        FCB_TRY(cudaMemcpyAsync(ranks + (static_cast<size_t>(f) * T + t0) * N, drk[b] + static_cast<size_t>(f) * tc * N,
-                                cnn * 4, cudaMemcpyDeviceToHost, s));
+      FCB_TRY(cudaMemcpyAsync(dx[j] + static_cast<size_t>(f) * tc * N, x + (static_cast<size_t>(f) * T + t0) * N,
+                              cnn * 4, cudaMemcpyHostToDevice, s_in));
+    FCB_TRY(cudaMemcpyAsync(dr[j], r + static_cast<size_t>(t0) * N, cnn * 4, cudaMemcpyHostToDevice, s_in));
+    if (fmask) FCB_TRY(cudaMemcpyAsync(dfm[j], fmask + static_cast<size_t>(t0) * N, cnn, cudaMemcpyHostToDevice, s_in));
+    if (rmask) FCB_TRY(cudaMemcpyAsync(drm[j], rmask + static_cast<size_t>(t0) * N, cnn, cudaMemcpyHostToDevice, s_in));
+    FCB_TRY(cudaEventRecord(ev_in[j], s_in));
+    FCB_TRY(cudaStreamWaitEvent(s_c, ev_in[j], 0));
+    if (learned) ws.poll_fit();
+    if (learned && ws.model_ready) {
+      const int e = fcb_dev_rank_ic_panel_learned(dx[j], dr[j], dfm[j], drm[j], F, tc, N, min_valid, drk[j], dic[j],
+                                                  ws.model, 0, nullptr, s_c);
+      if (e != 0) return e;
+      ++ws.learned_chunks;
+    } else {
+      RankIcArgs<float, float> a{dx[j], dr[j], dfm[j], drm[j], F, tc, N, min_valid, drk[j], dic[j], nullptr, nullptr};
+      FCB_TRY(launch_rank_ic<float, float>(a, dst, s_c));
     }
+    if (learned) {
+      ws.since_fit += tc;
+      if (!ws.fit_inflight && (!ws.model_ready || ws.since_fit >= kRefreshDates)) {
+        FCB_TRY(fcb::cdf_model_features(ws.model, dx[j], drk[j], tc, N, 0, tc, s_c));
+        FCB_TRY(cudaEventRecord(ev_feat, s_c));
+        FCB_TRY(cudaStreamWaitEvent(s_fit, ev_feat, 0));
+        ws.fit_slot = ws.model_ready ? (ws.model->cur ^ 1) : ws.model->cur;
+        FCB_TRY(fcb::cdf_model_train_tabulate(ws.model, ws.model_ready ? 100 : 1500, ws.model_ready ? 1e-3f : 3e-3f,
+                                              ws.fit_slot, s_fit));
+        FCB_TRY(cudaEventRecord(ws.ev_fit, s_fit));
+        ws.fit_inflight = true;
+        ws.since_fit = 0;
+        ++ws.fits;
+      }
+    }
+    FCB_TRY(cudaEventRecord(ev_comp[j], s_c));
+    FCB_TRY(cudaStreamWaitEvent(s_out, ev_comp[j], 0));
+    for (int f = 0; f < F; ++f) {
+      FCB_TRY(cudaMemcpyAsync(ic + static_cast<size_t>(f) * T + t0, dic[j] + static_cast<size_t>(f) * tc,
+                              static_cast<size_t>(tc) * 8, cudaMemcpyDeviceToHost, s_out));
+      if (ranks)
+        FCB_TRY(cudaMemcpyAsync(ranks + (static_cast<size_t>(f) * T + t0) * N, drk[j] + static_cast<size_t>(f) * tc * N,
+                                cnn * 4, cudaMemcpyDeviceToHost, s_out));
+    }
+    FCB_TRY(cudaEventRecord(ev_out[j], s_out));
   }
   int hst = 0;
-  FCB_TRY(cudaStreamSynchronize(ws.stream[0]));
-  FCB_TRY(cudaStreamSynchronize(ws.stream[1]));
+  FCB_TRY(cudaStreamSynchronize(s_in));
+  FCB_TRY(cudaStreamSynchronize(s_c));
+  FCB_TRY(cudaStreamSynchronize(s_out));
+  if (learned) ws.poll_fit();
+  if (&ws == &sc.tmp) ws.drop_model();  // a temporary workspace waits for its refit
   FCB_TRY(cudaMemcpy(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost));
   return check_status(&hst);
 }

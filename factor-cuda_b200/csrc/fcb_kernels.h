@@ -11,6 +11,10 @@ namespace fcb {
 // Largest cross-section the shared-memory rank kernels take (u16 column ids,
 // 1024 threads x 16 items).  Larger N goes through the global-memory path.
 constexpr int kSmemRankCap = 16384;
+// CDF network for learned splitters: hidden width, parameter count, table knots.
+constexpr int kCdfHidden = 32;
+constexpr int kCdfParams = 1 + 1 * 32 + 32 + 32 * 32 + 32 + 32;  // W1,b1,W2,b2,w3,b3 = 1153
+constexpr int kCdfKnots = 1024;
 constexpr size_t kMaxSmemPerBlock = 227 * 1024;
 
 struct ScanOut {
@@ -28,6 +32,11 @@ struct RankIcArgs {
   double* ic_out;           // (F,T)
   double* rank_f_out;       // (F,T,N) joint-set ranks, 0 elsewhere, or nullptr
   double* rank_r_out;       // (F,T,N) joint-set ranks of the returns, or nullptr
+  // learned splitters (used by the LEARNED instantiation only)
+  const float* cdf_table;   // (F, kCdfKnots) tabulated monotone CDF per factor
+  const float* cdf_zrange;  // (F, 2) grid range [lo, hi] in standardised units
+  int learn_cap;            // largest bucket the learned path accepts
+  int* learn_stats;         // (F,T,4): outcome, largest bucket, sum of squared bucket sizes, m; or nullptr
 };
 
 struct ColStat {  // one stock_corr column
@@ -58,6 +67,18 @@ template <typename TF, typename TR>
 size_t rank_ic_smem(int N);
 template <typename TF, typename TR>
 cudaError_t launch_rank_ic(const RankIcArgs<TF, TR>& a, int* status, cudaStream_t st);
+cudaError_t launch_rank_ic_learned(const RankIcArgs<float, float>& a, int* status, cudaStream_t st);
+
+// cdf_mlp.cu
+size_t cdf_train_smem();
+cudaError_t launch_cdf_features(const float* X, const float* ranks, int F, int T, int N, int t0, int tcount, int S,
+                                float2* samples, cudaStream_t s);
+cudaError_t launch_cdf_train(float* params, float* adam, const float2* samples, int F, int nsamp, int steps, float lr,
+                             int step0, float* loss_out, cudaStream_t s);
+cudaError_t launch_cdf_grad(const float* params, const float* z, const float* u, int n, float* grad, float* loss,
+                            cudaStream_t s);
+cudaError_t launch_cdf_tabulate(const float* params, const float2* samples, int F, int nsamp, float* zrange,
+                                float* table, bool linear, cudaStream_t s);
 
 // corr_kernels.cu
 cudaError_t launch_stock_corr_prep(const void* X, int dtype, const uint8_t* mask, int T, int N, int Tp,

@@ -19,6 +19,7 @@
 //                 (fc/_cpu_core.py:271-293).
 #include "block_sort.cuh"
 #include "fcb_kernels.h"
+#include "learned_sort.cuh"
 
 namespace fcb {
 
@@ -292,7 +293,7 @@ struct RankIcLayout {
     flags = o; o = align16(o + size_t(n) + 16);
     ir = o; o = align16(o + size_t(n) * 2);
     gr = o; o = align16(o + size_t(n) * 2);
-    rr = o; o = align16(o + size_t(n) * 2);
+    rr = o; o = align16(o + size_t(n) * 2 + 16);
     total = o;
   }
 };
@@ -306,7 +307,7 @@ FCB_DEV double spearman_from_sum(long long m, long long sum_rr) {
   return (sxy / sqrt(sxx)) / sqrt(sxx);
 }
 
-template <int NT, int MAXIPT, typename TF, typename TR>
+template <int NT, int MAXIPT, typename TF, typename TR, bool LEARNED>
 __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(RankIcArgs<TF, TR> a, int* status) {
   using KF = typename KeyOf<TF>::type;
   using KR = typename KeyOf<TR>::type;
@@ -384,9 +385,41 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(Ra
     const int mf = compact_keys<KF>(
         N, [&](int i) { return (flags[i] & 6u) == 6u; }, [&](int i) { return KeyOf<TF>::key(x[i]); }, kf0, i0,
         scan);
-    KF* kfs;
-    uint16_t* ifs;
-    block_radix_sort<NT, MAXIPT, KF>(kf0, i0, kf1, i1, mf, sm + L.scratch, &kfs, &ifs);
+    KF* kfs = kf0;
+    uint16_t* ifs = i0;
+    bool sorted = false;
+    if constexpr (LEARNED) {
+      // the radix histogram region is idle here: it holds this factor's table
+      float* tab = reinterpret_cast<float*>(sm + L.scratch);
+      for (int k = threadIdx.x; k < kCdfKnots; k += NT) tab[k] = a.cdf_table[static_cast<size_t>(f) * kCdfKnots + k];
+      __syncthreads();
+      int mb = 0, ss = 0;
+      const int st = learned_sort<NT>(reinterpret_cast<uint32_t*>(kf0), i0, reinterpret_cast<uint32_t*>(kf1), i1, mf,
+                                      RR, tab, a.cdf_zrange[2 * f], a.cdf_zrange[2 * f + 1], a.learn_cap,
+                                      reinterpret_cast<double*>(scan64), scan, &mb, &ss);
+      if (a.learn_stats != nullptr && threadIdx.x == 0) {
+        int* o = a.learn_stats + (static_cast<size_t>(f) * T + t) * 4;
+        o[0] = st;
+        o[1] = mb;
+        o[2] = ss;
+        o[3] = mf;
+      }
+      sorted = (st == kLearnOk);
+      if (st == kLearnJudge) {
+        // the buffers were permuted: rebuild the compacted input from the row
+        x = stage_issue(sm + L.k1, a.X + frow, N, &bars[3], arm[3]);
+        ok = stage_wait(&bars[3], ph[3], arm[3]);
+        if (__syncthreads_or(!ok)) {
+          if (threadIdx.x == 0) atomicExch(status, 1);
+          return;
+        }
+        (void)compact_keys<KF>(
+            N, [&](int i) { return (flags[i] & 6u) == 6u; }, [&](int i) { return KeyOf<TF>::key(x[i]); }, kf0, i0,
+            scan);
+      }
+      __syncthreads();
+    }
+    if (!sorted) block_radix_sort<NT, MAXIPT, KF>(kf0, i0, kf1, i1, mf, sm + L.scratch, &kfs, &ifs);
 
     // returns side: joint ranks in return order, first/last joint position
     int b, e;
@@ -519,15 +552,15 @@ template size_t rank_ic_smem<float, double>(int);
 template size_t rank_ic_smem<double, float>(int);
 template size_t rank_ic_smem<double, double>(int);
 
-template <int NT, typename TF, typename TR>
+template <int NT, typename TF, typename TR, bool LEARNED>
 static cudaError_t launch_rank_ic_nt(const RankIcArgs<TF, TR>& a, int* status, cudaStream_t st) {
   constexpr int KSZ = (sizeof(TF) > sizeof(TR)) ? int(sizeof(TF)) : int(sizeof(TR));
   const size_t smem = RankIcLayout(a.N, KSZ, SortScratch<NT>::bytes).total;
   if (smem > kMaxSmemPerBlock) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(k_rank_ic<NT, 16, TF, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = cudaFuncSetAttribute(k_rank_ic<NT, 16, TF, TR, LEARNED>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  k_rank_ic<NT, 16, TF, TR><<<a.T, NT, smem, st>>>(a, status);
+  k_rank_ic<NT, 16, TF, TR, LEARNED><<<a.T, NT, smem, st>>>(a, status);
   return cudaGetLastError();
 }
 
@@ -535,9 +568,18 @@ template <typename TF, typename TR>
 cudaError_t launch_rank_ic(const RankIcArgs<TF, TR>& a, int* status, cudaStream_t st) {
   if (a.N > kSmemRankCap) return cudaErrorInvalidValue;
   switch (pick_nt(a.N)) {
-    case 256: return launch_rank_ic_nt<256>(a, status, st);
-    case 512: return launch_rank_ic_nt<512>(a, status, st);
-    default: return launch_rank_ic_nt<1024>(a, status, st);
+    case 256: return launch_rank_ic_nt<256, TF, TR, false>(a, status, st);
+    case 512: return launch_rank_ic_nt<512, TF, TR, false>(a, status, st);
+    default: return launch_rank_ic_nt<1024, TF, TR, false>(a, status, st);
+  }
+}
+
+cudaError_t launch_rank_ic_learned(const RankIcArgs<float, float>& a, int* status, cudaStream_t st) {
+  if (a.N > kSmemRankCap || a.cdf_table == nullptr || a.cdf_zrange == nullptr) return cudaErrorInvalidValue;
+  switch (pick_nt(a.N)) {
+    case 256: return launch_rank_ic_nt<256, float, float, true>(a, status, st);
+    case 512: return launch_rank_ic_nt<512, float, float, true>(a, status, st);
+    default: return launch_rank_ic_nt<1024, float, float, true>(a, status, st);
   }
 }
 template cudaError_t launch_rank_ic<float, float>(const RankIcArgs<float, float>&, int*, cudaStream_t);

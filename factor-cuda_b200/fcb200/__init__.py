@@ -33,7 +33,7 @@ except Exception:  # pragma: no cover
 
 __version__ = "1.0.0"
 __all__ = ["cross_sectional_rank", "factor_plane", "factor_corr", "stock_corr", "rolling_ic",
-           "parameter_scan", "rank_ic_panel", "clear_workspaces", "__version__"]
+           "parameter_scan", "rank_ic_panel", "Workspace", "CdfModel", "clear_workspaces", "__version__"]
 
 _WHITELIST = (np.float32, np.float64)
 DOMAIN_MSG = ("correlation domain violation: max|x| > 1e150 or a nonzero |x| < 1e-150 "
@@ -392,8 +392,43 @@ def stock_corr(data, mask=None, backend="cuda"):
 # ---------------------------------------------------------------------------
 # extensions
 # ---------------------------------------------------------------------------
+class Workspace:
+    """Cached device buffers (and, for the learned method, the CDF model)
+    reused across ``rank_ic_panel`` calls.  Not thread-safe."""
+
+    def __init__(self):
+        self._h = nat.lib().fcb_workspace_create()
+        if not self._h:
+            raise MemoryError("fcb_workspace_create failed")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def learned_state(self):
+        import ctypes as C
+        r, f, lc = C.c_int(), C.c_int(), C.c_int()
+        nat.check(nat.lib().fcb_workspace_learned_state(self._h, C.byref(r), C.byref(f), C.byref(lc)),
+                  "fcb_workspace_learned_state")
+        return {"ready": bool(r.value), "fits": f.value, "learned_chunks": lc.value}
+
+    def clear(self):
+        nat.lib().fcb_workspace_clear(self._h)
+
+    def close(self):
+        if self._h:
+            nat.lib().fcb_workspace_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def rank_ic_panel(X, forward_returns, factor_mask=None, fwd_mask=None, min_valid=30,
-                  method="radix", return_ranks=True):
+                  method="radix", return_ranks=True, workspace=None):
     """cs_rank + rolling_ic of F factor panels X (F,T,N) f32 against one
     forward-return panel (T,N) f32, in one streamed call.  Returns
     ``(ranks (F,T,N) f32 | None, ic (F,T) f64)``; ranks follow
@@ -413,6 +448,73 @@ def rank_ic_panel(X, forward_returns, factor_mask=None, fwd_mask=None, min_valid
     ranks = np.empty((F, T, N), np.float32) if return_ranks else None
     ic = np.empty((F, T), np.float64)
     rc = nat.lib().fcb_rank_ic_panel(nat.ptr(X), nat.ptr(R), nat.ptr(fm), nat.ptr(rm), F, T, N, min_valid,
-                                     nat.ptr(ranks), nat.ptr(ic), meth, None)
+                                     nat.ptr(ranks), nat.ptr(ic), meth,
+                                     workspace.handle if workspace is not None else None)
     nat.check(rc, "rank_ic_panel")
     return ranks, ic
+
+
+class CdfModel:
+    """Learned-splitter CDF networks (one per factor) on the current device.
+
+    ``fit(d_x, d_ranks, t0, tcount)`` trains on dates [t0, t0+tcount) of
+    device-resident (F,T,N) f32 panels and their exact cs ranks (torch CUDA
+    tensors or raw device pointers); ``state()`` / ``load()`` save and restore
+    parameters, grid range and table (host numpy) for checkpoint / resume."""
+
+    def __init__(self, F, seed=20261203, linear=False):
+        self.F = int(F)
+        self._h = nat.lib().fcb_cdf_model_create(self.F, int(seed))
+        if not self._h:
+            raise RuntimeError("fcb_cdf_model_create failed (no CUDA device or out of memory)")
+        if linear:
+            nat.check(nat.lib().fcb_cdf_model_set_linear(self._h, 1), "fcb_cdf_model_set_linear")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def fit(self, d_x, d_ranks, T, N, t0, tcount, steps=1500, lr=3e-3, stream=None):
+        rc = nat.lib().fcb_cdf_model_fit(self._h, nat.ptr(d_x), nat.ptr(d_ranks), int(T), int(N), int(t0),
+                                         int(tcount), int(steps), float(lr), stream)
+        nat.check(rc, "fcb_cdf_model_fit")
+
+    def state(self):
+        P, K = 1153, 1024
+        params = np.empty((self.F, P), np.float32)
+        zr = np.empty((self.F, 2), np.float32)
+        tab = np.empty((self.F, K), np.float32)
+        loss = np.empty(self.F, np.float32)
+        nat.check(nat.lib().fcb_cdf_model_state(self._h, nat.ptr(params), nat.ptr(zr), nat.ptr(tab), nat.ptr(loss)),
+                  "fcb_cdf_model_state")
+        return {"params": params, "zrange": zr, "table": tab, "loss": loss}
+
+    def load(self, st):
+        p = np.ascontiguousarray(st["params"], np.float32)
+        z = np.ascontiguousarray(st["zrange"], np.float32)
+        t = np.ascontiguousarray(st["table"], np.float32)
+        nat.check(nat.lib().fcb_cdf_model_load(self._h, nat.ptr(p), nat.ptr(z), nat.ptr(t)), "fcb_cdf_model_load")
+
+    def close(self):
+        if self._h:
+            nat.lib().fcb_cdf_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cdf_grad(params, z, u):
+    """Loss and gradient of the CDF network on one batch (<= 256 samples),
+    computed by the GPU training kernel's forward/backward code."""
+    p = np.ascontiguousarray(params, np.float32)
+    z = np.ascontiguousarray(z, np.float32)
+    u = np.ascontiguousarray(u, np.float32)
+    g = np.empty(1153, np.float32)
+    loss = np.empty(1, np.float32)
+    nat.check(nat.lib().fcb_cdf_grad(nat.ptr(p), nat.ptr(z), nat.ptr(u), int(z.size), nat.ptr(g), nat.ptr(loss)),
+              "fcb_cdf_grad")
+    return float(loss[0]), g

@@ -35,6 +35,7 @@ PROTOTYPES = {
     "fcb_workspace_clear": (None, [_p]),
     "fcb_workspace_destroy": (None, [_p]),
     "fcb_workspace_stats": (_i, [_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "fcb_workspace_learned_state": (_i, [_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
     "fcb_version": (_i, []),
     "fcb_device_count": (_i, []),
     "fcb_status_string": (C.c_char_p, [_i]),
@@ -50,6 +51,14 @@ PROTOTYPES = {
     "fcb_dev_rank_ic_panel": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i, _p]),
     "fcb_dev_cs_rank_f32": (_i, [_p, _p, _i, _i, _i, _p, _p]),
     "fcb_dev_factor_corr_noalloc": (_i, [_p, _i, _p, _i, _i, _i, _p, _p]),
+    "fcb_cdf_model_create": (_p, [_i, C.c_uint64]),
+    "fcb_cdf_model_destroy": (None, [_p]),
+    "fcb_cdf_model_set_linear": (_i, [_p, _i]),
+    "fcb_cdf_model_fit": (_i, [_p, _p, _p, _i, _i, _i, _i, _i, C.c_float, _p]),
+    "fcb_cdf_model_state": (_i, [_p, _p, _p, _p, _p]),
+    "fcb_cdf_model_load": (_i, [_p, _p, _p, _p]),
+    "fcb_cdf_grad": (_i, [_p, _p, _p, _i, _p, _p]),
+    "fcb_dev_rank_ic_panel_learned": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _p, _i, _p, _p]),
 }
 
 

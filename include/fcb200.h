@@ -62,6 +62,11 @@ void fcb_workspace_destroy(fcb_workspace* ws);
 int fcb_workspace_stats(const fcb_workspace* ws, uint64_t* live_bytes, uint64_t* peak_bytes,
                         uint64_t* n_allocs);
 
+/* Learned-splitter state a workspace carries across fcb_rank_ic_panel calls
+ * (method 1): ready = a fitted table is in use, fits = refits scheduled so
+ * far, learned_chunks = date chunks ranked by the learned kernel so far. */
+int fcb_workspace_learned_state(const fcb_workspace* ws, int* ready, int* fits, int* learned_chunks);
+
 /* Library / device helpers. */
 int fcb_version(void);
 int fcb_device_count(void);
@@ -127,7 +132,10 @@ int fcb_stock_corr(const void* x, int dtype, const uint8_t* mask, int T, int N, 
  * :80-101, fused).  x (F,T,N) f32, r (T,N) f32, fmask / rmask (T,N) or NULL.
  * ranks (F,T,N) f32 (NULL = off) = cs_rank of each factor under fmask;
  * ic (F,T) f64 = rolling_ic(factor, r, fmask, rmask, min_valid).
- * method: 0 plain radix, 1 learned splitters (falls back to radix per date).
+ * method: 0 plain radix; 1 learned splitters: the first date chunk is ranked
+ * by radix and a CDF model is fitted on it, later chunks use the learned
+ * path, and the model is refitted (warm start) on the exact ranks of the
+ * latest chunk every 250 dates.
  * Host pointers; the panel is streamed through the device in date chunks
  * with copies overlapping the kernels.  No reference counterpart as one call. */
 int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* fmask, const uint8_t* rmask, int F,
@@ -143,6 +151,48 @@ int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const uint8_t* d_f
 /* Device-pointer cs_rank (asynchronous on `stream`). */
 int fcb_dev_cs_rank_f32(const float* d_x, const uint8_t* d_mask, int T, int N, int descending, float* d_out,
                         void* stream);
+
+/* ---------------------------------------------------- learned splitters ---
+ * No reference counterpart (a new form of the rank path).  A model holds one
+ * CDF network per factor (1 -> 32 -> 32 -> 1, tanh, sigmoid output) trained
+ * on the GPU by this library's forward/backward kernels, and its tabulated
+ * monotone CDF.  The learned rank path scatters each cross-section into
+ * buckets by that CDF and ranks each bucket exactly; every date is checked
+ * (strictly increasing (value, column) order over the whole output) and any
+ * failure, bucket above `cap` or unusable scale falls back to the radix sort,
+ * so ranks and IC are bit-identical to the radix path. */
+#define FCB_CDF_PARAMS 1153
+#define FCB_CDF_KNOTS 1024
+typedef struct fcb_cdf_model fcb_cdf_model;
+/* F networks, deterministic initialisation from seed; NULL on failure. */
+fcb_cdf_model* fcb_cdf_model_create(int F, uint64_t seed);
+void fcb_cdf_model_destroy(fcb_cdf_model* m);
+/* linear = 1: tabulate a linear ramp over the fitted range instead of the
+ * network (the bucket method without the network, for comparisons). */
+int fcb_cdf_model_set_linear(fcb_cdf_model* m, int linear);
+/* Fit on dates [t0, t0+tcount) of device panels d_x (F,T,N) f32 and their
+ * exact cs ranks d_ranks (F,T,N) f32 (NaN = unranked): 64 samples per date
+ * (standardised value, (rank-0.5)/m), `steps` Adam steps of 256 samples
+ * continuing from the model's previous state, then tabulation.  Async. */
+int fcb_cdf_model_fit(fcb_cdf_model* m, const float* d_x, const float* d_ranks, int T, int N, int t0, int tcount,
+                      int steps, float lr, void* stream);
+/* Save / restore (host buffers): params (F*FCB_CDF_PARAMS), zrange (F*2),
+ * table (F*FCB_CDF_KNOTS), last minibatch loss (F); NULL skips a field. */
+int fcb_cdf_model_state(const fcb_cdf_model* m, float* params, float* zrange, float* table, float* loss);
+int fcb_cdf_model_load(fcb_cdf_model* m, const float* params, const float* zrange, const float* table);
+/* Loss (sum of squared errors over samples with u >= 0) and its gradient
+ * w.r.t. the FCB_CDF_PARAMS parameters (mean-squared-error normalisation)
+ * for one batch of n <= 256 samples, by the training kernel's own
+ * forward/backward code.  Host pointers; for checking. */
+int fcb_cdf_grad(const float* params, const float* z, const float* u, int n, float* grad, float* loss);
+/* Learned rank + IC over device panels (as fcb_dev_rank_ic_panel); d_stats
+ * (NULL = off) receives (F,T,4) ints: outcome (1 learned, 2 bucket overflow,
+ * 3 judge rejected, 4 unusable scale; 2-4 fell back to radix), the largest
+ * bucket, the sum of squared bucket sizes (the per-date comparison work; m
+ * for perfectly even buckets of one) and m, the number of ranked cells. */
+int fcb_dev_rank_ic_panel_learned(const float* d_x, const float* d_r, const uint8_t* d_fmask,
+                                  const uint8_t* d_rmask, int F, int T, int N, int min_valid, float* d_ranks,
+                                  double* d_ic, const fcb_cdf_model* model, int cap, int* d_stats, void* stream);
 
 /* ------------------------------------------------ no-allocation variant ---
  * No counterpart in the reference.  factor_corr for callers that cannot let a
