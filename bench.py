@@ -68,6 +68,19 @@ def make_panel(T=T_DEF, N=N_DEF, F=F_DEF, seed=20261203):
     return X, R, fmask, rmask
 
 
+def make_stock_panel(T=1218, N=5000, seed=20261204):
+    """Stock returns for the stock_corr precision forms: 0.02 * t(4) noise
+    plus a 3-factor Gaussian common component (loadings ~ N(0, 0.5), factor
+    returns ~ N(0, 0.01^2)); mask = pre-listing gaps & Bernoulli(0.98)."""
+    rng = np.random.default_rng(seed)
+    B = rng.normal(0.0, 0.5, (N, 3))
+    f = rng.normal(0.0, 0.01, (T, 3))
+    X = (0.02 * rng.standard_t(4, (T, N)) + f @ B.T).astype(np.float32)
+    start = rng.integers(0, max(1, int(0.1 * T)), N)
+    mask = (np.arange(T)[:, None] >= start[None, :]) & (rng.random((T, N)) < 0.98)
+    return X, mask
+
+
 def algorithmic_bytes(F, T, N):
     """Bytes one launch must move: factor read + rank write (4+4 B/cell),
     returns + two masks per (t,i) (4+1+1 B), IC out (8 B per (f,t))."""
@@ -364,6 +377,58 @@ def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned
     return res
 
 
+def bench_stock_corr(dev, N, T=1218, steps=5, warmup=2):
+    """stock_corr precision forms on one (T,N) panel, device-resident:
+    BF16x3 tensor-core path vs plain FP32, error against the f64 path."""
+    import torch
+    from fcb200 import _native as nat
+    lib = nat.lib()
+    X, mask = make_stock_panel(T=T, N=N)
+    m8 = mask.astype(np.uint8)
+    ref = np.empty((N, N))
+    nat.check(lib.fcb_stock_corr(nat.ptr(X), 0, nat.ptr(m8), T, N, nat.ptr(ref), None, None), "fcb_stock_corr")
+    dX = torch.from_numpy(X).to(dev)
+    dM = torch.from_numpy(m8).to(dev)
+    dO = torch.empty((N, N), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ws = lib.fcb_workspace_create()
+    alg_flops = 4 * 2.0 * N * N * T           # X.X^T, X.M^T, X^2.M^T, M.M^T (dense-equivalent)
+    Tp = (T + 31) // 32 * 32
+    n_i = (N + 127) // 128
+    tiles = sum(1 for ti in range(n_i) for tj in range((N + 31) // 32) if tj * 32 + 31 >= ti * 128)
+    exec_flops = tiles * (Tp // 16) * 2.0 * 128 * 704 * 16   # issued MMA work (N-total 704 per 16 dates)
+    res = {"N": N, "T": T, "algorithmic_gflop": alg_flops / 1e9}
+    out = {}
+    for name, mode in (("bf16x3", 0), ("fp32", 1)):
+        def call():
+            nat.check(lib.fcb_dev_stock_corr_prec(dX.data_ptr(), dM.data_ptr(), T, N, mode, dO.data_ptr(), ws,
+                                                  stream.cuda_stream), "fcb_dev_stock_corr_prec")
+        for _ in range(warmup):
+            call()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / steps
+        got = dO.cpu().numpy()
+        err = np.abs(got - ref)
+        same_nan = bool(np.array_equal(np.isnan(got), np.isnan(ref)))
+        d = {"ms": ms, "tflops_algorithmic": alg_flops / (ms / 1e3) / 1e12,
+             "max_abs_err_vs_f64": float(np.nanmax(err)), "mean_abs_err_vs_f64": float(np.nanmean(err)),
+             "nan_pattern_matches": same_nan}
+        if mode == 0:
+            d["tflops_mma_issued"] = exec_flops / (ms / 1e3) / 1e12
+        out[name] = d
+    lib.fcb_workspace_destroy(ws)
+    res.update(out)
+    res["bf16x3_speedup_vs_fp32"] = out["fp32"]["ms"] / out["bf16x3"]["ms"]
+    return res
+
+
 def check_spot(X, R, fm, rm, dranks, dic):
     from oracle import fc_oracle as O
     F, T, N = X.shape
@@ -414,7 +479,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--method", choices=["radix", "learned"], default="radix")
+    ap.add_argument("--method", choices=["radix", "learned"], default="learned")
+    ap.add_argument("--no-stock-corr", action="store_true", help="skip the stock_corr precision-form leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--T", type=int, default=T_DEF)
@@ -436,6 +502,20 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     res = run_b200(args, rank, world)
+    if not args.no_stock_corr:
+        import torch
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+        peak_bf16 = None
+        p = ROOT / "MEASURED_PEAKS.json"
+        if p.exists():
+            peak_bf16 = float(json.loads(p.read_text())["bf16_tflops"])
+        sc = [bench_stock_corr(dev, N) for N in (2000, 5000)]
+        for r in sc:
+            if peak_bf16:
+                r["bf16x3"]["tensor_frac_of_measured_bf16_peak"] = r["bf16x3"]["tflops_mma_issued"] / peak_bf16
+        res["stock_corr"] = {"workload": "pairwise-complete (N,N) Pearson, T=1218, f32 returns "
+                                         "(0.02*t4 + 3-factor component), pre-listing gaps + Bernoulli(0.98) mask",
+                             "bf16_peak_tflops_measured": peak_bf16, "results": sc}
     if rank == 0:
         if not args.no_cpu_baseline:
             X, R, fm, rm = make_panel()

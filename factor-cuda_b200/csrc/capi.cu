@@ -26,6 +26,8 @@ enum Slot : int {
   S_X = 0, S_X2, S_MASK, S_MASK2, S_OUT, S_OUT1, S_OUT2, S_OUT3, S_STATUS, S_IC, S_RF, S_RR,
   S_SC_RAW, S_SC_C, S_SC_M, S_SC_ST, S_SC_SUM, S_FB_LIST, S_FB_CNT,
   S_FC_COLPART, S_FC_COLSTAT, S_FC_GRAM, S_FC_FLAGS,
+  S_PC_MU, S_PC_XH, S_PC_XM, S_PC_XL, S_PC_QH, S_PC_QM, S_PC_QL, S_PC_M16, S_PC_X32, S_PC_Q32, S_PC_M32, S_PC_TILES, S_PC_X, S_PC_MASK,
+  S_PC_OUT,
   // streamed panel: three chunk buffers each (upload / compute / download in flight)
   S_PX0, S_PX1, S_PX2, S_PR0, S_PR1, S_PR2, S_PFM0, S_PFM1, S_PFM2, S_PRM0, S_PRM1, S_PRM2,
   S_PRK0, S_PRK1, S_PRK2, S_PIC0, S_PIC1, S_PIC2,
@@ -677,6 +679,96 @@ extern "C" int fcb_factor_corr(const void* x, int dtype, const uint8_t* mask, in
   FCB_TRY(cudaMemcpyAsync(out, dout, static_cast<size_t>(F) * F * 8, cudaMemcpyDeviceToHost, s));
   if (fallback_out)
     FCB_TRY(cudaMemcpyAsync(fallback_out, dflags, static_cast<size_t>(F) * F, cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaStreamSynchronize(s));
+  return FCB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// stock_corr precision forms (BF16x3 tensor cores / FP32 SIMT)
+// ---------------------------------------------------------------------------
+static int prec_check(const void* x, const void* out, int T, int N, int mode) {
+  if (x == nullptr || out == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
+  if (mode != FCB_PREC_BF16X3 && mode != FCB_PREC_FP32) return FCB_ERR_ARG;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP2;
+  if (static_cast<long long>(N) * N > INT32_MAX) return FCB_ERR_CAP3;
+  return FCB_OK;
+}
+
+extern "C" int fcb_dev_stock_corr_prec(const float* d_x, const uint8_t* d_mask, int T, int N, int mode, double* d_out,
+                                       fcb_workspace* wsp, void* stream) {
+  const int chk = prec_check(d_x, d_out, T, N, mode);
+  if (chk != FCB_OK) return chk;
+  if (wsp == nullptr) return FCB_ERR_ARG;  // scratch must come from a caller-held workspace
+  fcb_workspace& ws = *wsp;
+  FCB_TRY(ws.bind());
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int Np = (N + 127) / 128 * 128;
+  const int Tp = (T + 31) / 32 * 32;
+  const size_t e = static_cast<size_t>(Np) * Tp;
+  PrecOperands op{};
+  float* mu;
+  int* dst;
+  FCB_TRY(ws.get(S_PC_MU, static_cast<size_t>(Np) * 4, &mu));
+  FCB_TRY(ws.get(S_STATUS, 64, &dst));
+  std::vector<int2> tiles;
+  if (mode == FCB_PREC_BF16X3) {
+    FCB_TRY(ws.get(S_PC_XH, e * 2, &op.h));
+    FCB_TRY(ws.get(S_PC_XM, e * 2, &op.mm));
+    FCB_TRY(ws.get(S_PC_XL, e * 2, &op.l));
+    FCB_TRY(ws.get(S_PC_QH, e * 2, &op.qh));
+    FCB_TRY(ws.get(S_PC_QM, e * 2, &op.qm));
+    FCB_TRY(ws.get(S_PC_QL, e * 2, &op.ql));
+    FCB_TRY(ws.get(S_PC_M16, e * 2, &op.m16));
+    for (int ti = 0; ti * kPrecTileTcM < N; ++ti)
+      for (int tj = 0; tj * kPrecTileTcN < N; ++tj)
+        if (tj * kPrecTileTcN + kPrecTileTcN - 1 >= ti * kPrecTileTcM) tiles.push_back(make_int2(ti, tj));
+  } else {
+    FCB_TRY(ws.get(S_PC_X32, e * 4, &op.x32));
+    FCB_TRY(ws.get(S_PC_Q32, e * 4, &op.q32));
+    FCB_TRY(ws.get(S_PC_M32, e * 4, &op.m32));
+    for (int ti = 0; ti * kPrecTileFp32 < N; ++ti)
+      for (int tj = ti; tj * kPrecTileFp32 < N; ++tj) tiles.push_back(make_int2(ti, tj));
+  }
+  int2* dt;
+  FCB_TRY(ws.get(S_PC_TILES, tiles.size() * sizeof(int2), &dt));
+  FCB_TRY(cudaMemcpyAsync(dt, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+  FCB_TRY(launch_prec_prep(d_x, d_mask, T, N, Np, Tp, mu, op, s));
+  if (mode == FCB_PREC_BF16X3) {
+    FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), s));
+    FCB_TRY(launch_corr_bf16x3(op, dt, static_cast<int>(tiles.size()), N, Np, Tp, d_out, dst, s));
+  } else {
+    FCB_TRY(launch_corr_fp32(op, dt, static_cast<int>(tiles.size()), N, Tp, d_out, s));
+  }
+  // the tile list upload reads a host vector: finish it before returning
+  FCB_TRY(cudaStreamSynchronize(s));
+  if (mode == FCB_PREC_BF16X3) {
+    int hst = 0;
+    FCB_TRY(cudaMemcpy(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hst != 0) return FCB_ERR_DEVICE_WAIT;
+  }
+  return FCB_OK;
+}
+
+extern "C" int fcb_stock_corr_prec(const float* x, const uint8_t* mask, int T, int N, int mode, double* out,
+                                   fcb_workspace* wsp) {
+  const int chk = prec_check(x, out, T, N, mode);
+  if (chk != FCB_OK) return chk;
+  WsScope sc(wsp);
+  fcb_workspace& ws = *sc.ws;
+  FCB_TRY(ws.bind());
+  cudaStream_t s = ws.stream[0];
+  const size_t n = static_cast<size_t>(T) * N;
+  float* dx;
+  uint8_t* dm = nullptr;
+  double* dout;
+  FCB_TRY(ws.get(S_PC_X, n * 4, &dx));
+  if (mask) FCB_TRY(ws.get(S_PC_MASK, n, &dm));
+  FCB_TRY(ws.get(S_PC_OUT, static_cast<size_t>(N) * N * 8, &dout));
+  FCB_TRY(cudaMemcpyAsync(dx, x, n * 4, cudaMemcpyHostToDevice, s));
+  if (mask) FCB_TRY(cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, s));
+  const int e = fcb_dev_stock_corr_prec(dx, dm, T, N, mode, dout, &ws, s);
+  if (e != FCB_OK) return e;
+  FCB_TRY(cudaMemcpyAsync(out, dout, static_cast<size_t>(N) * N * 8, cudaMemcpyDeviceToHost, s));
   FCB_TRY(cudaStreamSynchronize(s));
   return FCB_OK;
 }

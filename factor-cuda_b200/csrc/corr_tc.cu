@@ -1,0 +1,458 @@
+// corr_tc.cu -- precision forms of stock_corr: BF16x3 on the tcgen05 tensor
+// cores and a plain FP32 SIMT path, both with an FP64 finalize.
+//
+// Pairwise-complete Pearson over t needs six moment sums per stock pair
+// (i,j) over the joint valid dates: n, sum x, sum y, sum xy, sum x^2, sum y^2
+// (the masked products X.M^T, X.X^T, X^2.M^T, M.M^T of the reference's
+// masked-GEMM formulation, fc/_cpu_core.py:139-169).  Each column is first
+// centred by its own valid-date mean (the pairwise formula is shift
+// invariant), so the products stay well conditioned.
+//
+// BF16x3: x' and x'^2 are each split into three bf16 limbs (hi + mid + lo,
+// 24 significant bits -- exact for an f32 value); the mask M is exact in bf16.
+// The B operand of a tile is the stack [M; H; Mm; L; Qh; Qm; Ql] of the j
+// block, so one MMA against a stacked B yields several moment blocks at once.
+// Per 16-deep k step (tcgen05.mma kind::f16, bf16 in, fp32 accumulate in TMEM):
+//   D1 (N=128) += a . [M; H; Mm; L]^T    for a in {H, Mm, L}   -> sx | sum of
+//                 the 9 limb products of sxy in three column blocks
+//   D2 (N=224)  = M . [M; H; Mm; L; Qh; Qm; Ql]^T             -> n | sy (3) | sy2 (3)
+//   D3 (N=32)  += q . M^T                for q in {Qh, Qm, Ql} -> sx2
+// Operands are staged by TMA (cp.async.bulk.tensor, no swizzle, no cluster
+// multicast) into the canonical K-major no-swizzle layout: 8-row x 16-byte
+// core matrices, one 2D box per 8-column k chunk.  The FP64 finalize is
+//   cov = sxy - sx sy / n, vx = sx2 - sx^2/n, vy = sy2 - sy^2/n,
+//   r = (cov/sqrt(vx))/sqrt(vy),  NaN for n < 2 or a non-positive variance.
+#include <cuda.h>
+
+#include <cmath>
+
+#include "fcb_common.cuh"
+#include "fcb_kernels.h"
+
+namespace fcb {
+
+constexpr int kTcM = 128;      // output rows per tile (stocks i)
+constexpr int kTcN = 32;       // output columns per tile (stocks j)
+constexpr int kTcK = 32;       // k depth per pipeline stage
+constexpr int kTcStages = 3;
+constexpr int kTcMats = 7;     // A side: H Mm L Qh Qm Ql M;  B side: M H Mm L Qh Qm Ql
+constexpr int kChunksPerStage = kTcK / 8;
+constexpr int kAMat = kTcM * 16;                      // one A matrix, one 8-column k chunk
+constexpr int kBMat = kTcN * 16;                      // one B matrix, one k chunk
+constexpr int kAChunk = kTcMats * kAMat;              // all A matrices of one k chunk
+constexpr int kBChunk = kTcMats * kBMat;
+constexpr int kABytesStage = kChunksPerStage * kAChunk;
+constexpr int kBBytesStage = kChunksPerStage * kBChunk;
+constexpr int kStageBytes = kABytesStage + kBBytesStage;
+constexpr int kD1 = 0, kD2 = 128, kD3 = 352;          // TMEM column of each accumulator
+constexpr int kTmemCols = 512;                        // 384 used, rounded to a power of two
+
+// ---------------------------------------------------------------------------
+// prep: (T,N) f32 + mask -> K-major (Np, Tp) operands
+// ---------------------------------------------------------------------------
+__global__ void k_prec_colmean(const float* __restrict__ X, const uint8_t* __restrict__ mask, int T, int N,
+                               float* __restrict__ mu) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double s = 0.0, c = 0.0;
+  for (int t = 0; t < T; ++t) {
+    const float v = X[static_cast<size_t>(t) * N + i];
+    if (finite_f32(v) && (mask == nullptr || mask[static_cast<size_t>(t) * N + i])) {
+      s += v;
+      c += 1.0;
+    }
+  }
+  mu[i] = c > 0 ? static_cast<float>(s / c) : 0.0f;
+}
+
+// Transposing split: one 32x32 (t,i) tile per block.
+__global__ void k_prec_split(const float* __restrict__ X, const uint8_t* __restrict__ mask, const float* __restrict__ mu,
+                             int T, int N, int Tp, PrecOperands op) {
+  __shared__ float tv[32][33];
+  __shared__ float tm[32][33];
+  const int t0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int t = t0 + r, i = i0 + threadIdx.x;
+    float v = 0.0f, m = 0.0f;
+    if (t < T && i < N) {
+      const size_t e = static_cast<size_t>(t) * N + i;
+      const float x = X[e];
+      if (finite_f32(x) && (mask == nullptr || mask[e])) {
+        v = x - mu[i];
+        m = 1.0f;
+      }
+    }
+    tv[r][threadIdx.x] = v;
+    tm[r][threadIdx.x] = m;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, t = t0 + threadIdx.x;
+    if (t >= Tp) continue;
+    const size_t o = static_cast<size_t>(i) * Tp + t;  // rows up to Np (zero pad)
+    const float v = tv[threadIdx.x][r];
+    const float m = tm[threadIdx.x][r];
+    if (op.h != nullptr) {
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      const float r1 = v - __bfloat162float(h);
+      const __nv_bfloat16 mm = __float2bfloat16_rn(r1);
+      const __nv_bfloat16 l = __float2bfloat16_rn(r1 - __bfloat162float(mm));
+      const float q = v * v;
+      const __nv_bfloat16 qh = __float2bfloat16_rn(q);
+      const float s1 = q - __bfloat162float(qh);
+      const __nv_bfloat16 qm = __float2bfloat16_rn(s1);
+      const __nv_bfloat16 ql = __float2bfloat16_rn(s1 - __bfloat162float(qm));
+      op.h[o] = h;
+      op.mm[o] = mm;
+      op.l[o] = l;
+      op.qh[o] = qh;
+      op.qm[o] = qm;
+      op.ql[o] = ql;
+      op.m16[o] = __float2bfloat16_rn(m);
+    }
+    if (op.x32 != nullptr) {
+      op.x32[o] = v;
+      op.q32[o] = v * v;
+      op.m32[o] = m;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 helpers
+// ---------------------------------------------------------------------------
+FCB_DEV uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);
+  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;  // descriptor version (Blackwell)
+  // base offset 0, absolute-LBO mode off, layout type 0 = no swizzle
+  return d;
+}
+
+// kind::f16 instruction descriptor: bf16 A/B, f32 D, K-major A and B, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4)                                   // D format f32
+         | (1u << 7)                                 // A format bf16
+         | (1u << 10)                                // B format bf16
+         | (static_cast<uint32_t>(N >> 3) << 17)     // N / 8
+         | (static_cast<uint32_t>(M >> 4) << 24);    // M / 16
+}
+
+FCB_DEV void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+FCB_DEV void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+FCB_DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+FCB_DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+FCB_DEV void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+FCB_DEV void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+FCB_DEV double pearson_from_moments(double n, double sx, double sy, double sxy, double sx2, double sy2) {
+  if (n < 2.0) return __longlong_as_double(0x7ff8000000000000ll);
+  const double cov = sxy - sx * sy / n;
+  const double vx = sx2 - sx * sx / n;
+  const double vy = sy2 - sy * sy / n;
+  if (!(vx > 0.0 && vy > 0.0)) return __longlong_as_double(0x7ff8000000000000ll);
+  const double r = (cov / sqrt(vx)) / sqrt(vy);
+  return isfinite(r) ? r : __longlong_as_double(0x7ff8000000000000ll);
+}
+
+FCB_DEV void write_pair(double* out, int N, int i, int j, double r) {
+  if (i == j) r = isfinite(r) ? 1.0 : r;
+  out[static_cast<size_t>(i) * N + j] = r;
+  out[static_cast<size_t>(j) * N + i] = r;
+}
+
+// ---------------------------------------------------------------------------
+// BF16x3 tcgen05 kernel: one 128 x 32 output tile per CTA
+// warps: 0 TMA producer, 1 TMEM owner + MMA issuer, 2..5 epilogue
+// ---------------------------------------------------------------------------
+struct TcMaps {
+  CUtensorMap a[kTcMats];  // box {8, 128}, order H Mm L Qh Qm Ql M
+  CUtensorMap b[kTcMats];  // box {8, 32},  order M H Mm L Qh Qm Ql
+};
+
+// sum of `nb` 16-column TMEM blocks spaced 32 columns apart, in f64
+FCB_DEV void tmem_sum_blocks(uint32_t taddr, int nb, double* acc) {
+#pragma unroll
+  for (int u = 0; u < 16; ++u) acc[u] = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    float v[16];
+    tmem_ld16(taddr + b * kTcN, v);
+#pragma unroll
+    for (int u = 0; u < 16; ++u) acc[u] += static_cast<double>(v[u]);
+  }
+}
+
+__global__ void __launch_bounds__(192, 1)
+    k_corr_bf16x3(const __grid_constant__ TcMaps maps, const int2* __restrict__ tiles, int N, int Tp,
+                  double* __restrict__ out, int* __restrict__ status) {
+  extern __shared__ __align__(1024) uint8_t sm_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + kTcStages * kStageBytes);
+  uint64_t* empty = full + kTcStages;
+  uint64_t* accb = empty + kTcStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
+  int* err = reinterpret_cast<int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int2 tile = tiles[blockIdx.x];
+  const int i0 = tile.x * kTcM, j0 = tile.y * kTcN;
+  const int nkt = Tp / kTcK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kTcStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accb, 1);
+    *err = 0;
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int kt = 0; kt < nkt; ++kt) {
+        const int s = kt % kTcStages, round = kt / kTcStages;
+        if (round > 0 && !mbar_wait(&empty[s], (round - 1) & 1)) {
+          atomicExch(err, 1);
+          break;
+        }
+        uint8_t* st = sm + s * kStageBytes;
+        mbar_expect_tx(&full[s], kStageBytes);
+        for (int c = 0; c < kChunksPerStage; ++c) {
+          const int x = kt * kTcK + c * 8;
+          for (int m = 0; m < kTcMats; ++m) {
+            tma_load_2d(st + c * kAChunk + m * kAMat, &maps.a[m], x, i0, &full[s]);
+            tma_load_2d(st + kABytesStage + c * kBChunk + m * kBMat, &maps.b[m], x, j0, &full[s]);
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t id128 = idesc_bf16(kTcM, 4 * kTcN);
+      constexpr uint32_t id224 = idesc_bf16(kTcM, 7 * kTcN);
+      constexpr uint32_t id32 = idesc_bf16(kTcM, kTcN);
+      for (int kt = 0; kt < nkt; ++kt) {
+        const int s = kt % kTcStages, round = kt / kTcStages;
+        if (!mbar_wait(&full[s], round & 1)) {
+          atomicExch(err, 1);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t abase = smem_u32(sm + s * kStageBytes);
+        const uint32_t bbase = abase + kABytesStage;
+#pragma unroll
+        for (int ks = 0; ks < kTcK / 16; ++ks) {
+          const uint32_t ak = abase + 2 * ks * kAChunk;
+          const uint32_t bk = bbase + 2 * ks * kBChunk;
+          const uint64_t bstack = smem_desc(bk, kBChunk, 128);  // [M; H; Mm; L; Qh; Qm; Ql] rows
+          const uint32_t first = (kt == 0 && ks == 0) ? 0u : 1u;
+          // D1: x limbs against [M; H; Mm; L]
+          mma_bf16(tmem + kD1, smem_desc(ak + 0 * kAMat, kAChunk, 128), bstack, id128, first);
+          mma_bf16(tmem + kD1, smem_desc(ak + 1 * kAMat, kAChunk, 128), bstack, id128, 1u);
+          mma_bf16(tmem + kD1, smem_desc(ak + 2 * kAMat, kAChunk, 128), bstack, id128, 1u);
+          // D2: mask against the whole stack
+          mma_bf16(tmem + kD2, smem_desc(ak + 6 * kAMat, kAChunk, 128), bstack, id224, first);
+          // D3: x'^2 limbs against M
+          mma_bf16(tmem + kD3, smem_desc(ak + 3 * kAMat, kAChunk, 128), bstack, id32, first);
+          mma_bf16(tmem + kD3, smem_desc(ak + 4 * kAMat, kAChunk, 128), bstack, id32, 1u);
+          mma_bf16(tmem + kD3, smem_desc(ak + 5 * kAMat, kAChunk, 128), bstack, id32, 1u);
+        }
+        mma_commit(&empty[s]);  // frees the stage when these MMAs complete
+      }
+      mma_commit(accb);
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 (its row quadrant)
+    const int quad = warp & 3;
+    const int row = quad * 32 + lane;
+    const bool ok = mbar_wait(accb, 0);
+    tc_fence_after();
+    if (!ok) atomicExch(err, 1);
+    const int i = i0 + row;
+    const uint32_t lrow = static_cast<uint32_t>(quad * 32) << 16;
+    for (int c0 = 0; c0 < kTcN; c0 += 16) {
+      float sx[16], n[16], sx2[16];
+      double sxy[16], sy[16], sy2[16];
+      tmem_ld16(tmem + lrow + kD1 + c0, sx);
+      tmem_sum_blocks(tmem + lrow + kD1 + kTcN + c0, 3, sxy);
+      tmem_ld16(tmem + lrow + kD2 + c0, n);
+      tmem_sum_blocks(tmem + lrow + kD2 + kTcN + c0, 3, sy);
+      tmem_sum_blocks(tmem + lrow + kD2 + 4 * kTcN + c0, 3, sy2);
+      tmem_ld16(tmem + lrow + kD3 + c0, sx2);
+      if (ok && *err == 0 && i < N) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const int j = j0 + c0 + u;
+          if (j < N && i <= j)
+            write_pair(out, N, i, j, pearson_from_moments(n[u], sx[u], sy[u], sxy[u], sx2[u], sy2[u]));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  }
+  if (threadIdx.x == 0 && *err != 0) atomicExch(status, 1);
+}
+
+// ---------------------------------------------------------------------------
+// plain FP32 SIMT path: 64 x 64 tiles, 256 threads, 4x4 cells per thread
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_corr_fp32(const float* __restrict__ X, const float* __restrict__ Q,
+                                                   const float* __restrict__ M, const int2* __restrict__ tiles,
+                                                   int N, int Tp, double* __restrict__ out) {
+  constexpr int TS = 64, KT = 16;
+  __shared__ float ax[KT][TS + 4], aq[KT][TS + 4], am[KT][TS + 4];
+  __shared__ float bx[KT][TS + 4], bq[KT][TS + 4], bm[KT][TS + 4];
+  const int2 tile = tiles[blockIdx.x];
+  const int i0 = tile.x * TS, j0 = tile.y * TS;
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+  float acc[6][4][4];
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[q][a][b] = 0.0f;
+  for (int k0 = 0; k0 < Tp; k0 += KT) {
+    for (int e = threadIdx.x; e < TS * KT; e += 256) {
+      const int r = e / KT, k = e % KT;
+      const size_t oi = static_cast<size_t>(i0 + r) * Tp + k0 + k;
+      const size_t oj = static_cast<size_t>(j0 + r) * Tp + k0 + k;
+      ax[k][r] = X[oi];
+      aq[k][r] = Q[oi];
+      am[k][r] = M[oi];
+      bx[k][r] = X[oj];
+      bq[k][r] = Q[oj];
+      bm[k][r] = M[oj];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < KT; ++k) {
+      float xi[4], qi[4], mi[4], xj[4], qj[4], mj[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        xi[a] = ax[k][ty * 4 + a];
+        qi[a] = aq[k][ty * 4 + a];
+        mi[a] = am[k][ty * 4 + a];
+        xj[a] = bx[k][tx * 4 + a];
+        qj[a] = bq[k][tx * 4 + a];
+        mj[a] = bm[k][tx * 4 + a];
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          acc[0][a][b] = fmaf(mi[a], mj[b], acc[0][a][b]);
+          acc[1][a][b] = fmaf(xi[a], mj[b], acc[1][a][b]);
+          acc[2][a][b] = fmaf(mi[a], xj[b], acc[2][a][b]);
+          acc[3][a][b] = fmaf(xi[a], xj[b], acc[3][a][b]);
+          acc[4][a][b] = fmaf(qi[a], mj[b], acc[4][a][b]);
+          acc[5][a][b] = fmaf(mi[a], qj[b], acc[5][a][b]);
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = i0 + ty * 4 + a, j = j0 + tx * 4 + b;
+      if (i < N && j < N && i <= j)
+        write_pair(out, N, i, j,
+                   pearson_from_moments(acc[0][a][b], acc[1][a][b], acc[2][a][b], acc[3][a][b], acc[4][a][b],
+                                        acc[5][a][b]));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+size_t prec_tc_smem() { return kTcStages * kStageBytes + 1024 + 256; }
+
+cudaError_t launch_prec_prep(const float* X, const uint8_t* mask, int T, int N, int Np, int Tp, float* mu,
+                             PrecOperands op, cudaStream_t s) {
+  k_prec_colmean<<<(N + 127) / 128, 128, 0, s>>>(X, mask, T, N, mu);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  dim3 g((Tp + 31) / 32, (Np + 31) / 32), b(32, 8);
+  k_prec_split<<<g, b, 0, s>>>(X, mask, mu, T, N, Tp, op);
+  return cudaGetLastError();
+}
+
+static CUresult make_map(CUtensorMap* map, const void* base, int Np, int Tp, int box_rows) {
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(Tp), static_cast<cuuint64_t>(Np)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(Tp) * 2};
+  const cuuint32_t box[2] = {8, static_cast<cuuint32_t>(box_rows)};
+  const cuuint32_t estr[2] = {1, 1};
+  return cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
+                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+}
+
+cudaError_t launch_corr_bf16x3(const PrecOperands& op, const int2* tiles, int ntiles, int N, int Np, int Tp,
+                               double* out, int* status, cudaStream_t s) {
+  TcMaps maps;
+  const __nv_bfloat16* amats[kTcMats] = {op.h, op.mm, op.l, op.qh, op.qm, op.ql, op.m16};
+  const __nv_bfloat16* bmats[kTcMats] = {op.m16, op.h, op.mm, op.l, op.qh, op.qm, op.ql};
+  for (int m = 0; m < kTcMats; ++m) {
+    if (make_map(&maps.a[m], amats[m], Np, Tp, kTcM) != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    if (make_map(&maps.b[m], bmats[m], Np, Tp, kTcN) != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  }
+  const size_t smem = prec_tc_smem();
+  cudaError_t e = cudaFuncSetAttribute(k_corr_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  k_corr_bf16x3<<<ntiles, 192, smem, s>>>(maps, tiles, N, Tp, out, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_corr_fp32(const PrecOperands& op, const int2* tiles, int ntiles, int N, int Tp, double* out,
+                             cudaStream_t s) {
+  k_corr_fp32<<<ntiles, 256, 0, s>>>(op.x32, op.q32, op.m32, tiles, N, Tp, out);
+  return cudaGetLastError();
+}
+
+}  // namespace fcb

@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 namespace fcb {
@@ -79,6 +80,25 @@ cudaError_t launch_cdf_grad(const float* params, const float* z, const float* u,
                             cudaStream_t s);
 cudaError_t launch_cdf_tabulate(const float* params, const float2* samples, int F, int nsamp, float* zrange,
                                 float* table, bool linear, cudaStream_t s);
+
+// Operands of the stock_corr precision forms, K-major (Np rows x Tp dates),
+// column-centred; unused members are nullptr.
+struct PrecOperands {
+  __nv_bfloat16 *h, *mm, *l;     // three bf16 limbs of x'
+  __nv_bfloat16 *qh, *qm, *ql;   // three bf16 limbs of x'^2
+  __nv_bfloat16* m16;            // 0/1 mask
+  float *x32, *q32, *m32;        // FP32 x', x'^2, mask
+};
+
+// corr_tc.cu
+constexpr int kPrecTileTcM = 128, kPrecTileTcN = 32, kPrecTileFp32 = 64;
+size_t prec_tc_smem();
+cudaError_t launch_prec_prep(const float* X, const uint8_t* mask, int T, int N, int Np, int Tp, float* mu,
+                             PrecOperands op, cudaStream_t s);
+cudaError_t launch_corr_bf16x3(const PrecOperands& op, const int2* tiles, int ntiles, int N, int Np, int Tp,
+                               double* out, int* status, cudaStream_t s);
+cudaError_t launch_corr_fp32(const PrecOperands& op, const int2* tiles, int ntiles, int N, int Tp, double* out,
+                             cudaStream_t s);
 
 // corr_kernels.cu
 cudaError_t launch_stock_corr_prep(const void* X, int dtype, const uint8_t* mask, int T, int N, int Tp,

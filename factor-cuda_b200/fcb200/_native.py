@@ -51,6 +51,8 @@ PROTOTYPES = {
     "fcb_dev_rank_ic_panel": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i, _p]),
     "fcb_dev_cs_rank_f32": (_i, [_p, _p, _i, _i, _i, _p, _p]),
     "fcb_dev_factor_corr_noalloc": (_i, [_p, _i, _p, _i, _i, _i, _p, _p]),
+    "fcb_stock_corr_prec": (_i, [_p, _p, _i, _i, _i, _p, _p]),
+    "fcb_dev_stock_corr_prec": (_i, [_p, _p, _i, _i, _i, _p, _p, _p]),
     "fcb_cdf_model_create": (_p, [_i, C.c_uint64]),
     "fcb_cdf_model_destroy": (None, [_p]),
     "fcb_cdf_model_set_linear": (_i, [_p, _i]),

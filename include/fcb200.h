@@ -194,6 +194,26 @@ int fcb_dev_rank_ic_panel_learned(const float* d_x, const float* d_r, const uint
                                   const uint8_t* d_rmask, int F, int T, int N, int min_valid, float* d_ranks,
                                   double* d_ic, const fcb_cdf_model* model, int cap, int* d_stats, void* stream);
 
+/* ------------------------------------------------------ precision forms ---
+ * No reference counterpart (a new form of stock_corr).  Pairwise-complete
+ * (N,N) Pearson of an f32 (T,N) panel with column-centred moments formed by
+ *   FCB_PREC_BF16X3: x' and x'^2 split into three bf16 limbs each, all limb
+ *                    products on the tcgen05 tensor cores (7 MMAs per 16
+ *                    dates against a stacked B operand, fp32 accumulation
+ *                    in TMEM);
+ *   FCB_PREC_FP32:   plain fp32 FMA on the CUDA cores;
+ * both finalised in f64: cov = sxy - sx sy/n etc., r = (cov/sqrt(vx))/sqrt(vy),
+ * NaN for n < 2 or a non-positive variance, diagonal 1.0 iff finite, lower
+ * triangle mirrored.  No cancellation fallback: tolerance, not bit parity,
+ * against the f64 path (tests state the bound).  The device variant takes
+ * its scratch from the workspace (required) and synchronises `stream`. */
+#define FCB_PREC_BF16X3 0
+#define FCB_PREC_FP32 1
+int fcb_stock_corr_prec(const float* x, const uint8_t* mask, int T, int N, int mode, double* out,
+                        fcb_workspace* ws);
+int fcb_dev_stock_corr_prec(const float* d_x, const uint8_t* d_mask, int T, int N, int mode, double* d_out,
+                            fcb_workspace* ws, void* stream);
+
 /* ------------------------------------------------ no-allocation variant ---
  * No counterpart in the reference.  factor_corr for callers that cannot let a
  * library allocate device memory: applications whose device memory belongs to
