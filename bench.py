@@ -483,6 +483,8 @@ def main():
     ap.add_argument("--no-stock-corr", action="store_true", help="skip the stock_corr precision-form leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--only-stock-corr", type=int, default=0, metavar="N",
+                    help="run only the stock_corr precision leg at this N (profiling)")
     ap.add_argument("--T", type=int, default=T_DEF)
     ap.add_argument("--N", type=int, default=N_DEF)
     ap.add_argument("--F", type=int, default=F_DEF)
@@ -490,6 +492,11 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
 
+    if args.only_stock_corr:
+        import torch
+        print(json.dumps(bench_stock_corr(torch.device("cuda", 0), args.only_stock_corr, steps=args.steps,
+                                          warmup=args.warmup)))
+        return
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)))

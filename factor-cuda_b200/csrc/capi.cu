@@ -30,7 +30,7 @@ enum Slot : int {
   S_PC_OUT,
   // streamed panel: three chunk buffers each (upload / compute / download in flight)
   S_PX0, S_PX1, S_PX2, S_PR0, S_PR1, S_PR2, S_PFM0, S_PFM1, S_PFM2, S_PRM0, S_PRM1, S_PRM2,
-  S_PRK0, S_PRK1, S_PRK2, S_PIC0, S_PIC1, S_PIC2,
+  S_PRK0, S_PRK1, S_PRK2, S_PIC,
   S_COUNT
 };
 
@@ -482,14 +482,14 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
   uint8_t* dfm[NB] = {};
   uint8_t* drm[NB] = {};
   float* drk[NB] = {};
-  double* dic[NB];
+  double* dic;  // whole (F,T) IC panel, downloaded once at the end
   int* dst;
   const size_t cn = static_cast<size_t>(Tc) * N;
   FCB_TRY(ws.get(S_STATUS, 64, &dst));
+  FCB_TRY(ws.get(S_PIC, static_cast<size_t>(F) * T * 8, &dic));
   for (int b = 0; b < NB; ++b) {
     FCB_TRY(ws.get(static_cast<Slot>(S_PX0 + b), cn * F * 4, &dx[b]));
     FCB_TRY(ws.get(static_cast<Slot>(S_PR0 + b), cn * 4, &dr[b]));
-    FCB_TRY(ws.get(static_cast<Slot>(S_PIC0 + b), static_cast<size_t>(F) * Tc * 8, &dic[b]));
     if (fmask) FCB_TRY(ws.get(static_cast<Slot>(S_PFM0 + b), cn, &dfm[b]));
     if (rmask) FCB_TRY(ws.get(static_cast<Slot>(S_PRM0 + b), cn, &drm[b]));
     if (need_ranks) FCB_TRY(ws.get(static_cast<Slot>(S_PRK0 + b), cn * F * 4, &drk[b]));
@@ -531,9 +531,9 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
     const int tc = (t0 + Tc <= T) ? Tc : (T - t0);
     const size_t cnn = static_cast<size_t>(tc) * N;
     if (c >= NB) FCB_TRY(cudaStreamWaitEvent(s_in, ev_out[j], 0));  // buffer set j drained
-    for (int f = 0; f < F; ++f)
-      FCB_TRY(cudaMemcpyAsync(dx[j] + static_cast<size_t>(f) * tc * N, x + (static_cast<size_t>(f) * T + t0) * N,
-                              cnn * 4, cudaMemcpyHostToDevice, s_in));
+    // one strided copy moves this date range of all F factor panels
+    FCB_TRY(cudaMemcpy2DAsync(dx[j], cnn * 4, x + static_cast<size_t>(t0) * N, static_cast<size_t>(T) * N * 4, cnn * 4,
+                              F, cudaMemcpyHostToDevice, s_in));
     FCB_TRY(cudaMemcpyAsync(dr[j], r + static_cast<size_t>(t0) * N, cnn * 4, cudaMemcpyHostToDevice, s_in));
     if (fmask) FCB_TRY(cudaMemcpyAsync(dfm[j], fmask + static_cast<size_t>(t0) * N, cnn, cudaMemcpyHostToDevice, s_in));
     if (rmask) FCB_TRY(cudaMemcpyAsync(drm[j], rmask + static_cast<size_t>(t0) * N, cnn, cudaMemcpyHostToDevice, s_in));
@@ -541,12 +541,13 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
     FCB_TRY(cudaStreamWaitEvent(s_c, ev_in[j], 0));
     if (learned) ws.poll_fit();
     if (learned && ws.model_ready) {
-      const int e = fcb_dev_rank_ic_panel_learned(dx[j], dr[j], dfm[j], drm[j], F, tc, N, min_valid, drk[j], dic[j],
-                                                  ws.model, 0, nullptr, s_c);
+      const int e = fcb::rank_ic_learned_ld(dx[j], dr[j], dfm[j], drm[j], F, tc, N, min_valid, drk[j], dic + t0, T,
+                                            ws.model, 0, nullptr, s_c);
       if (e != 0) return e;
       ++ws.learned_chunks;
     } else {
-      RankIcArgs<float, float> a{dx[j], dr[j], dfm[j], drm[j], F, tc, N, min_valid, drk[j], dic[j], nullptr, nullptr};
+      RankIcArgs<float, float> a{dx[j], dr[j], dfm[j], drm[j], F, tc, N, min_valid, drk[j], dic + t0, nullptr, nullptr};
+      a.ic_ld = T;
       FCB_TRY(launch_rank_ic<float, float>(a, dst, s_c));
     }
     if (learned) {
@@ -566,15 +567,13 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
     }
     FCB_TRY(cudaEventRecord(ev_comp[j], s_c));
     FCB_TRY(cudaStreamWaitEvent(s_out, ev_comp[j], 0));
-    for (int f = 0; f < F; ++f) {
-      FCB_TRY(cudaMemcpyAsync(ic + static_cast<size_t>(f) * T + t0, dic[j] + static_cast<size_t>(f) * tc,
-                              static_cast<size_t>(tc) * 8, cudaMemcpyDeviceToHost, s_out));
-      if (ranks)
-        FCB_TRY(cudaMemcpyAsync(ranks + (static_cast<size_t>(f) * T + t0) * N, drk[j] + static_cast<size_t>(f) * tc * N,
-                                cnn * 4, cudaMemcpyDeviceToHost, s_out));
-    }
+    if (ranks)
+      FCB_TRY(cudaMemcpy2DAsync(ranks + static_cast<size_t>(t0) * N, static_cast<size_t>(T) * N * 4, drk[j], cnn * 4,
+                                cnn * 4, F, cudaMemcpyDeviceToHost, s_out));
     FCB_TRY(cudaEventRecord(ev_out[j], s_out));
   }
+  FCB_TRY(cudaStreamWaitEvent(s_out, ev_comp[(nchunk - 1) % NB], 0));
+  FCB_TRY(cudaMemcpyAsync(ic, dic, static_cast<size_t>(F) * T * 8, cudaMemcpyDeviceToHost, s_out));
   int hst = 0;
   FCB_TRY(cudaStreamSynchronize(s_in));
   FCB_TRY(cudaStreamSynchronize(s_c));
@@ -712,13 +711,8 @@ extern "C" int fcb_dev_stock_corr_prec(const float* d_x, const uint8_t* d_mask, 
   FCB_TRY(ws.get(S_STATUS, 64, &dst));
   std::vector<int2> tiles;
   if (mode == FCB_PREC_BF16X3) {
-    FCB_TRY(ws.get(S_PC_XH, e * 2, &op.h));
-    FCB_TRY(ws.get(S_PC_XM, e * 2, &op.mm));
-    FCB_TRY(ws.get(S_PC_XL, e * 2, &op.l));
-    FCB_TRY(ws.get(S_PC_QH, e * 2, &op.qh));
-    FCB_TRY(ws.get(S_PC_QM, e * 2, &op.qm));
-    FCB_TRY(ws.get(S_PC_QL, e * 2, &op.ql));
-    FCB_TRY(ws.get(S_PC_M16, e * 2, &op.m16));
+    FCB_TRY(ws.get(S_PC_XH, e * 2 * 7, &op.h));
+    op.np = Np;
     for (int ti = 0; ti * kPrecTileTcM < N; ++ti)
       for (int tj = 0; tj * kPrecTileTcN < N; ++tj)
         if (tj * kPrecTileTcN + kPrecTileTcN - 1 >= ti * kPrecTileTcM) tiles.push_back(make_int2(ti, tj));

@@ -32,4 +32,8 @@ cudaError_t cdf_model_features(fcb_cdf_model* m, const float* d_x, const float* 
                                int tcount, cudaStream_t s);
 // Adam steps on the extracted samples, then tabulate into table slot `slot`.
 cudaError_t cdf_model_train_tabulate(fcb_cdf_model* m, int steps, float lr, int slot, cudaStream_t s);
+// Learned rank + IC with an explicit IC row stride (ic_ld = 0: T).
+int rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d_fmask, const uint8_t* d_rmask, int F,
+                       int T, int N, int min_valid, float* d_ranks, double* d_ic, int ic_ld,
+                       const fcb_cdf_model* model, int cap, int* d_stats, cudaStream_t stream);
 }  // namespace fcb

@@ -18,8 +18,8 @@
 //   D2 (N=224)  = M . [M; H; Mm; L; Qh; Qm; Ql]^T             -> n | sy (3) | sy2 (3)
 //   D3 (N=32)  += q . M^T                for q in {Qh, Qm, Ql} -> sx2
 // Operands are staged by TMA (cp.async.bulk.tensor, no swizzle, no cluster
-// multicast) into the canonical K-major no-swizzle layout: 8-row x 16-byte
-// core matrices, one 2D box per 8-column k chunk.  The FP64 finalize is
+// multicast) into the canonical K-major no-swizzle layout of 8-row x 16-byte
+// core matrices; one 4D box per operand fills a whole pipeline stage.  The FP64 finalize is
 //   cov = sxy - sx sy / n, vx = sx2 - sx^2/n, vy = sy2 - sy^2/n,
 //   r = (cov/sqrt(vx))/sqrt(vy),  NaN for n < 2 or a non-positive variance.
 #include <cuda.h>
@@ -35,7 +35,7 @@ constexpr int kTcM = 128;      // output rows per tile (stocks i)
 constexpr int kTcN = 32;       // output columns per tile (stocks j)
 constexpr int kTcK = 32;       // k depth per pipeline stage
 constexpr int kTcStages = 3;
-constexpr int kTcMats = 7;     // A side: H Mm L Qh Qm Ql M;  B side: M H Mm L Qh Qm Ql
+constexpr int kTcMats = 7;     // operand matrices, order M H Mm L Qh Qm Ql
 constexpr int kChunksPerStage = kTcK / 8;
 constexpr int kAMat = kTcM * 16;                      // one A matrix, one 8-column k chunk
 constexpr int kBMat = kTcN * 16;                      // one B matrix, one k chunk
@@ -52,17 +52,31 @@ constexpr int kTmemCols = 512;                        // 384 used, rounded to a 
 // ---------------------------------------------------------------------------
 __global__ void k_prec_colmean(const float* __restrict__ X, const uint8_t* __restrict__ mask, int T, int N,
                                float* __restrict__ mu) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+  // block (32, 8): 32 columns, 8 date strides; coalesced row reads
+  __shared__ double ss[8][33];
+  __shared__ double sc[8][33];
+  const int i = blockIdx.x * 32 + threadIdx.x;
   double s = 0.0, c = 0.0;
-  for (int t = 0; t < T; ++t) {
-    const float v = X[static_cast<size_t>(t) * N + i];
-    if (finite_f32(v) && (mask == nullptr || mask[static_cast<size_t>(t) * N + i])) {
-      s += v;
-      c += 1.0;
+  if (i < N) {
+    for (int t = threadIdx.y; t < T; t += 8) {
+      const size_t e = static_cast<size_t>(t) * N + i;
+      const float v = X[e];
+      if (finite_f32(v) && (mask == nullptr || mask[e])) {
+        s += v;
+        c += 1.0;
+      }
     }
   }
-  mu[i] = c > 0 ? static_cast<float>(s / c) : 0.0f;
+  ss[threadIdx.y][threadIdx.x] = s;
+  sc[threadIdx.y][threadIdx.x] = c;
+  __syncthreads();
+  if (threadIdx.y == 0 && i < N) {
+    for (int y = 1; y < 8; ++y) {
+      s += ss[y][threadIdx.x];
+      c += sc[y][threadIdx.x];
+    }
+    mu[i] = c > 0 ? static_cast<float>(s / c) : 0.0f;
+  }
 }
 
 // Transposing split: one 32x32 (t,i) tile per block.
@@ -102,13 +116,15 @@ __global__ void k_prec_split(const float* __restrict__ X, const uint8_t* __restr
       const float s1 = q - __bfloat162float(qh);
       const __nv_bfloat16 qm = __float2bfloat16_rn(s1);
       const __nv_bfloat16 ql = __float2bfloat16_rn(s1 - __bfloat162float(qm));
-      op.h[o] = h;
-      op.mm[o] = mm;
-      op.l[o] = l;
-      op.qh[o] = qh;
-      op.qm[o] = qm;
-      op.ql[o] = ql;
-      op.m16[o] = __float2bfloat16_rn(m);
+      const size_t plane = static_cast<size_t>(op.np) * Tp;
+      __nv_bfloat16* b = op.h;  // [7][Np][Tp]: M H Mm L Qh Qm Ql
+      b[o] = __float2bfloat16_rn(m);
+      b[plane + o] = h;
+      b[2 * plane + o] = mm;
+      b[3 * plane + o] = l;
+      b[4 * plane + o] = qh;
+      b[5 * plane + o] = qm;
+      b[6 * plane + o] = ql;
     }
     if (op.x32 != nullptr) {
       op.x32[o] = v;
@@ -163,6 +179,14 @@ FCB_DEV void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64
       : "memory");
 }
 
+FCB_DEV void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+
 FCB_DEV void tmem_ld16(uint32_t taddr, float* v) {
   uint32_t r[16];
   asm volatile(
@@ -195,9 +219,13 @@ FCB_DEV void write_pair(double* out, int N, int i, int j, double r) {
 // BF16x3 tcgen05 kernel: one 128 x 32 output tile per CTA
 // warps: 0 TMA producer, 1 TMEM owner + MMA issuer, 2..5 epilogue
 // ---------------------------------------------------------------------------
+// One 4D view of the [7][Np][Tp] operand buffer: dims {8 dates, Np rows,
+// 7 matrices, Tp/8 chunks}.  A box {8, rows, 7, 4} lands in shared memory in
+// (chunk, matrix, row) order -- exactly the stacked core-matrix layout -- so
+// one TMA per operand fills a whole stage.
 struct TcMaps {
-  CUtensorMap a[kTcMats];  // box {8, 128}, order H Mm L Qh Qm Ql M
-  CUtensorMap b[kTcMats];  // box {8, 32},  order M H Mm L Qh Qm Ql
+  CUtensorMap a;  // box {8, 128, 7, 4}
+  CUtensorMap b;  // box {8, 32, 7, 4}
 };
 
 // sum of `nb` 16-column TMEM blocks spaced 32 columns apart, in f64
@@ -256,13 +284,8 @@ __global__ void __launch_bounds__(192, 1)
         }
         uint8_t* st = sm + s * kStageBytes;
         mbar_expect_tx(&full[s], kStageBytes);
-        for (int c = 0; c < kChunksPerStage; ++c) {
-          const int x = kt * kTcK + c * 8;
-          for (int m = 0; m < kTcMats; ++m) {
-            tma_load_2d(st + c * kAChunk + m * kAMat, &maps.a[m], x, i0, &full[s]);
-            tma_load_2d(st + kABytesStage + c * kBChunk + m * kBMat, &maps.b[m], x, j0, &full[s]);
-          }
-        }
+        tma_load_4d(st, &maps.a, 0, i0, 0, kt * kChunksPerStage, &full[s]);
+        tma_load_4d(st + kABytesStage, &maps.b, 0, j0, 0, kt * kChunksPerStage, &full[s]);
       }
     }
   } else if (warp == 1) {
@@ -286,15 +309,15 @@ __global__ void __launch_bounds__(192, 1)
           const uint64_t bstack = smem_desc(bk, kBChunk, 128);  // [M; H; Mm; L; Qh; Qm; Ql] rows
           const uint32_t first = (kt == 0 && ks == 0) ? 0u : 1u;
           // D1: x limbs against [M; H; Mm; L]
-          mma_bf16(tmem + kD1, smem_desc(ak + 0 * kAMat, kAChunk, 128), bstack, id128, first);
-          mma_bf16(tmem + kD1, smem_desc(ak + 1 * kAMat, kAChunk, 128), bstack, id128, 1u);
+          mma_bf16(tmem + kD1, smem_desc(ak + 1 * kAMat, kAChunk, 128), bstack, id128, first);
           mma_bf16(tmem + kD1, smem_desc(ak + 2 * kAMat, kAChunk, 128), bstack, id128, 1u);
+          mma_bf16(tmem + kD1, smem_desc(ak + 3 * kAMat, kAChunk, 128), bstack, id128, 1u);
           // D2: mask against the whole stack
-          mma_bf16(tmem + kD2, smem_desc(ak + 6 * kAMat, kAChunk, 128), bstack, id224, first);
+          mma_bf16(tmem + kD2, smem_desc(ak + 0 * kAMat, kAChunk, 128), bstack, id224, first);
           // D3: x'^2 limbs against M
-          mma_bf16(tmem + kD3, smem_desc(ak + 3 * kAMat, kAChunk, 128), bstack, id32, first);
-          mma_bf16(tmem + kD3, smem_desc(ak + 4 * kAMat, kAChunk, 128), bstack, id32, 1u);
+          mma_bf16(tmem + kD3, smem_desc(ak + 4 * kAMat, kAChunk, 128), bstack, id32, first);
           mma_bf16(tmem + kD3, smem_desc(ak + 5 * kAMat, kAChunk, 128), bstack, id32, 1u);
+          mma_bf16(tmem + kD3, smem_desc(ak + 6 * kAMat, kAChunk, 128), bstack, id32, 1u);
         }
         mma_commit(&empty[s]);  // frees the stage when these MMAs complete
       }
@@ -414,7 +437,7 @@ size_t prec_tc_smem() { return kTcStages * kStageBytes + 1024 + 256; }
 
 cudaError_t launch_prec_prep(const float* X, const uint8_t* mask, int T, int N, int Np, int Tp, float* mu,
                              PrecOperands op, cudaStream_t s) {
-  k_prec_colmean<<<(N + 127) / 128, 128, 0, s>>>(X, mask, T, N, mu);
+  k_prec_colmean<<<(N + 31) / 32, dim3(32, 8), 0, s>>>(X, mask, T, N, mu);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   dim3 g((Tp + 31) / 32, (Np + 31) / 32), b(32, 8);
@@ -422,12 +445,16 @@ cudaError_t launch_prec_prep(const float* X, const uint8_t* mask, int T, int N, 
   return cudaGetLastError();
 }
 
-static CUresult make_map(CUtensorMap* map, const void* base, int Np, int Tp, int box_rows) {
-  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(Tp), static_cast<cuuint64_t>(Np)};
-  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(Tp) * 2};
-  const cuuint32_t box[2] = {8, static_cast<cuuint32_t>(box_rows)};
-  const cuuint32_t estr[2] = {1, 1};
-  return cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
+static CUresult make_map4(CUtensorMap* map, const void* base, int Np, int Tp, int box_rows) {
+  const cuuint64_t dims[4] = {8, static_cast<cuuint64_t>(Np), static_cast<cuuint64_t>(kTcMats),
+                              static_cast<cuuint64_t>(Tp / 8)};
+  const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Tp) * 2,                       // next row
+                                 static_cast<cuuint64_t>(Np) * static_cast<cuuint64_t>(Tp) * 2,  // next matrix
+                                 16};                                                    // next 8-date chunk
+  const cuuint32_t box[4] = {8, static_cast<cuuint32_t>(box_rows), static_cast<cuuint32_t>(kTcMats),
+                             static_cast<cuuint32_t>(kChunksPerStage)};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box,
                                 estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
@@ -435,12 +462,8 @@ static CUresult make_map(CUtensorMap* map, const void* base, int Np, int Tp, int
 cudaError_t launch_corr_bf16x3(const PrecOperands& op, const int2* tiles, int ntiles, int N, int Np, int Tp,
                                double* out, int* status, cudaStream_t s) {
   TcMaps maps;
-  const __nv_bfloat16* amats[kTcMats] = {op.h, op.mm, op.l, op.qh, op.qm, op.ql, op.m16};
-  const __nv_bfloat16* bmats[kTcMats] = {op.m16, op.h, op.mm, op.l, op.qh, op.qm, op.ql};
-  for (int m = 0; m < kTcMats; ++m) {
-    if (make_map(&maps.a[m], amats[m], Np, Tp, kTcM) != CUDA_SUCCESS) return cudaErrorInvalidValue;
-    if (make_map(&maps.b[m], bmats[m], Np, Tp, kTcN) != CUDA_SUCCESS) return cudaErrorInvalidValue;
-  }
+  if (make_map4(&maps.a, op.h, Np, Tp, kTcM) != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  if (make_map4(&maps.b, op.h, Np, Tp, kTcN) != CUDA_SUCCESS) return cudaErrorInvalidValue;
   const size_t smem = prec_tc_smem();
   cudaError_t e = cudaFuncSetAttribute(k_corr_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));

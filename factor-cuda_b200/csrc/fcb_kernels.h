@@ -38,6 +38,7 @@ struct RankIcArgs {
   const float* cdf_zrange;  // (F, 2) grid range [lo, hi] in standardised units
   int learn_cap;            // largest bucket the learned path accepts
   int* learn_stats;         // (F,T,4): outcome, largest bucket, sum of squared bucket sizes, m; or nullptr
+  int ic_ld;                // row stride of ic_out (0 = T)
 };
 
 struct ColStat {  // one stock_corr column
@@ -84,9 +85,8 @@ cudaError_t launch_cdf_tabulate(const float* params, const float2* samples, int 
 // Operands of the stock_corr precision forms, K-major (Np rows x Tp dates),
 // column-centred; unused members are nullptr.
 struct PrecOperands {
-  __nv_bfloat16 *h, *mm, *l;     // three bf16 limbs of x'
-  __nv_bfloat16 *qh, *qm, *ql;   // three bf16 limbs of x'^2
-  __nv_bfloat16* m16;            // 0/1 mask
+  __nv_bfloat16* h;  // [7][Np][Tp] bf16: mask, three limbs of x', three limbs of x'^2 (or nullptr)
+  int np;            // Np (row count of each plane)
   float *x32, *q32, *m32;        // FP32 x', x'^2, mask
 };
 

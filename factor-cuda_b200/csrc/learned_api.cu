@@ -197,10 +197,23 @@ extern "C" int fcb_cdf_grad(const float* params, const float* z, const float* u,
   return r;
 }
 
+namespace fcb {
+int rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d_fmask, const uint8_t* d_rmask, int F,
+                       int T, int N, int min_valid, float* d_ranks, double* d_ic, int ic_ld,
+                       const fcb_cdf_model* model, int cap, int* d_stats, cudaStream_t stream);
+}
+
 extern "C" int fcb_dev_rank_ic_panel_learned(const float* d_x, const float* d_r, const uint8_t* d_fmask,
                                              const uint8_t* d_rmask, int F, int T, int N, int min_valid,
                                              float* d_ranks, double* d_ic, const fcb_cdf_model* model, int cap,
                                              int* d_stats, void* stream) {
+  return fcb::rank_ic_learned_ld(d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, 0, model, cap,
+                                 d_stats, static_cast<cudaStream_t>(stream));
+}
+
+int fcb::rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d_fmask, const uint8_t* d_rmask,
+                            int F, int T, int N, int min_valid, float* d_ranks, double* d_ic, int ic_ld,
+                            const fcb_cdf_model* model, int cap, int* d_stats, cudaStream_t stream) {
   if (d_x == nullptr || d_r == nullptr || d_ic == nullptr || model == nullptr || F < 1 || T < 1 || N < 1)
     return FCB_ERR_ARG;
   if (F != model->F) return FCB_ERR_ARG;
@@ -210,6 +223,7 @@ extern "C" int fcb_dev_rank_ic_panel_learned(const float* d_x, const float* d_r,
   static int* d_status = nullptr;
   if (d_status == nullptr) FCB_TRY(cudaMalloc(&d_status, sizeof(int)));
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr,
-                             model->table[model->cur], model->zrange[model->cur], cap > 0 ? cap : 64, d_stats};
-  return rc(launch_rank_ic_learned(a, d_status, static_cast<cudaStream_t>(stream)));
+                             model->table[model->cur], model->zrange[model->cur], cap > 0 ? cap : 64, d_stats,
+                             ic_ld};
+  return rc(launch_rank_ic_learned(a, d_status, stream));
 }

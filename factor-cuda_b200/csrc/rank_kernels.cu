@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(Ra
         const bool rconst = GR[rfirst] == GR[rlast];
         if (!fconst && !rconst) ic = spearman_from_sum(m, sum);
       }
-      a.ic_out[static_cast<size_t>(f) * T + t] = ic;
+      a.ic_out[static_cast<size_t>(f) * (a.ic_ld > 0 ? a.ic_ld : T) + t] = ic;
     }
     __syncthreads();
     if (want_ranks) store_row_f32(a.ranks_out + frow, rbuf, N);
