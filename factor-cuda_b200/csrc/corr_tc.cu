@@ -17,9 +17,13 @@
 //                 the 9 limb products of sxy in three column blocks
 //   D2 (N=224)  = M . [M; H; Mm; L; Qh; Qm; Ql]^T             -> n | sy (3) | sy2 (3)
 //   D3 (N=32)  += q . M^T                for q in {Qh, Qm, Ql} -> sx2
-// Operands are staged by TMA (cp.async.bulk.tensor, no swizzle, no cluster
-// multicast) into the canonical K-major no-swizzle layout of 8-row x 16-byte
-// core matrices; one 4D box per operand fills a whole pipeline stage.  The FP64 finalize is
+// Operands are staged by TMA (cp.async.bulk.tensor, no cluster multicast) in
+// the canonical K-major 64-byte-swizzle layout: each stock row holds the stage's
+// 32 dates as one 64-byte line, 8-row groups 512 bytes apart, and the seven
+// matrices of an operand follow one another, so the stacked B operand is just
+// 224 consecutive rows.  One 3D box per operand fills a stage with full 64-byte
+// row reads (a 16-byte-wide box would fetch a 32-byte sector per 16 bytes used).
+// The FP64 finalize is
 //   cov = sxy - sx sy / n, vx = sx2 - sx^2/n, vy = sy2 - sy^2/n,
 //   r = (cov/sqrt(vx))/sqrt(vy),  NaN for n < 2 or a non-positive variance.
 #include <cuda.h>
@@ -36,13 +40,11 @@ constexpr int kTcN = 32;       // output columns per tile (stocks j)
 constexpr int kTcK = 32;       // k depth per pipeline stage
 constexpr int kTcStages = 3;
 constexpr int kTcMats = 7;     // operand matrices, order M H Mm L Qh Qm Ql
-constexpr int kChunksPerStage = kTcK / 8;
-constexpr int kAMat = kTcM * 16;                      // one A matrix, one 8-column k chunk
-constexpr int kBMat = kTcN * 16;                      // one B matrix, one k chunk
-constexpr int kAChunk = kTcMats * kAMat;              // all A matrices of one k chunk
-constexpr int kBChunk = kTcMats * kBMat;
-constexpr int kABytesStage = kChunksPerStage * kAChunk;
-constexpr int kBBytesStage = kChunksPerStage * kBChunk;
+constexpr int kRowBytes = kTcK * 2;                   // one stock's dates of a stage (64 B)
+constexpr int kAMat = kTcM * kRowBytes;               // one A matrix of a stage
+constexpr int kBMat = kTcN * kRowBytes;               // one B matrix of a stage
+constexpr int kABytesStage = kTcMats * kAMat;
+constexpr int kBBytesStage = kTcMats * kBMat;
 constexpr int kStageBytes = kABytesStage + kBBytesStage;
 constexpr int kD1 = 0, kD2 = 128, kD3 = 352;          // TMEM column of each accumulator
 constexpr int kTmemCols = 512;                        // 384 used, rounded to a power of two
@@ -137,13 +139,17 @@ __global__ void k_prec_split(const float* __restrict__ X, const uint8_t* __restr
 // ---------------------------------------------------------------------------
 // tcgen05 helpers
 // ---------------------------------------------------------------------------
-FCB_DEV uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+// Shared-memory matrix descriptor of a K-major operand in the 64-byte swizzle
+// layout: 64-byte rows, 8-row groups 512 bytes apart (stride byte offset), the
+// leading byte offset fixed at 16 bytes, layout type 4 (SWIZZLE_64B).  A 16-deep
+// k step inside the 32-date line starts 32 bytes further on.
+FCB_DEV uint64_t smem_desc_sw64(uint32_t saddr) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);
-  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
-  d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(16 >> 4) << 16;
+  d |= static_cast<uint64_t>(512 >> 4) << 32;
   d |= static_cast<uint64_t>(1) << 46;  // descriptor version (Blackwell)
-  // base offset 0, absolute-LBO mode off, layout type 0 = no swizzle
+  d |= static_cast<uint64_t>(4) << 61;  // SWIZZLE_64B; base offset 0
   return d;
 }
 
@@ -179,11 +185,11 @@ FCB_DEV void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64
       : "memory");
 }
 
-FCB_DEV void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, uint64_t* bar) {
+FCB_DEV void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
   asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-      "[%6];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
       : "memory");
 }
 
@@ -219,13 +225,11 @@ FCB_DEV void write_pair(double* out, int N, int i, int j, double r) {
 // BF16x3 tcgen05 kernel: one 128 x 32 output tile per CTA
 // warps: 0 TMA producer, 1 TMEM owner + MMA issuer, 2..5 epilogue
 // ---------------------------------------------------------------------------
-// One 4D view of the [7][Np][Tp] operand buffer: dims {8 dates, Np rows,
-// 7 matrices, Tp/8 chunks}.  A box {8, rows, 7, 4} lands in shared memory in
-// (chunk, matrix, row) order -- exactly the stacked core-matrix layout -- so
-// one TMA per operand fills a whole stage.
+// Two 3D views of the [7][Np][Tp] operand buffer (64-byte swizzle): one TMA
+// per operand fills a whole stage.
 struct TcMaps {
-  CUtensorMap a;  // box {8, 128, 7, 4}
-  CUtensorMap b;  // box {8, 32, 7, 4}
+  CUtensorMap a;  // box {32, 128, 7}
+  CUtensorMap b;  // box {32, 32, 7}
 };
 
 // sum of `nb` 16-column TMEM blocks spaced 32 columns apart, in f64
@@ -284,8 +288,8 @@ __global__ void __launch_bounds__(192, 1)
         }
         uint8_t* st = sm + s * kStageBytes;
         mbar_expect_tx(&full[s], kStageBytes);
-        tma_load_4d(st, &maps.a, 0, i0, 0, kt * kChunksPerStage, &full[s]);
-        tma_load_4d(st + kABytesStage, &maps.b, 0, j0, 0, kt * kChunksPerStage, &full[s]);
+        tma_load_3d(st, &maps.a, kt * kTcK, i0, 0, &full[s]);
+        tma_load_3d(st + kABytesStage, &maps.b, kt * kTcK, j0, 0, &full[s]);
       }
     }
   } else if (warp == 1) {
@@ -304,20 +308,19 @@ __global__ void __launch_bounds__(192, 1)
         const uint32_t bbase = abase + kABytesStage;
 #pragma unroll
         for (int ks = 0; ks < kTcK / 16; ++ks) {
-          const uint32_t ak = abase + 2 * ks * kAChunk;
-          const uint32_t bk = bbase + 2 * ks * kBChunk;
-          const uint64_t bstack = smem_desc(bk, kBChunk, 128);  // [M; H; Mm; L; Qh; Qm; Ql] rows
+          const uint32_t ak = abase + ks * 32;
+          const uint64_t bstack = smem_desc_sw64(bbase + ks * 32);  // [M; H; Mm; L; Qh; Qm; Ql] rows
           const uint32_t first = (kt == 0 && ks == 0) ? 0u : 1u;
           // D1: x limbs against [M; H; Mm; L]
-          mma_bf16(tmem + kD1, smem_desc(ak + 1 * kAMat, kAChunk, 128), bstack, id128, first);
-          mma_bf16(tmem + kD1, smem_desc(ak + 2 * kAMat, kAChunk, 128), bstack, id128, 1u);
-          mma_bf16(tmem + kD1, smem_desc(ak + 3 * kAMat, kAChunk, 128), bstack, id128, 1u);
+          mma_bf16(tmem + kD1, smem_desc_sw64(ak + 1 * kAMat), bstack, id128, first);
+          mma_bf16(tmem + kD1, smem_desc_sw64(ak + 2 * kAMat), bstack, id128, 1u);
+          mma_bf16(tmem + kD1, smem_desc_sw64(ak + 3 * kAMat), bstack, id128, 1u);
           // D2: mask against the whole stack
-          mma_bf16(tmem + kD2, smem_desc(ak + 0 * kAMat, kAChunk, 128), bstack, id224, first);
+          mma_bf16(tmem + kD2, smem_desc_sw64(ak + 0 * kAMat), bstack, id224, first);
           // D3: x'^2 limbs against M
-          mma_bf16(tmem + kD3, smem_desc(ak + 4 * kAMat, kAChunk, 128), bstack, id32, first);
-          mma_bf16(tmem + kD3, smem_desc(ak + 5 * kAMat, kAChunk, 128), bstack, id32, 1u);
-          mma_bf16(tmem + kD3, smem_desc(ak + 6 * kAMat, kAChunk, 128), bstack, id32, 1u);
+          mma_bf16(tmem + kD3, smem_desc_sw64(ak + 4 * kAMat), bstack, id32, first);
+          mma_bf16(tmem + kD3, smem_desc_sw64(ak + 5 * kAMat), bstack, id32, 1u);
+          mma_bf16(tmem + kD3, smem_desc_sw64(ak + 6 * kAMat), bstack, id32, 1u);
         }
         mma_commit(&empty[s]);  // frees the stage when these MMAs complete
       }
@@ -445,25 +448,27 @@ cudaError_t launch_prec_prep(const float* X, const uint8_t* mask, int T, int N, 
   return cudaGetLastError();
 }
 
-static CUresult make_map4(CUtensorMap* map, const void* base, int Np, int Tp, int box_rows) {
-  const cuuint64_t dims[4] = {8, static_cast<cuuint64_t>(Np), static_cast<cuuint64_t>(kTcMats),
-                              static_cast<cuuint64_t>(Tp / 8)};
-  const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Tp) * 2,                       // next row
-                                 static_cast<cuuint64_t>(Np) * static_cast<cuuint64_t>(Tp) * 2,  // next matrix
-                                 16};                                                    // next 8-date chunk
-  const cuuint32_t box[4] = {8, static_cast<cuuint32_t>(box_rows), static_cast<cuuint32_t>(kTcMats),
-                             static_cast<cuuint32_t>(kChunksPerStage)};
-  const cuuint32_t estr[4] = {1, 1, 1, 1};
-  return cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box,
-                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+// 3D map over the [7][Np][Tp] operand block: dims {Tp dates, Np stocks, 7
+// matrices}; a box {32, rows, 7} is one stage of one operand, landing as
+// (matrix, row, 64-byte swizzled line).
+static CUresult make_map3(CUtensorMap* map, const void* base, int Np, int Tp, int box_rows) {
+  const cuuint64_t dims[3] = {static_cast<cuuint64_t>(Tp), static_cast<cuuint64_t>(Np),
+                              static_cast<cuuint64_t>(kTcMats)};
+  const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Tp) * 2,                                 // next stock
+                                 static_cast<cuuint64_t>(Np) * static_cast<cuuint64_t>(Tp) * 2};  // next matrix
+  const cuuint32_t box[3] = {static_cast<cuuint32_t>(kTcK), static_cast<cuuint32_t>(box_rows),
+                             static_cast<cuuint32_t>(kTcMats)};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box,
+                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
 cudaError_t launch_corr_bf16x3(const PrecOperands& op, const int2* tiles, int ntiles, int N, int Np, int Tp,
                                double* out, int* status, cudaStream_t s) {
   TcMaps maps;
-  if (make_map4(&maps.a, op.h, Np, Tp, kTcM) != CUDA_SUCCESS) return cudaErrorInvalidValue;
-  if (make_map4(&maps.b, op.h, Np, Tp, kTcN) != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  if (make_map3(&maps.a, op.h, Np, Tp, kTcM) != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  if (make_map3(&maps.b, op.h, Np, Tp, kTcN) != CUDA_SUCCESS) return cudaErrorInvalidValue;
   const size_t smem = prec_tc_smem();
   cudaError_t e = cudaFuncSetAttribute(k_corr_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
