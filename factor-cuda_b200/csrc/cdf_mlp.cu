@@ -282,7 +282,11 @@ __global__ void __launch_bounds__(512) k_cdf_range(const float2* __restrict__ sa
 }
 
 // Tabulate u(z) on kCdfKnots uniform knots over [lo, hi]; cummax makes it
-// monotone.  One block per factor.
+// monotone, and a small linear share (kCdfLinearShare of the buckets spread
+// uniformly over the knots) keeps a floor of buckets in every knot interval:
+// where the network's sigmoid saturates in a heavy tail (u within 1e-3 of 0 or
+// 1 over a wide z range) the tail cells would otherwise crowd into one bucket.
+// One block per factor.
 __global__ void __launch_bounds__(256) k_cdf_tabulate(const float* __restrict__ params, const float* __restrict__ zrange,
                                                       float* __restrict__ table) {
   const int f = blockIdx.x;
@@ -313,7 +317,7 @@ __global__ void __launch_bounds__(256) k_cdf_tabulate(const float* __restrict__ 
     float run = 0.0f;
     for (int k = 0; k < kCdfKnots; ++k) {
       run = fmaxf(run, u[k]);
-      u[k] = run;
+      u[k] = (1.0f - kCdfLinearShare) * run + kCdfLinearShare * (static_cast<float>(k) / (kCdfKnots - 1));
     }
   }
   __syncthreads();

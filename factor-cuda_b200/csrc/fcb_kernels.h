@@ -16,6 +16,8 @@ constexpr int kSmemRankCap = 16384;
 constexpr int kCdfHidden = 32;
 constexpr int kCdfParams = 1 + 1 * 32 + 32 + 32 * 32 + 32 + 32;  // W1,b1,W2,b2,w3,b3 = 1153
 constexpr int kCdfKnots = 1024;
+// Share of the buckets the tabulated CDF spreads uniformly over its knots.
+constexpr float kCdfLinearShare = 0.03f;
 constexpr size_t kMaxSmemPerBlock = 227 * 1024;
 
 struct ScanOut {

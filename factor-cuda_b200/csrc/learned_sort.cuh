@@ -48,27 +48,61 @@ FCB_DEV uint32_t packed_inc(uint16_t* arr, int b) {
   return (old >> sh) & 0xFFFFu;
 }
 
+// Block-wide sum by xor shuffles: one shared slot per warp, every thread adds
+// the warp totals.  scratch: >= 32 T.  All threads must call.
+template <typename T>
+FCB_DEV T block_reduce_add(T v, T* scratch) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane_id() == 0) scratch[w] = v;
+  __syncthreads();
+  T t = T(0);
+  for (int i = 0; i < nw; ++i) t += scratch[i];
+  __syncthreads();
+  return t;
+}
+
 // Outcome codes written to the per-(factor,date) statistics.
 constexpr int kLearnOk = 1, kLearnOverflow = 2, kLearnJudge = 3, kLearnScale = 4;
+
+// Start and end of the bucket holding sorted position q, from the bitmap of
+// bucket starts (bit p set <=> a non-empty bucket starts at p; bit 0 is always
+// set).  Buckets hold at most `cap` (<= 64) cells, so each scan is short.
+FCB_DEV void bucket_bounds(const uint32_t* bits, int q, int m, int& lo, int& hi) {
+  int w = q >> 5;
+  const int sh = q & 31;
+  uint32_t x = bits[w] & (0xFFFFFFFFu >> (31 - sh));  // starts at or before q
+  while (x == 0u) x = bits[--w];
+  lo = w * 32 + 31 - __clz(x);
+  w = q >> 5;
+  x = (sh == 31) ? 0u : (bits[w] & (0xFFFFFFFFu << (sh + 1)));  // starts after q
+  while (x == 0u && (w + 1) * 32 < m) x = bits[++w];
+  hi = (x != 0u) ? min(m, w * 32 + __ffs(x) - 1) : m;
+}
 
 // Sort the m compacted pairs (kA, iA) with the bucket map.  On success the
 // sorted sequence is in (kA, iA) and the return is kLearnOk.  kLearnOverflow /
 // kLearnScale leave (kA, iA) untouched; kLearnJudge leaves them permuted (the
-// caller must rebuild them before falling back).  cnt: u16 array of at least
-// m+2 entries, 4-byte aligned.  dscratch: >= 66 doubles; scan: >= 33 u32.
-template <int NT>
+// caller must rebuild them before falling back).
+//   cnt:   u16 array of at least m+2 entries, 4-byte aligned (bucket counters)
+//   bits:  u32 bitmap of at least m/32+2 words (bucket starts)
+//   fscratch: >= 32 doubles; scan: >= 33 u32.
+// The bucket of each cell is evaluated once (histogram pass) and parked in iB,
+// which is idle until the scatter; the scatter reads it back into registers.
+template <int NT, int MAXIPT>
 FCB_DEV int learned_sort(uint32_t* kA, uint16_t* iA, uint32_t* kB, uint16_t* iB, int m, uint16_t* cnt,
-                         const float* tab, float lo, float hi, int cap, double* dscratch, uint32_t* scan,
-                         int* max_bucket_out, int* sumsq_out) {
+                         uint32_t* bits, const float* tab, float lo, float hi, int cap, double* dscratch,
+                         uint32_t* scan, int* max_bucket_out, int* sumsq_out) {
   if (m <= 1) return kLearnOk;
   // per-date standardisation: mean and mean absolute deviation of the values
   double s = 0.0;
   for (int p = threadIdx.x; p < m; p += NT) s += key_to_f32(kA[p]);
-  s = block_sum(s, dscratch);
+  s = block_reduce_add(s, dscratch);
   const double mean = s / m;
   double a = 0.0;
   for (int p = threadIdx.x; p < m; p += NT) a += fabs(key_to_f32(kA[p]) - mean);
-  a = block_sum(a, dscratch);
+  a = block_reduce_add(a, dscratch);
   const double mad = a / m;
   BucketMap bm;
   bm.tab = tab;
@@ -81,56 +115,79 @@ FCB_DEV int learned_sort(uint32_t* kA, uint16_t* iA, uint32_t* kB, uint16_t* iB,
   if (!(mad > 0.0) || !isfinite(bm.loc) || !isfinite(bm.inv_scale) || !(bm.inv_scale > 0.0f) ||
       !isfinite(bm.inv_dz) || !(bm.inv_dz > 0.0f))
     return kLearnScale;
-  // histogram (packed 16-bit counters)
+  // histogram (packed 16-bit counters); each cell's bucket parked in iB
+  const int nwords = (m >> 5) + 2;
   for (int b = threadIdx.x; b < (m + 2) / 2; b += NT) reinterpret_cast<uint32_t*>(cnt)[b] = 0u;
+  for (int w = threadIdx.x; w < nwords; w += NT) bits[w] = 0u;
   __syncthreads();
-  for (int p = threadIdx.x; p < m; p += NT) packed_inc(cnt, bm(kA[p]));
+  for (int p = threadIdx.x; p < m; p += NT) {
+    const int b = bm(kA[p]);
+    packed_inc(cnt, b);
+    iB[p] = static_cast<uint16_t>(b);
+  }
   __syncthreads();
-  // largest bucket
-  int mx = 0;
-  for (int b = threadIdx.x; b < m; b += NT) mx = max(mx, static_cast<int>(cnt[b]));
-  mx = block_max_int(mx, reinterpret_cast<int*>(scan));
-  if (max_bucket_out != nullptr) *max_bucket_out = mx;
-  if (mx > cap) return kLearnOverflow;
-  // exclusive scan of the counts -> bucket starts (in place)
+  // exclusive scan of the counts -> bucket starts (in place), largest bucket,
+  // sum of squared sizes, bitmap of bucket starts
   {
     const int per = (m + NT - 1) / NT;
     const int b0 = threadIdx.x * per, b1 = min(m, b0 + per);
     uint32_t c = 0, c2 = 0;
+    int mx = 0;
     for (int b = b0; b < b1; ++b) {
-      c += cnt[b];
-      c2 += static_cast<uint32_t>(cnt[b]) * cnt[b];
+      const uint32_t v = cnt[b];
+      c += v;
+      c2 += v * v;
+      mx = max(mx, static_cast<int>(v));
     }
-    c2 = block_sum(c2, scan);
+    mx = block_max_int(mx, reinterpret_cast<int*>(scan));
+    if (max_bucket_out != nullptr) *max_bucket_out = mx;
+    if (mx > cap) return kLearnOverflow;  // uniform across the block
+    c2 = block_reduce_add(c2, scan);
     if (sumsq_out != nullptr) *sumsq_out = static_cast<int>(c2);
     uint32_t total;
     uint32_t run = block_exclusive_sum(c, scan, total);
     for (int b = b0; b < b1; ++b) {
       const uint32_t v = cnt[b];
       cnt[b] = static_cast<uint16_t>(run);
+      if (v != 0u) atomicOr(&bits[run >> 5], 1u << (run & 31));
       run += v;
     }
     __syncthreads();
   }
   // scatter into bucket slots (order inside a bucket is arbitrary)
-  for (int p = threadIdx.x; p < m; p += NT) {
-    const uint32_t key = kA[p];
-    const uint32_t pos = packed_inc(cnt, bm(key));
-    kB[pos] = key;
-    iB[pos] = iA[p];
+  {
+    uint32_t breg[(MAXIPT + 1) / 2];
+#pragma unroll
+    for (int j = 0; j < MAXIPT; j += 2) {
+      const int p0 = threadIdx.x + j * NT, p1 = p0 + NT;
+      const uint32_t b0 = p0 < m ? iB[p0] : 0u;
+      const uint32_t b1 = (j + 1 < MAXIPT && p1 < m) ? iB[p1] : 0u;
+      breg[j >> 1] = b0 | (b1 << 16);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < MAXIPT; ++j) {
+      const int p = threadIdx.x + j * NT;
+      if (p < m) {
+        const int b = static_cast<int>((breg[j >> 1] >> ((j & 1) * 16)) & 0xFFFFu);
+        const uint32_t pos = packed_inc(cnt, b);
+        kB[pos] = kA[p];
+        iB[pos] = iA[p];
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  // rank inside the bucket by (key, column); cnt[b] now holds bucket b's end
+  // rank inside the bucket by (key, column): keys first, column ids on ties
   for (int q = threadIdx.x; q < m; q += NT) {
     const uint32_t key = kB[q];
     const uint16_t id = iB[q];
-    const int b = bm(key);
-    const int lo_b = b == 0 ? 0 : cnt[b - 1];
-    const int hi_b = cnt[b];
+    int lo_b, hi_b;
+    bucket_bounds(bits, q, m, lo_b, hi_b);
     int r = 0;
     for (int s2 = lo_b; s2 < hi_b; ++s2) {
       const uint32_t k2 = kB[s2];
-      r += (k2 < key || (k2 == key && iB[s2] < id)) ? 1 : 0;
+      r += (k2 < key) ? 1 : 0;
+      if (k2 == key) r += (iB[s2] < id) ? 1 : 0;
     }
     kA[lo_b + r] = key;
     iA[lo_b + r] = id;
