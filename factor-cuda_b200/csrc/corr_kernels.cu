@@ -410,7 +410,9 @@ cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const d
 }
 
 // ---------------------------------------------------------------------------
-// factor_corr: rows r = t*N+i of a (T,N,F) panel, F <= 128 columns
+// factor_corr: rows r = t*N+i, F <= 128 columns; element (r, f) at
+// X[r*sr + f*sf] -- (sr, sf) = (F, 1) for a (T,N,F) panel (the reference's
+// layout), (1, T*N) for F stacked (T,N) factor planes.
 // ---------------------------------------------------------------------------
 
 // Per-block column partials over a contiguous row range: count, Kahan sum,
@@ -418,14 +420,14 @@ cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const d
 // strided slice; partials are merged in a fixed order by k_fc_colfinal.
 template <typename TIN>
 __global__ void k_fc_colpart(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
-                             long long rows_per_block, FcColPart* __restrict__ part) {
+                             long long sr, long long sf, long long rows_per_block, FcColPart* __restrict__ part) {
   const long long r0 = blockIdx.x * rows_per_block;
   const long long r1 = min(R, r0 + rows_per_block);
   for (int f = threadIdx.y; f < F; f += blockDim.y) {
     Kahan k;
     double cnt = 0.0, mn = kBigPos, mx = -kBigPos;
     for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-      const double x = static_cast<double>(X[r * F + f]);
+      const double x = static_cast<double>(X[r * sr + f * sf]);
       if (finite_f64(x) && (mask == nullptr || mask[r] != 0)) {
         cnt += 1.0;
         k.add(x);
@@ -491,7 +493,8 @@ constexpr int kFcRowsChunk = 32;
 
 template <typename TIN>
 __global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
-                                                 long long R, int F, int Fp, long long rows_per_block,
+                                                 long long R, int F, long long sr, long long sf, int Fp,
+                                                 long long rows_per_block,
                                                  const FcColStat* __restrict__ st, int tasks_total,
                                                  int tasks_per_block, double* __restrict__ part) {
   extern __shared__ __align__(16) double fsm[];
@@ -522,19 +525,22 @@ __global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, cons
   for (long long c0 = r0; c0 < r1; c0 += kFcRowsChunk) {
     const int nr = static_cast<int>(min(static_cast<long long>(kFcRowsChunk), r1 - c0));
     for (int e = threadIdx.x; e < kFcRowsChunk * Fp; e += 256) {
-      const int rr = e / Fp, f = e % Fp;
+      // consecutive threads read consecutive elements of X in either layout
+      const int rr = (sf == 1) ? e / Fp : e % kFcRowsChunk;
+      const int f = (sf == 1) ? e % Fp : e / kFcRowsChunk;
+      const int ei = rr * Fp + f;
       double v = 0.0, mv = 0.0;
       if (rr < nr && f < F) {
         const long long r = c0 + rr;
-        const double x = static_cast<double>(X[r * F + f]);
+        const double x = static_cast<double>(X[r * sr + f * sf]);
         if (finite_f64(x) && (mask == nullptr || mask[r] != 0)) {
           v = x - st[f].mean;
           mv = 1.0;
         }
       }
-      sx[e] = v;
-      sm[e] = mv;
-      sq[e] = v * v;
+      sx[ei] = v;
+      sm[ei] = mv;
+      sq[ei] = v * v;
     }
     __syncthreads();
     if (active) {
@@ -620,8 +626,8 @@ __global__ void k_fc_final(const double* __restrict__ part, int nblk, int F, int
 // tree (the reference's kahan_reduce kernels, src/factor_corr.cu:188-322).
 template <typename TIN>
 __global__ void k_fc_fallback(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
-                              const int* __restrict__ fb_list, const int* __restrict__ fb_count,
-                              double* __restrict__ out) {
+                              long long sr, long long sf, const int* __restrict__ fb_list,
+                              const int* __restrict__ fb_count, double* __restrict__ out) {
   if (static_cast<int>(blockIdx.x) >= *fb_count) return;
   const int e = fb_list[blockIdx.x];
   const int i = e / F, j = e % F;
@@ -634,8 +640,8 @@ __global__ void k_fc_fallback(const TIN* __restrict__ X, const uint8_t* __restri
     // idle threads still take part in the barriers below
   }
   auto valid = [&](long long r, double& x, double& y) {
-    x = static_cast<double>(X[r * F + i]);
-    y = static_cast<double>(X[r * F + j]);
+    x = static_cast<double>(X[r * sr + i * sf]);
+    y = static_cast<double>(X[r * sr + j * sf]);
     return finite_f64(x) && finite_f64(y) && (mask == nullptr || mask[r] != 0);
   };
   Kahan kx, ky;
@@ -748,8 +754,9 @@ size_t fc_gram_smem(int Fp, int tasks_per_block) {
          sizeof(double);
 }
 
-cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
-                               double* out, uint8_t* flags, cudaStream_t s) {
+cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* mask, long long R, int F,
+                                       long long sr, long long sf, FcWork& w, double* out, uint8_t* flags,
+                                       cudaStream_t s) {
   const int Fp = (F + 3) / 4 * 4;
   const int tb = Fp / 4;
   const int tasks_total = 4 * tb * tb;
@@ -759,9 +766,11 @@ cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, lo
   const long long rpb_gram = (R + w.nblk_gram - 1) / w.nblk_gram;
   dim3 cb(32, 8);
   if (dtype == 0)
-    k_fc_colpart<float><<<w.nblk_cols, cb, 0, s>>>(static_cast<const float*>(X), mask, R, F, rpb_cols, w.colpart);
+    k_fc_colpart<float><<<w.nblk_cols, cb, 0, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, rpb_cols,
+                                                   w.colpart);
   else
-    k_fc_colpart<double><<<w.nblk_cols, cb, 0, s>>>(static_cast<const double*>(X), mask, R, F, rpb_cols, w.colpart);
+    k_fc_colpart<double><<<w.nblk_cols, cb, 0, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf, rpb_cols,
+                                                    w.colpart);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_fc_colfinal<<<(F + 127) / 128, 128, 0, s>>>(w.colpart, w.nblk_cols, F, w.colstat);
@@ -771,13 +780,13 @@ cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, lo
   if (dtype == 0) {
     e = cudaFuncSetAttribute(k_fc_gram<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    k_fc_gram<float><<<gg, 256, smem, s>>>(static_cast<const float*>(X), mask, R, F, Fp, rpb_gram, w.colstat,
-                                           tasks_total, tasks_per_block, w.gram);
+    k_fc_gram<float><<<gg, 256, smem, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, Fp, rpb_gram,
+                                           w.colstat, tasks_total, tasks_per_block, w.gram);
   } else {
     e = cudaFuncSetAttribute(k_fc_gram<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    k_fc_gram<double><<<gg, 256, smem, s>>>(static_cast<const double*>(X), mask, R, F, Fp, rpb_gram, w.colstat,
-                                            tasks_total, tasks_per_block, w.gram);
+    k_fc_gram<double><<<gg, 256, smem, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf, Fp, rpb_gram,
+                                            w.colstat, tasks_total, tasks_per_block, w.gram);
   }
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(w.fb_count, 0, sizeof(int), s)) != cudaSuccess) return e;
@@ -786,12 +795,17 @@ cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, lo
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const int maxpairs = F * (F - 1) / 2 > 0 ? F * (F - 1) / 2 : 1;
   if (dtype == 0)
-    k_fc_fallback<float><<<maxpairs, 256, 0, s>>>(static_cast<const float*>(X), mask, R, F, w.fb_list, w.fb_count,
-                                                  out);
+    k_fc_fallback<float><<<maxpairs, 256, 0, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, w.fb_list,
+                                                  w.fb_count, out);
   else
-    k_fc_fallback<double><<<maxpairs, 256, 0, s>>>(static_cast<const double*>(X), mask, R, F, w.fb_list,
+    k_fc_fallback<double><<<maxpairs, 256, 0, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf, w.fb_list,
                                                    w.fb_count, out);
   return cudaGetLastError();
+}
+
+cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
+                               double* out, uint8_t* flags, cudaStream_t s) {
+  return launch_factor_corr_strided(X, dtype, mask, R, F, F, 1, w, out, flags, s);
 }
 
 }  // namespace fcb

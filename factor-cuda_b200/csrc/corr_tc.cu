@@ -29,6 +29,7 @@
 #include <cuda.h>
 
 #include <cmath>
+#include <mutex>
 
 #include "fcb_common.cuh"
 #include "fcb_kernels.h"
@@ -448,6 +449,26 @@ cudaError_t launch_prec_prep(const float* X, const uint8_t* mask, int T, int N, 
   return cudaGetLastError();
 }
 
+// cuTensorMapEncodeTiled is a driver-API call; it is resolved at run time
+// through the runtime's entry-point query so that the library does not link
+// libcuda and loads on hosts without a GPU driver.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
 // 3D map over the [7][Np][Tp] operand block: dims {Tp dates, Np stocks, 7
 // matrices}; a box {32, rows, 7} is one stage of one operand, landing as
 // (matrix, row, 64-byte swizzled line).
@@ -459,7 +480,9 @@ static CUresult make_map3(CUtensorMap* map, const void* base, int Np, int Tp, in
   const cuuint32_t box[3] = {static_cast<cuuint32_t>(kTcK), static_cast<cuuint32_t>(box_rows),
                              static_cast<cuuint32_t>(kTcMats)};
   const cuuint32_t estr[3] = {1, 1, 1};
-  return cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box,
+  const EncodeTiledFn encode = encode_tiled();
+  if (encode == nullptr) return CUDA_ERROR_NOT_SUPPORTED;
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box,
                                 estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }

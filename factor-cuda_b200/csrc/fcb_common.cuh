@@ -125,6 +125,10 @@ FCB_DEV T* stage_issue(uint8_t* region, const T* src, int n, uint64_t* bar, bool
     const int i0 = static_cast<int>((a0 - s) / sizeof(T));
     const int i1 = static_cast<int>((a1 - s) / sizeof(T));
     if (threadIdx.x == 0) {
+      // the region was last touched by ordinary loads/stores (made visible to
+      // this thread by the caller's barrier): order them before the copy's
+      // async-proxy writes
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(bar, static_cast<uint32_t>(a1 - a0));
       bulk_g2s(dst + i0, src + i0, static_cast<uint32_t>(a1 - a0), bar);
     }

@@ -111,5 +111,17 @@ cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const d
 size_t fc_gram_smem(int Fp, int tasks_per_block);
 cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
                                double* out, uint8_t* flags, cudaStream_t s);
+// Persistent rank+IC over (panel, date) items; nt in {256, 512, 1024}.  With
+// occ != nullptr nothing is launched: *occ receives the CTAs per SM that fit.
+template <typename TF, typename TR>
+size_t rank_ic_batch_smem(int nt, int maxN);
+template <typename TF, typename TR>
+cudaError_t launch_rank_ic_batch(int nt, bool learned, const RankIcArgs<TF, TR>* panels, const int2* items,
+                                 int nitems, int* counter, int grid, size_t smem, int* status, cudaStream_t st,
+                                 int* occ);
+// Same with element (r, f) at X[r*sr + f*sf].
+cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* mask, long long R, int F,
+                                       long long sr, long long sf, FcWork& w, double* out, uint8_t* flags,
+                                       cudaStream_t s);
 
 }  // namespace fcb

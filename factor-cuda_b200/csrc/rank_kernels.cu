@@ -17,6 +17,8 @@
 //                 (sum r_f*r_r in int64) with one f64 finalize.  Semantics of
 //                 rolling_ic_gpu (src/rolling_ic.cu:306-540) / np_rolling_ic
 //                 (fc/_cpu_core.py:271-293).
+#include <type_traits>
+
 #include "block_sort.cuh"
 #include "fcb_kernels.h"
 #include "learned_sort.cuh"
@@ -307,19 +309,31 @@ FCB_DEV double spearman_from_sum(long long m, long long sum_rr) {
   return (sxy / sqrt(sxx)) / sqrt(sxx);
 }
 
+// The four staging barriers sit at the start of every rank+IC layout.
+FCB_DEV void rank_ic_cta_init(uint8_t* sm) {
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm);
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < 4; ++b) mbar_init(&bars[b], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+}
+
+// One date t of one panel: sort the returns, then rank every factor and
+// evaluate its IC.  `ph` carries the staging barriers' phase bits from one
+// call to the next (persistent CTAs process many dates).  Returns false when a
+// staged copy did not land (status set); all threads return together.
 template <int NT, int MAXIPT, typename TF, typename TR, bool LEARNED>
-__global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(RankIcArgs<TF, TR> a, int* status) {
+FCB_DEV bool rank_ic_date(const RankIcArgs<TF, TR>& a, const int t, uint8_t* sm, uint32_t* ph, int* status) {
   using KF = typename KeyOf<TF>::type;
   using KR = typename KeyOf<TR>::type;
   constexpr int KSZ = (sizeof(KF) > sizeof(KR)) ? int(sizeof(KF)) : int(sizeof(KR));
-  extern __shared__ __align__(16) uint8_t sm[];
   const int N = a.N, T = a.T;
   const RankIcLayout L(N, KSZ, SortScratch<NT>::bytes);
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L.bars);
   uint32_t* scan = reinterpret_cast<uint32_t*>(sm + L.scratch + SortScratch<NT>::hist_bytes +
                                                SortScratch<NT>::base_bytes);
   unsigned long long* scan64 = reinterpret_cast<unsigned long long*>(scan);
-  const int t = blockIdx.x;
   const size_t row = static_cast<size_t>(t) * N;
   uint8_t* flags = sm + L.flags;
   uint16_t* IR = reinterpret_cast<uint16_t*>(sm + L.ir);
@@ -328,12 +342,6 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(Ra
   uint16_t* i0 = reinterpret_cast<uint16_t*>(sm + L.i0);
   uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
 
-  if (threadIdx.x == 0) {
-    for (int b = 0; b < 4; ++b) mbar_init(&bars[b], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  uint32_t ph[4] = {0, 0, 0, 0};
   bool arm[4] = {false, false, false, false};
 
   // ---- stage forward returns and both masks; flags bit0 = return valid, bit1 = factor mask
@@ -347,7 +355,7 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(Ra
   ok = stage_wait(&bars[2], ph[2], arm[2]) && ok;
   if (__syncthreads_or(!ok)) {
     if (threadIdx.x == 0) atomicExch(status, 1);
-    return;
+    return false;
   }
   for (int i = threadIdx.x; i < N; i += NT) {
     const bool rv = KeyOf<TR>::finite(r[i]) && (rm == nullptr || rm[i] != 0);
@@ -375,7 +383,7 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(Ra
     ok = stage_wait(&bars[3], ph[3], arm[3]);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) atomicExch(status, 1);
-      return;
+      return false;
     }
     for (int i = threadIdx.x; i < N; i += NT)
       flags[i] = static_cast<uint8_t>((flags[i] & 3u) | (KeyOf<TF>::finite(x[i]) ? 4u : 0u));
@@ -388,7 +396,7 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(Ra
     KF* kfs = kf0;
     uint16_t* ifs = i0;
     bool sorted = false;
-    if constexpr (LEARNED) {
+    if (LEARNED && a.cdf_table != nullptr) {
       // the radix histogram and digit-base regions are idle here: they hold
       // this factor's table and the bitmap of bucket starts
       using S = SortScratch<NT>;
@@ -420,7 +428,7 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(Ra
         ok = stage_wait(&bars[3], ph[3], arm[3]);
         if (__syncthreads_or(!ok)) {
           if (threadIdx.x == 0) atomicExch(status, 1);
-          return;
+          return false;
         }
         (void)compact_keys<KF>(
             N, [&](int i) { return (flags[i] & 6u) == 6u; }, [&](int i) { return KeyOf<TF>::key(x[i]); }, kf0, i0,
@@ -494,6 +502,39 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(Ra
     __syncthreads();
     if (want_ranks) store_row_f32(a.ranks_out + frow, rbuf, N);
     __syncthreads();
+  }
+  return true;
+}
+
+template <int NT, int MAXIPT, typename TF, typename TR, bool LEARNED>
+__global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(RankIcArgs<TF, TR> a, int* status) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  rank_ic_cta_init(sm);
+  uint32_t ph[4] = {0, 0, 0, 0};
+  (void)rank_ic_date<NT, MAXIPT, TF, TR, LEARNED>(a, blockIdx.x, sm, ph, status);
+}
+
+// Persistent rank+IC over many panels: each CTA takes (panel, date) items
+// from a device queue until it is empty.  items[k] = (panel index, date); the
+// panels' N must all fit this block size (N <= NT * MAXIPT) and the dynamic
+// shared memory was sized for the largest of them.
+template <int NT, int MAXIPT, typename TF, typename TR, bool LEARNED>
+__global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT))
+    k_rank_ic_batch(const RankIcArgs<TF, TR>* __restrict__ panels, const int2* __restrict__ items, int nitems,
+                    int* __restrict__ counter, int* __restrict__ status) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  __shared__ int s_item;
+  rank_ic_cta_init(sm);
+  uint32_t ph[4] = {0, 0, 0, 0};
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= nitems) break;
+    const int2 w = items[it];
+    const RankIcArgs<TF, TR> a = panels[w.x];
+    if (!rank_ic_date<NT, MAXIPT, TF, TR, LEARNED>(a, w.y, sm, ph, status)) break;
   }
 }
 
@@ -595,5 +636,58 @@ template cudaError_t launch_rank_ic<float, float>(const RankIcArgs<float, float>
 template cudaError_t launch_rank_ic<float, double>(const RankIcArgs<float, double>&, int*, cudaStream_t);
 template cudaError_t launch_rank_ic<double, float>(const RankIcArgs<double, float>&, int*, cudaStream_t);
 template cudaError_t launch_rank_ic<double, double>(const RankIcArgs<double, double>&, int*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// persistent batch launchers
+// ---------------------------------------------------------------------------
+template <typename TF, typename TR>
+size_t rank_ic_batch_smem(int nt, int maxN) {
+  constexpr int KSZ = (sizeof(TF) > sizeof(TR)) ? int(sizeof(TF)) : int(sizeof(TR));
+  switch (nt) {
+    case 256: return RankIcLayout(maxN, KSZ, SortScratch<256>::bytes).total;
+    case 512: return RankIcLayout(maxN, KSZ, SortScratch<512>::bytes).total;
+    default: return RankIcLayout(maxN, KSZ, SortScratch<1024>::bytes).total;
+  }
+}
+
+template <int NT, typename TF, typename TR, bool LEARNED>
+static cudaError_t batch_nt(const RankIcArgs<TF, TR>* panels, const int2* items, int nitems, int* counter,
+                            int grid, size_t smem, int* status, cudaStream_t st, int* occ) {
+  auto* k = k_rank_ic_batch<NT, 16, TF, TR, LEARNED>;
+  if (smem > kMaxSmemPerBlock) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  if (occ != nullptr) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, NT, smem);
+  k<<<grid, NT, smem, st>>>(panels, items, nitems, counter, status);
+  return cudaGetLastError();
+}
+
+template <typename TF, typename TR>
+cudaError_t launch_rank_ic_batch(int nt, bool learned, const RankIcArgs<TF, TR>* panels, const int2* items,
+                                 int nitems, int* counter, int grid, size_t smem, int* status, cudaStream_t st,
+                                 int* occ) {
+  if (learned) {
+    if constexpr (std::is_same<TF, float>::value && std::is_same<TR, float>::value) {
+      switch (nt) {
+        case 256: return batch_nt<256, TF, TR, true>(panels, items, nitems, counter, grid, smem, status, st, occ);
+        case 512: return batch_nt<512, TF, TR, true>(panels, items, nitems, counter, grid, smem, status, st, occ);
+        default: return batch_nt<1024, TF, TR, true>(panels, items, nitems, counter, grid, smem, status, st, occ);
+      }
+    } else {
+      return cudaErrorInvalidValue;
+    }
+  }
+  switch (nt) {
+    case 256: return batch_nt<256, TF, TR, false>(panels, items, nitems, counter, grid, smem, status, st, occ);
+    case 512: return batch_nt<512, TF, TR, false>(panels, items, nitems, counter, grid, smem, status, st, occ);
+    default: return batch_nt<1024, TF, TR, false>(panels, items, nitems, counter, grid, smem, status, st, occ);
+  }
+}
+template size_t rank_ic_batch_smem<float, float>(int, int);
+template size_t rank_ic_batch_smem<double, double>(int, int);
+template cudaError_t launch_rank_ic_batch<float, float>(int, bool, const RankIcArgs<float, float>*, const int2*, int,
+                                                         int*, int, size_t, int*, cudaStream_t, int*);
+template cudaError_t launch_rank_ic_batch<double, double>(int, bool, const RankIcArgs<double, double>*, const int2*,
+                                                           int, int*, int, size_t, int*, cudaStream_t, int*);
 
 }  // namespace fcb

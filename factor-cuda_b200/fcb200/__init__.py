@@ -18,6 +18,7 @@ forward-return panel in one call), ``workspace_stats``.
 """
 from __future__ import annotations
 
+import ctypes as C
 import threading
 import time
 from contextlib import contextmanager
@@ -33,7 +34,8 @@ except Exception:  # pragma: no cover
 
 __version__ = "1.0.0"
 __all__ = ["cross_sectional_rank", "factor_plane", "factor_corr", "stock_corr", "rolling_ic",
-           "parameter_scan", "rank_ic_panel", "Workspace", "CdfModel", "clear_workspaces", "__version__"]
+           "parameter_scan", "rank_ic_panel", "Workspace", "CdfModel", "Batch", "clear_workspaces",
+           "__version__"]
 
 _WHITELIST = (np.float32, np.float64)
 DOMAIN_MSG = ("correlation domain violation: max|x| > 1e150 or a nonzero |x| < 1e-150 "
@@ -518,3 +520,102 @@ def cdf_grad(params, z, u):
     nat.check(nat.lib().fcb_cdf_grad(nat.ptr(p), nat.ptr(z), nat.ptr(u), int(z.size), nat.ptr(g), nat.ptr(loss)),
               "fcb_cdf_grad")
     return float(loss[0]), g
+
+
+class Batch:
+    """Many panels of uneven T x N per launch (fcb_batch_* in include/fcb200.h).
+
+    ``panels`` is a list of dicts of device-resident torch tensors on the
+    current CUDA device: ``X`` (F,T,N) factor planes, ``R`` (T,N) forward
+    returns, optional ``fmask`` / ``rmask`` (T,N) uint8, outputs ``ic`` (F,T)
+    f64 (required), ``ranks`` (F,T,N) f32 and ``corr`` (F,F) f64 (optional),
+    and optional ``model`` (a fitted :class:`CdfModel`, f32 panels).  All
+    panels share one dtype pair, (f32, f32) or (f64, f64).  The tensors are
+    kept referenced for the batch's lifetime.  ``run()`` replays the batch's
+    CUDA graph on the current stream; ``run_per_panel()`` issues the same work
+    one panel at a time (the comparison arm); results agree bit for bit."""
+
+    def __init__(self, panels, min_valid=30, config=None):
+        _require_cuda("Batch")
+        if not panels:
+            raise ValueError("Batch needs at least one panel")
+        self._keep = []
+        arr = (nat.FcbPanel * len(panels))()
+        dts = set()
+        for k, p in enumerate(panels):
+            X, R = p["X"], p["R"]
+            F, T, N = (int(v) for v in X.shape)
+            if tuple(R.shape) != (T, N):
+                raise ValueError(f"panel {k}: R must be (T,N) = {(T, N)}")
+            dts.add((str(X.dtype), str(R.dtype)))
+            model = p.get("model")
+            arr[k] = nat.FcbPanel(T, N, F, nat.ptr(X), nat.ptr(R), nat.ptr(p.get("fmask")), nat.ptr(p.get("rmask")),
+                                  nat.ptr(p.get("ranks")), nat.ptr(p["ic"]), nat.ptr(p.get("corr")),
+                                  model.handle if model is not None else None)
+            self._keep.append(p)
+        if len(dts) != 1:
+            raise ValueError("all panels of a batch share one dtype pair")
+        (dx, dr), = dts
+        code = {"torch.float32": nat.FCB_DTYPE_F32, "torch.float64": nat.FCB_DTYPE_F64}
+        if dx not in code or dr not in code:
+            raise TypeError(f"unsupported panel dtypes {dx}, {dr}")
+        cfgp = None
+        if config is not None:
+            cfg = nat.FcbBatchConfig()
+            nat.lib().fcb_batch_default_config(C.byref(cfg))
+            for k2, v in dict(config).items():
+                setattr(cfg, k2, int(v))
+            cfgp = C.byref(cfg)
+        h = C.c_void_p()
+        nat.check(nat.lib().fcb_batch_create(arr, len(panels), code[dx], code[dr], int(min_valid), cfgp, C.byref(h)),
+                  "fcb_batch_create")
+        self._h = h
+        self._arr = arr
+
+    def _stream(self):
+        return C.c_void_p(_torch.cuda.current_stream().cuda_stream)
+
+    def run(self):
+        nat.check(nat.lib().fcb_batch_run(self._h, self._stream()), "fcb_batch_run")
+
+    def run_per_panel(self):
+        nat.check(nat.lib().fcb_batch_run_per_panel(self._h, self._stream()), "fcb_batch_run_per_panel")
+
+    def status(self):
+        nat.check(nat.lib().fcb_batch_status(self._h), "fcb_batch_status")
+
+    @property
+    def config(self):
+        cfg = nat.FcbBatchConfig()
+        nat.check(nat.lib().fcb_batch_get_config(self._h, C.byref(cfg)), "fcb_batch_get_config")
+        return cfg.as_dict()
+
+    @config.setter
+    def config(self, value):
+        cfg = nat.FcbBatchConfig()
+        nat.check(nat.lib().fcb_batch_get_config(self._h, C.byref(cfg)), "fcb_batch_get_config")
+        for k, v in dict(value).items():
+            setattr(cfg, k, int(v))
+        nat.check(nat.lib().fcb_batch_set_config(self._h, C.byref(cfg)), "fcb_batch_set_config")
+
+    def autotune(self, reps=3, cache_path=None):
+        """Measure alternative configurations and keep the fastest; returns
+        (config dict, mean ms per replay, from_cache)."""
+        cfg = nat.FcbBatchConfig()
+        ms = C.c_float()
+        path = None if cache_path is None else str(cache_path).encode()
+        rc = nat.lib().fcb_batch_autotune(self._h, int(reps), path, C.byref(cfg), C.byref(ms))
+        if rc not in (0, 1):
+            nat.check(rc, "fcb_batch_autotune")
+        return cfg.as_dict(), float(ms.value), rc == 1
+
+    def close(self):
+        if getattr(self, "_h", None):
+            nat.lib().fcb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -29,6 +29,25 @@ _p = C.c_void_p
 _i = C.c_int
 _d = C.POINTER(C.c_double)
 
+
+
+class FcbPanel(C.Structure):
+    """struct fcb_panel (include/fcb200.h)."""
+    _fields_ = [("T", C.c_int), ("N", C.c_int), ("F", C.c_int), ("X", _p), ("R", _p), ("fmask", _p),
+                ("rmask", _p), ("ranks_out", _p), ("ic_out", _p), ("corr_out", _p), ("model", _p)]
+
+
+class FcbBatchConfig(C.Structure):
+    """struct fcb_batch_config (include/fcb200.h)."""
+    _fields_ = [("nt_small_max", C.c_int), ("nt_mid_max", C.c_int), ("ctas_per_sm", C.c_int),
+                ("concurrent", C.c_int), ("order", C.c_int), ("learn_cap", C.c_int)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+_cfgp = C.POINTER(FcbBatchConfig)
+
 # name -> (restype, argtypes); the symbol table of include/fcb200.h
 PROTOTYPES = {
     "fcb_workspace_create": (_p, []),
@@ -61,6 +80,15 @@ PROTOTYPES = {
     "fcb_cdf_model_load": (_i, [_p, _p, _p, _p]),
     "fcb_cdf_grad": (_i, [_p, _p, _p, _i, _p, _p]),
     "fcb_dev_rank_ic_panel_learned": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _p, _i, _p, _p]),
+    "fcb_batch_default_config": (None, [_cfgp]),
+    "fcb_batch_create": (_i, [C.POINTER(FcbPanel), _i, _i, _i, _i, _cfgp, C.POINTER(_p)]),
+    "fcb_batch_destroy": (None, [_p]),
+    "fcb_batch_get_config": (_i, [_p, _cfgp]),
+    "fcb_batch_set_config": (_i, [_p, _cfgp]),
+    "fcb_batch_run": (_i, [_p, _p]),
+    "fcb_batch_run_per_panel": (_i, [_p, _p]),
+    "fcb_batch_status": (_i, [_p]),
+    "fcb_batch_autotune": (_i, [_p, _i, C.c_char_p, _cfgp, C.POINTER(C.c_float)]),
 }
 
 

@@ -81,7 +81,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     lib = lib_path()
     if force or _stale(lib, objs):
         _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(lib), *map(str, objs),
-              "-cudart", "static", "-lcuda"])
+              "-cudart", "static"])
         if verbose:
             print(f"  link {lib.name}")
 

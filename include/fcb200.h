@@ -235,6 +235,69 @@ int fcb_dev_stock_corr_prec(const float* d_x, const uint8_t* d_mask, int T, int 
 int fcb_dev_factor_corr_noalloc(const void* d_x, int dtype, const uint8_t* d_mask, int T, int N, int F,
                                 double* d_out, void* stream);
 
+/* ------------------------------------------------------ batched panels ---
+ * No counterpart in the reference (which processes one panel per call, so a
+ * caller with many panels loops over fc.rolling_ic / fc.factor_corr).  One
+ * batch holds many panels of uneven T x N on the current device; each run
+ * computes, for every panel, what fcb_dev_rank_ic_panel (cs_rank ranks +
+ * rolling_ic) and fcb_factor_corr compute for it alone -- bit for bit.
+ * Rank + IC runs as persistent kernels taking (panel, date) items from device
+ * queues; factor_corr follows; the sequence is captured once into a CUDA
+ * graph and replayed.  All pointers are DEVICE pointers owned by the caller
+ * and must stay valid for the batch's lifetime; runs are asynchronous on
+ * `stream` (NULL = legacy stream). */
+typedef struct fcb_batch fcb_batch;
+
+typedef struct fcb_panel {
+  int T, N, F;                 /* N <= 16384 (else FCB_ERR_UNSUPPORTED)          */
+  const void* X;               /* F factor planes, each (T,N), dtype_x           */
+  const void* R;               /* (T,N) forward returns, dtype_r                 */
+  const uint8_t* fmask;        /* (T,N) factor mask or NULL                      */
+  const uint8_t* rmask;        /* (T,N) returns mask or NULL                     */
+  float* ranks_out;            /* (F,T,N) cs_rank ranks or NULL                  */
+  double* ic_out;              /* (F,T) rolling IC                               */
+  double* corr_out;            /* (F,F) factor_corr over the panel's (t,i) rows
+                                  (fmask broadcast per column; F <= 128) or NULL */
+  const fcb_cdf_model* model;  /* learned splitters for this panel's factors
+                                  (f32 only, fitted, model F == F) or NULL       */
+} fcb_panel;
+
+/* Scheduling knobs.  None of them changes a result. */
+typedef struct fcb_batch_config {
+  int nt_small_max;  /* largest N ranked by 256-thread CTAs (1..4096)            */
+  int nt_mid_max;    /* largest N ranked by 512-thread CTAs (..8192); larger N
+                        use 1024-thread CTAs                                    */
+  int ctas_per_sm;   /* persistent CTAs per SM per size class, 0 = all that fit  */
+  int concurrent;    /* 1: size classes run side by side with grids split by
+                        work; 0: one after another, each on the whole GPU        */
+  int order;         /* 1: items longest first; 0: panel order                   */
+  int learn_cap;     /* largest learned bucket before the radix fallback         */
+} fcb_batch_config;
+
+void fcb_batch_default_config(fcb_batch_config* cfg);
+/* dtype pair (F32,F32) or (F64,F64); min_valid >= 2 (else FCB_ERR_CAP4); cfg
+ * NULL = defaults.  Same caps as the single-panel entry points. */
+int fcb_batch_create(const fcb_panel* panels, int npanels, int dtype_x, int dtype_r, int min_valid,
+                     const fcb_batch_config* cfg, fcb_batch** out);
+void fcb_batch_destroy(fcb_batch* b);
+int fcb_batch_get_config(const fcb_batch* b, fcb_batch_config* cfg);
+int fcb_batch_set_config(fcb_batch* b, const fcb_batch_config* cfg);
+/* One replay of the batch's graph (captured on first use or after a config
+ * change). */
+int fcb_batch_run(fcb_batch* b, void* stream);
+/* The same work as one launch sequence per panel, no graph: what a caller
+ * looping over the single-panel entry points does (the comparison arm). */
+int fcb_batch_run_per_panel(fcb_batch* b, void* stream);
+/* Synchronises the device; FCB_OK, or FCB_ERR_DEVICE_WAIT if a staged copy
+ * in any run since the last call did not land. */
+int fcb_batch_status(fcb_batch* b);
+/* Measures the batch under alternative configurations (coordinate descent,
+ * `reps` replays each) and keeps the fastest.  cache_path (or NULL): a text
+ * file of "signature<TAB>config ms" lines; a batch whose signature is found
+ * takes that configuration without measuring (returns 1), a measured winner is
+ * appended.  Returns 0 after measuring. */
+int fcb_batch_autotune(fcb_batch* b, int reps, const char* cache_path, fcb_batch_config* best, float* best_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,38 @@ def test_contract_errors_without_device(native):
     assert lib.fcb_status_string(-4).decode()
 
 
+def test_batch_contract_errors_without_device(native):
+    """fcb_batch_create rejects bad panels with the single-panel codes before
+    it touches a device; the default configuration is the documented one."""
+    lib = native.lib()
+    cfg = native.FcbBatchConfig()
+    lib.fcb_batch_default_config(C.byref(cfg))
+    assert cfg.as_dict() == {"nt_small_max": 4096, "nt_mid_max": 8192, "ctas_per_sm": 0, "concurrent": 0,
+                             "order": 1, "learn_cap": 64}
+    h = C.c_void_p()
+    arr = (native.FcbPanel * 2)()
+    arr[0] = native.FcbPanel(10, 500, 2, 16, 16, None, None, None, 16, None, None)
+    arr[1] = native.FcbPanel(10, 500, 2, 16, 16, None, None, None, 16, None, None)
+    assert lib.fcb_batch_create(None, 0, 0, 0, 30, None, C.byref(h)) == -1
+    assert lib.fcb_batch_create(arr, 2, 0, 0, 30, None, None) == -1
+    assert lib.fcb_batch_create(arr, 2, 0, 0, 1, None, C.byref(h)) == -4          # min_valid < 2
+    assert lib.fcb_batch_create(arr, 2, 0, 1, 30, None, C.byref(h)) == -5         # mixed dtypes
+    arr[1].N = 20000
+    assert lib.fcb_batch_create(arr, 2, 0, 0, 30, None, C.byref(h)) == -5         # N above the SMEM cap
+    arr[1].N = 500
+    arr[1].ic_out = None
+    assert lib.fcb_batch_create(arr, 2, 0, 0, 30, None, C.byref(h)) == -1
+    arr[1].ic_out = 16
+    arr[1].F, arr[1].corr_out = 129, 16
+    assert lib.fcb_batch_create(arr, 2, 0, 0, 30, None, C.byref(h)) == -3         # factor_corr F cap
+    arr[1].F, arr[1].corr_out = 2, None
+    bad = native.FcbBatchConfig()
+    lib.fcb_batch_default_config(C.byref(bad))
+    bad.nt_mid_max = 100                                                           # below nt_small_max
+    assert lib.fcb_batch_create(arr, 2, 0, 0, 30, C.byref(bad), C.byref(h)) == -1
+    assert not h.value
+
+
 def test_workspace_lifecycle_without_device(native):
     lib = native.lib()
     ws = lib.fcb_workspace_create()
