@@ -377,6 +377,93 @@ def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned
     return res
 
 
+def make_batch_panels(dev, n=64, F=8, seed=20261205):
+    """Seeded uneven panels for the batched path, generated on the device:
+    N ~ U[300, 6000], T ~ U[250, 2500]; half the factors Gaussian, half
+    lognormal(sigma=1); per-panel missing rate q ~ U[0, 0.2] as per-stock
+    pre-listing gaps (start date ~ U[0, 2qT)); returns = 0.03 * factor 0 +
+    N(0, 1) noise."""
+    import torch
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    nan = float("nan")
+    panels = []
+    for _ in range(n):
+        N = int(rng.integers(300, 6001))
+        T = int(rng.integers(250, 2501))
+        q = float(rng.uniform(0.0, 0.2))
+        X = torch.randn((F, T, N), generator=g, device=dev, dtype=torch.float32)
+        X[F // 2:].exp_()
+        start = torch.from_numpy(rng.integers(0, max(1, int(2 * q * T)), N)).to(dev)
+        listed = torch.arange(T, device=dev)[:, None] >= start[None, :]
+        X.masked_fill_(~listed[None], nan)
+        R = 0.03 * torch.nan_to_num(X[0]) + torch.randn((T, N), generator=g, device=dev, dtype=torch.float32)
+        R.masked_fill_(~listed, nan)
+        panels.append({"X": X, "R": R, "fmask": listed.to(torch.uint8), "rmask": torch.isfinite(R).to(torch.uint8),
+                       "ranks": torch.empty((F, T, N), dtype=torch.float32, device=dev),
+                       "ic": torch.empty((F, T), dtype=torch.float64, device=dev),
+                       "corr": torch.empty((F, F), dtype=torch.float64, device=dev)})
+    return panels
+
+
+def bench_batch(dev, steps=5, warmup=2):
+    """Batched uneven panels: one autotuned CUDA-graph replay of the
+    persistent rank+IC kernels + per-panel factor_corr, against the same work
+    issued one panel at a time.  Device-resident inputs (8.8 GB of factors,
+    far above L2)."""
+    import torch
+    import fcb200
+    panels = make_batch_panels(dev)
+    cells = sum(int(p["X"].numel()) for p in panels)
+    torch.cuda.synchronize(dev)
+    b = fcb200.Batch(panels, min_valid=MIN_VALID)
+    t0 = time.perf_counter()
+    cfg, tuned_ms, cached = b.autotune(reps=2)
+    tune_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / steps
+
+    ms_graph = timed(b.run)
+    b.status()
+    ic_g = [p["ic"].clone() for p in panels]
+    corr_g = [p["corr"].clone() for p in panels]
+    rk_g = [p["ranks"][:, :3].clone() for p in panels]
+    ms_pp = timed(b.run_per_panel)
+    b.status()
+    same = all(torch.equal(torch.nan_to_num(a, nan=7.0), torch.nan_to_num(p["ic"], nan=7.0)) and
+               torch.equal(torch.nan_to_num(c, nan=7.0), torch.nan_to_num(p["corr"], nan=7.0)) and
+               torch.equal(r.view(torch.int32), p["ranks"][:, :3].view(torch.int32))
+               for a, c, r, p in zip(ic_g, corr_g, rk_g, panels))
+    classes = sorted({0 if p["X"].shape[2] <= cfg["nt_small_max"] else (1 if p["X"].shape[2] <= cfg["nt_mid_max"]
+                                                                           else 2) for p in panels})
+    res = {"workload": "64 uneven panels (N ~ U[300,6000], T ~ U[250,2500], F=8, gaps ~ U[0,0.2]): "
+                       "cs_rank + rolling_ic(30) + factor_corr per panel",
+           "cells": cells, "unit": "Gelem/s",
+           "graph": {"ms": ms_graph, "value": cells / (ms_graph / 1e3) / 1e9,
+                     "kernels_per_replay": len(classes) + 5 * len(panels)},
+           "per_panel": {"ms": ms_pp, "value": cells / (ms_pp / 1e3) / 1e9, "kernels_per_step": 6 * len(panels)},
+           "speedup_graph_vs_per_panel": ms_pp / ms_graph,
+           "bit_exact_graph_vs_per_panel": bool(same),
+           "autotune": {"config": cfg, "tuned_ms": tuned_ms, "tuning_s": tune_s, "from_cache": cached}}
+    b.close()
+    del panels
+    torch.cuda.empty_cache()
+    return res
+
+
 def bench_stock_corr(dev, N, T=1218, steps=5, warmup=2):
     """stock_corr precision forms on one (T,N) panel, device-resident:
     BF16x3 tensor-core path vs plain FP32, error against the f64 path."""
@@ -485,6 +572,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--only-stock-corr", type=int, default=0, metavar="N",
                     help="run only the stock_corr precision leg at this N (profiling)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-panel leg")
+    ap.add_argument("--only-batch", action="store_true", help="run only the batched uneven-panel leg")
     ap.add_argument("--T", type=int, default=T_DEF)
     ap.add_argument("--N", type=int, default=N_DEF)
     ap.add_argument("--F", type=int, default=F_DEF)
@@ -496,6 +585,10 @@ def main():
         import torch
         print(json.dumps(bench_stock_corr(torch.device("cuda", 0), args.only_stock_corr, steps=args.steps,
                                           warmup=args.warmup)))
+        return
+    if args.only_batch:
+        import torch
+        print(json.dumps(bench_batch(torch.device("cuda", 0), steps=args.steps, warmup=args.warmup)))
         return
     if args.impl == "reference":
         if rank == 0:
@@ -523,6 +616,9 @@ def main():
         res["stock_corr"] = {"workload": "pairwise-complete (N,N) Pearson, T=1218, f32 returns "
                                          "(0.02*t4 + 3-factor component), pre-listing gaps + Bernoulli(0.98) mask",
                              "bf16_peak_tflops_measured": peak_bf16, "results": sc}
+    if not args.no_batch:
+        import torch
+        res["batch"] = bench_batch(torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
     if rank == 0:
         if not args.no_cpu_baseline:
             X, R, fm, rm = make_panel()

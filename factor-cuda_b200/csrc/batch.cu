@@ -369,8 +369,9 @@ extern "C" int fcb_batch_create(const fcb_panel* panels, int npanels, int dtype_
     const size_t b_colstat = static_cast<size_t>(F) * sizeof(FcColStat);
     const size_t b_gram = static_cast<size_t>(w.nblk_gram) * 4 * Fp * Fp * sizeof(double);
     const size_t b_fb = static_cast<size_t>(F) * F * sizeof(int) + 16;
+    const size_t b_part = fc_fb_part_doubles(R, F) * sizeof(double);
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    const size_t total = al(b_colpart) + al(b_colstat) + al(b_gram) + al(b_fb) + 256;
+    const size_t total = al(b_colpart) + al(b_colstat) + al(b_gram) + al(b_fb) + 256 + al(b_part);
     void* m = nullptr;
     e = cudaMalloc(&m, total);
     if (e != cudaSuccess) return fail(rcode(e));
@@ -385,6 +386,8 @@ extern "C" int fcb_batch_create(const fcb_panel* panels, int npanels, int dtype_
     w.fb_list = reinterpret_cast<int*>(c8);
     c8 += al(b_fb);
     w.fb_count = reinterpret_cast<int*>(c8);
+    c8 += 256;
+    w.fb_part = reinterpret_cast<double*>(c8);
   }
   const int r = (dtype_x == FCB_DTYPE_F32) ? upload_args<float, float>(*b) : upload_args<double, double>(*b);
   if (r != FCB_OK) return fail(r);

@@ -25,7 +25,7 @@ using namespace fcb;
 enum Slot : int {
   S_X = 0, S_X2, S_MASK, S_MASK2, S_OUT, S_OUT1, S_OUT2, S_OUT3, S_STATUS, S_IC, S_RF, S_RR,
   S_SC_RAW, S_SC_C, S_SC_M, S_SC_ST, S_SC_SUM, S_FB_LIST, S_FB_CNT,
-  S_FC_COLPART, S_FC_COLSTAT, S_FC_GRAM, S_FC_FLAGS,
+  S_FC_COLPART, S_FC_COLSTAT, S_FC_GRAM, S_FC_FLAGS, S_FC_FBPART,
   S_PC_MU, S_PC_XH, S_PC_XM, S_PC_XL, S_PC_QH, S_PC_QM, S_PC_QL, S_PC_M16, S_PC_X32, S_PC_Q32, S_PC_M32, S_PC_TILES, S_PC_X, S_PC_MASK,
   S_PC_OUT,
   // streamed panel: three chunk buffers each (upload / compute / download in flight)
@@ -667,6 +667,7 @@ extern "C" int fcb_factor_corr(const void* x, int dtype, const uint8_t* mask, in
   FCB_TRY(ws.get(S_FC_GRAM, static_cast<size_t>(w.nblk_gram) * 4 * Fp * Fp * 8, &w.gram));
   FCB_TRY(ws.get(S_FB_LIST, static_cast<size_t>(F) * F * 4, &w.fb_list));
   FCB_TRY(ws.get(S_FB_CNT, 64, &w.fb_count));
+  FCB_TRY(ws.get(S_FC_FBPART, fc_fb_part_doubles(R, F) * sizeof(double), &w.fb_part));
   FCB_TRY(ws.get(S_OUT, static_cast<size_t>(F) * F * 8, &dout));
   if (fallback_out) {
     FCB_TRY(ws.get(S_FC_FLAGS, static_cast<size_t>(F) * F, &dflags));

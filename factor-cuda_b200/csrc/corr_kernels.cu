@@ -25,6 +25,8 @@
 // bitwise.
 #include <cmath>
 
+#include <algorithm>
+
 #include "fcb_common.cuh"
 #include "fcb_kernels.h"
 
@@ -748,6 +750,242 @@ __global__ void k_fc_fallback(const TIN* __restrict__ X, const uint8_t* __restri
   }
 }
 
+// Multi-block fallback for large pools: the rows are split into `nblk` fixed
+// ranges; each block forms per-range Kahan partials (threads stride the range,
+// a fixed binary tree merges them), a per-pair kernel merges the ranges in
+// order.  Two passes as in k_fc_fallback: counts / means / min / max, then the
+// centred sums.  Deterministic for a given nblk; agrees with the single-block
+// form to rounding (the reference's multi-block kahan_reduce kernels,
+// src/factor_corr.cu:188-322, split the rows the same way).
+constexpr int kFbThreads = 256;
+constexpr int kFbP1 = 9;  // n, sx.s, sx.c, sy.s, sy.c, min x, max x, min y, max y
+constexpr int kFbP2 = 6;  // sxx.s, sxx.c, syy.s, syy.c, sxy.s, sxy.c
+
+FCB_DEV void fb_tree_kahan(double (*sh)[kFbThreads], int q0, int nq) {
+  const int tid = threadIdx.x;
+  for (int st = kFbThreads / 2; st > 0; st >>= 1) {
+    if (tid < st) {
+      for (int q = q0; q < q0 + nq; ++q) {
+        Kahan u, v;
+        u.s = sh[2 * q][tid];
+        u.c = sh[2 * q + 1][tid];
+        v.s = sh[2 * q][tid + st];
+        v.c = sh[2 * q + 1][tid + st];
+        u.merge(v);
+        sh[2 * q][tid] = u.s;
+        sh[2 * q + 1][tid] = u.c;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename TIN>
+__global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass1(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                            long long R, int F, long long sr, long long sf, int nblk,
+                                                            const int* __restrict__ fb_list,
+                                                            const int* __restrict__ fb_count,
+                                                            double* __restrict__ part) {
+  __shared__ double sh[5][kFbThreads];
+  __shared__ double mm[4][kFbThreads / 32];
+  const long long rpb = (R + nblk - 1) / nblk;
+  const long long r0 = blockIdx.x * rpb, r1 = min(R, r0 + rpb);
+  const int tid = threadIdx.x;
+  for (int slot = blockIdx.y; slot < *fb_count; slot += gridDim.y) {
+    const int e = fb_list[slot];
+    const int i = e / F, j = e % F;
+    Kahan kx, ky;
+    double n = 0.0, mnx = kBigPos, mxx = -kBigPos, mny = kBigPos, mxy = -kBigPos;
+    for (long long r = r0 + tid; r < r1; r += kFbThreads) {
+      const double x = static_cast<double>(X[r * sr + i * sf]);
+      const double y = static_cast<double>(X[r * sr + j * sf]);
+      if (finite_f64(x) && finite_f64(y) && (mask == nullptr || mask[r] != 0)) {
+        n += 1.0;
+        kx.add(x);
+        ky.add(y);
+        mnx = fmin(mnx, x);
+        mxx = fmax(mxx, x);
+        mny = fmin(mny, y);
+        mxy = fmax(mxy, y);
+      }
+    }
+    sh[0][tid] = kx.s;
+    sh[1][tid] = kx.c;
+    sh[2][tid] = ky.s;
+    sh[3][tid] = ky.c;
+    sh[4][tid] = n;
+    __syncthreads();
+    for (int st = kFbThreads / 2; st > 0; st >>= 1) {
+      if (tid < st) {
+        for (int q = 0; q < 2; ++q) {
+          Kahan u, v;
+          u.s = sh[2 * q][tid];
+          u.c = sh[2 * q + 1][tid];
+          v.s = sh[2 * q][tid + st];
+          v.c = sh[2 * q + 1][tid + st];
+          u.merge(v);
+          sh[2 * q][tid] = u.s;
+          sh[2 * q + 1][tid] = u.c;
+        }
+        sh[4][tid] += sh[4][tid + st];
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mnx = fmin(mnx, __shfl_xor_sync(kFull, mnx, o));
+      mxx = fmax(mxx, __shfl_xor_sync(kFull, mxx, o));
+      mny = fmin(mny, __shfl_xor_sync(kFull, mny, o));
+      mxy = fmax(mxy, __shfl_xor_sync(kFull, mxy, o));
+    }
+    if ((tid & 31) == 0) {
+      mm[0][tid >> 5] = mnx;
+      mm[1][tid >> 5] = mxx;
+      mm[2][tid >> 5] = mny;
+      mm[3][tid >> 5] = mxy;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int w = 1; w < kFbThreads / 32; ++w) {
+        mnx = fmin(mnx, mm[0][w]);
+        mxx = fmax(mxx, mm[1][w]);
+        mny = fmin(mny, mm[2][w]);
+        mxy = fmax(mxy, mm[3][w]);
+      }
+      double* P = part + (static_cast<size_t>(slot) * nblk + blockIdx.x) * kFbP1;
+      P[0] = sh[4][0];
+      P[1] = sh[0][0];
+      P[2] = sh[1][0];
+      P[3] = sh[2][0];
+      P[4] = sh[3][0];
+      P[5] = mnx;
+      P[6] = mxx;
+      P[7] = mny;
+      P[8] = mxy;
+    }
+    __syncthreads();
+  }
+}
+
+// Per flagged pair: merge the pass-1 ranges in order -> (n, mean x, mean y,
+// degenerate flag) in pair[slot*4 ..]; a degenerate pair is finished here.
+__global__ void k_fc_fb_mid(int F, int nblk, const int* __restrict__ fb_list, const int* __restrict__ fb_count,
+                            const double* __restrict__ part, double* __restrict__ pair, double* __restrict__ out) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= *fb_count) return;
+  Kahan kx, ky;
+  double n = 0.0, mnx = kBigPos, mxx = -kBigPos, mny = kBigPos, mxy = -kBigPos;
+  for (int b = 0; b < nblk; ++b) {
+    const double* P = part + (static_cast<size_t>(slot) * nblk + b) * kFbP1;
+    Kahan o;
+    o.s = P[1];
+    o.c = P[2];
+    kx.merge(o);
+    o.s = P[3];
+    o.c = P[4];
+    ky.merge(o);
+    n += P[0];
+    mnx = fmin(mnx, P[5]);
+    mxx = fmax(mxx, P[6]);
+    mny = fmin(mny, P[7]);
+    mxy = fmax(mxy, P[8]);
+  }
+  const bool degenerate = (n < 2.0 || mnx == mxx || mny == mxy);
+  double* Q = pair + static_cast<size_t>(slot) * 4;
+  Q[0] = n;
+  Q[1] = n > 0 ? kx.s / n : 0.0;
+  Q[2] = n > 0 ? ky.s / n : 0.0;
+  Q[3] = degenerate ? 1.0 : 0.0;
+  if (degenerate) {
+    const int e = fb_list[slot];
+    const int i = e / F, j = e % F;
+    out[i * F + j] = dnan();
+    out[j * F + i] = dnan();
+  }
+}
+
+template <typename TIN>
+__global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass2(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                            long long R, int F, long long sr, long long sf, int nblk,
+                                                            const int* __restrict__ fb_list,
+                                                            const int* __restrict__ fb_count,
+                                                            const double* __restrict__ pair,
+                                                            double* __restrict__ part) {
+  __shared__ double sh[6][kFbThreads];
+  const long long rpb = (R + nblk - 1) / nblk;
+  const long long r0 = blockIdx.x * rpb, r1 = min(R, r0 + rpb);
+  const int tid = threadIdx.x;
+  for (int slot = blockIdx.y; slot < *fb_count; slot += gridDim.y) {
+    const double* Q = pair + static_cast<size_t>(slot) * 4;
+    if (Q[3] != 0.0) continue;  // degenerate: finished by k_fc_fb_mid (uniform per block)
+    const int e = fb_list[slot];
+    const int i = e / F, j = e % F;
+    const double mx = Q[1], my = Q[2];
+    Kahan a, b, c;
+    for (long long r = r0 + tid; r < r1; r += kFbThreads) {
+      const double x = static_cast<double>(X[r * sr + i * sf]);
+      const double y = static_cast<double>(X[r * sr + j * sf]);
+      if (finite_f64(x) && finite_f64(y) && (mask == nullptr || mask[r] != 0)) {
+        const double dx = x - mx, dy = y - my;
+        a.add(dx * dx);
+        b.add(dy * dy);
+        c.add(dx * dy);
+      }
+    }
+    sh[0][tid] = a.s;
+    sh[1][tid] = a.c;
+    sh[2][tid] = b.s;
+    sh[3][tid] = b.c;
+    sh[4][tid] = c.s;
+    sh[5][tid] = c.c;
+    __syncthreads();
+    fb_tree_kahan(sh, 0, 3);
+    if (tid < kFbP2) part[(static_cast<size_t>(slot) * nblk + blockIdx.x) * kFbP2 + tid] = sh[tid][0];
+    __syncthreads();
+  }
+}
+
+__global__ void k_fc_fb_final(int F, int nblk, const int* __restrict__ fb_list, const int* __restrict__ fb_count,
+                              const double* __restrict__ pair, const double* __restrict__ part,
+                              double* __restrict__ out) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= *fb_count) return;
+  if (pair[static_cast<size_t>(slot) * 4 + 3] != 0.0) return;
+  Kahan a, b, c;
+  for (int k = 0; k < nblk; ++k) {
+    const double* P = part + (static_cast<size_t>(slot) * nblk + k) * kFbP2;
+    Kahan o;
+    o.s = P[0];
+    o.c = P[1];
+    a.merge(o);
+    o.s = P[2];
+    o.c = P[3];
+    b.merge(o);
+    o.s = P[4];
+    o.c = P[5];
+    c.merge(o);
+  }
+  const int e = fb_list[slot];
+  const int i = e / F, j = e % F;
+  const double r = safe_pearson(c.s - c.c, a.s - a.c, b.s - b.c);
+  out[i * F + j] = r;
+  out[j * F + i] = r;
+}
+
+size_t fc_fb_part_doubles(long long R, int F) {
+  const int maxpairs = F * (F - 1) / 2 > 0 ? F * (F - 1) / 2 : 1;
+  const int nblk = fc_fb_nblk(R, F);
+  return static_cast<size_t>(maxpairs) * nblk * kFbP1 + static_cast<size_t>(maxpairs) * 4;
+}
+
+int fc_fb_nblk(long long R, int F) {
+  const int maxpairs = F * (F - 1) / 2 > 0 ? F * (F - 1) / 2 : 1;
+  long long nb = R / 32768;
+  nb = std::min<long long>(nb, 64);
+  nb = std::min<long long>(nb, 65536 / maxpairs);
+  return static_cast<int>(std::max<long long>(nb, 1));
+}
+
 size_t fc_gram_smem(int Fp, int tasks_per_block) {
   const int slices = 256 / tasks_per_block;
   return (3 * static_cast<size_t>(kFcRowsChunk) * Fp + static_cast<size_t>(slices) * tasks_per_block * 16) *
@@ -794,6 +1032,31 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
                                                  flags);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const int maxpairs = F * (F - 1) / 2 > 0 ? F * (F - 1) / 2 : 1;
+  const int nblk = fc_fb_nblk(R, F);
+  if (w.fb_part != nullptr && R >= 4096 && nblk > 1) {
+    // large pools, caller-provided partials: rows split over nblk blocks per pair
+    double* pair = w.fb_part + static_cast<size_t>(maxpairs) * nblk * kFbP1;
+    const int ysl = std::max(1, std::min(maxpairs, 2048 / nblk));
+    dim3 g(nblk, ysl);
+    if (dtype == 0)
+      k_fc_fb_pass1<float><<<g, kFbThreads, 0, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, nblk,
+                                                     w.fb_list, w.fb_count, w.fb_part);
+    else
+      k_fc_fb_pass1<double><<<g, kFbThreads, 0, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf, nblk,
+                                                      w.fb_list, w.fb_count, w.fb_part);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_fc_fb_mid<<<(maxpairs + 127) / 128, 128, 0, s>>>(F, nblk, w.fb_list, w.fb_count, w.fb_part, pair, out);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (dtype == 0)
+      k_fc_fb_pass2<float><<<g, kFbThreads, 0, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, nblk,
+                                                     w.fb_list, w.fb_count, pair, w.fb_part);
+    else
+      k_fc_fb_pass2<double><<<g, kFbThreads, 0, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf, nblk,
+                                                      w.fb_list, w.fb_count, pair, w.fb_part);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_fc_fb_final<<<(maxpairs + 127) / 128, 128, 0, s>>>(F, nblk, w.fb_list, w.fb_count, pair, w.fb_part, out);
+    return cudaGetLastError();
+  }
   if (dtype == 0)
     k_fc_fallback<float><<<maxpairs, 256, 0, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, w.fb_list,
                                                   w.fb_count, out);

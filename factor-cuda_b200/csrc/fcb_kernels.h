@@ -59,7 +59,12 @@ struct FcWork {
   double* gram;        // [nblk_gram][4][Fp][Fp]
   int* fb_list;        // [F*F]
   int* fb_count;       // [1]
+  double* fb_part;     // fc_fb_part_doubles(R, F) doubles, or nullptr (single-block fallback)
 };
+// Row blocks per flagged pair of the multi-block fallback, and the partials
+// buffer it needs (doubles).
+int fc_fb_nblk(long long R, int F);
+size_t fc_fb_part_doubles(long long R, int F);
 
 // rank_kernels.cu
 size_t cs_rank_smem(int N);

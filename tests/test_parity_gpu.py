@@ -217,6 +217,39 @@ def test_factor_corr_random(fcp):
     assert np.array_equal(got, fcp.factor_corr_f64(F3.astype(np.float64), m), equal_nan=True)
 
 
+def test_factor_corr_large_pool_fallback():
+    """Pairs the cancellation gate flags on a large pool (200k rows) take the
+    multi-block two-pass fallback: same results as the oracle (<= 1e-12) and
+    as the single-block fallback of the no-allocation entry point."""
+    import torch
+    from fcb200 import _native as nat
+    rng = np.random.default_rng(21)
+    T, N, F = 200, 1000, 5
+    F3 = rng.standard_normal((T, N, F))
+    F3[..., 0] = 1e3 + F3[..., 0]                          # |mean| >> std: gate fires against 1, 2
+    F3[..., 1] = 5e2 + 0.3 * F3[..., 0] + F3[..., 1]
+    F3[..., 2] = np.exp(F3[..., 2])                        # lognormal
+    F3[..., 3] = 3.0                                       # constant -> NaN row / column
+    F3[rng.random((T, N, F)) < 0.02] = np.nan
+    m = rng.random((T, N)) < 0.95
+    for dt in (np.float64, np.float32):
+        X = np.ascontiguousarray(F3.astype(dt))
+        m8 = m.astype(np.uint8)
+        out = np.empty((F, F))
+        flags = np.zeros((F, F), np.uint8)
+        nat.check(nat.lib().fcb_factor_corr(nat.ptr(X), 0 if dt == np.float32 else 1, nat.ptr(m8), T, N, F,
+                                            nat.ptr(out), nat.ptr(flags)), "fcb_factor_corr")
+        assert flags.sum() >= 2, "the gate should flag the biased pairs"
+        assert corr_match(out, O.factor_corr(X, m))
+        dX = torch.from_numpy(X).cuda()
+        dM = torch.from_numpy(m8).cuda()
+        dO = torch.empty((F, F), dtype=torch.float64, device="cuda")
+        nat.check(nat.lib().fcb_dev_factor_corr_noalloc(dX.data_ptr(), 0 if dt == np.float32 else 1, dM.data_ptr(),
+                                                        T, N, F, dO.data_ptr(), None), "noalloc")
+        torch.cuda.synchronize()
+        assert corr_match(out, dO.cpu().numpy())
+
+
 def test_adapter_end_to_end():
     import fcb200
     rng = np.random.default_rng(1)
