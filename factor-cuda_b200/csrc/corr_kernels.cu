@@ -464,12 +464,15 @@ __global__ void k_fc_colpart(const TIN* __restrict__ X, const uint8_t* __restric
   }
 }
 
+// One warp per column: lane l merges partials l, l+32, ... in order, then a
+// fixed shuffle tree merges the lanes.
 __global__ void k_fc_colfinal(const FcColPart* __restrict__ part, int nblk, int F, FcColStat* __restrict__ st) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= F) return;
+  const int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (f >= F) return;  // whole warps exit together
   Kahan k;
   double cnt = 0.0, mn = kBigPos, mx = -kBigPos;
-  for (int b = 0; b < nblk; ++b) {
+  for (int b = lane; b < nblk; b += 32) {
     const FcColPart& p = part[static_cast<size_t>(b) * F + f];
     Kahan o;
     o.s = p.s;
@@ -479,6 +482,21 @@ __global__ void k_fc_colfinal(const FcColPart* __restrict__ part, int nblk, int 
     mn = fmin(mn, p.min);
     mx = fmax(mx, p.max);
   }
+  for (int o = 1; o < 32; o <<= 1) {
+    const double os = __shfl_down_sync(kFull, k.s, o), oc = __shfl_down_sync(kFull, k.c, o);
+    const double on = __shfl_down_sync(kFull, cnt, o);
+    const double omn = __shfl_down_sync(kFull, mn, o), omx = __shfl_down_sync(kFull, mx, o);
+    if ((lane & (2 * o - 1)) == 0) {
+      Kahan kk;
+      kk.s = os;
+      kk.c = oc;
+      k.merge(kk);
+      cnt += on;
+      mn = fmin(mn, omn);
+      mx = fmax(mx, omx);
+    }
+  }
+  if (lane != 0) return;
   FcColStat s;
   s.count = cnt;
   s.mean = cnt > 0.0 ? k.s / cnt : 0.0;
@@ -491,7 +509,9 @@ __global__ void k_fc_colfinal(const FcColPart* __restrict__ part, int nblk, int 
 // 2 sx2=(x'^2,m), 3 sxy=(x',x').  Each thread owns a 4x4 (f,g) tile of one
 // product and a slice of the staged rows; slices are summed in shared memory
 // in a fixed order at the end of the block.
-constexpr int kFcRowsChunk = 32;
+// Rows staged per step: 32 for F >= 64, more for narrower panels so that the
+// staged tile stays near 48 KB (fewer barriers per row, two blocks per SM).
+__host__ __device__ inline int fc_rows_chunk(int Fp) { return 32 * (64 / Fp > 8 ? 8 : (64 / Fp < 1 ? 1 : 64 / Fp)); }
 
 template <typename TIN>
 __global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
@@ -501,9 +521,10 @@ __global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, cons
                                                  int tasks_per_block, double* __restrict__ part) {
   extern __shared__ __align__(16) double fsm[];
   double* sx = fsm;                                  // [chunk][Fp] centred values
-  double* sm = sx + kFcRowsChunk * Fp;               // [chunk][Fp] validity
-  double* sq = sm + kFcRowsChunk * Fp;               // [chunk][Fp] squares
-  double* red = sq + kFcRowsChunk * Fp;              // [slices][tasks_per_block][16]
+  const int chunk = fc_rows_chunk(Fp);
+  double* sm = sx + chunk * Fp;                      // [chunk][Fp] validity
+  double* sq = sm + chunk * Fp;                      // [chunk][Fp] squares
+  double* red = sq + chunk * Fp;                     // [slices][tasks_per_block][16]
   const int tb = Fp / 4;
   const int task0 = blockIdx.y * tasks_per_block;
   const int ntask = min(tasks_per_block, tasks_total - task0);
@@ -524,12 +545,12 @@ __global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, cons
   for (int q = 0; q < 16; ++q) acc[q] = 0.0;
   const long long r0 = blockIdx.x * rows_per_block;
   const long long r1 = min(R, r0 + rows_per_block);
-  for (long long c0 = r0; c0 < r1; c0 += kFcRowsChunk) {
-    const int nr = static_cast<int>(min(static_cast<long long>(kFcRowsChunk), r1 - c0));
-    for (int e = threadIdx.x; e < kFcRowsChunk * Fp; e += 256) {
+  for (long long c0 = r0; c0 < r1; c0 += chunk) {
+    const int nr = static_cast<int>(min(static_cast<long long>(chunk), r1 - c0));
+    for (int e = threadIdx.x; e < chunk * Fp; e += 256) {
       // consecutive threads read consecutive elements of X in either layout
-      const int rr = (sf == 1) ? e / Fp : e % kFcRowsChunk;
-      const int f = (sf == 1) ? e % Fp : e / kFcRowsChunk;
+      const int rr = (sf == 1) ? e / Fp : e % chunk;
+      const int f = (sf == 1) ? e % Fp : e / chunk;
       const int ei = rr * Fp + f;
       double v = 0.0, mv = 0.0;
       if (rr < nr && f < F) {
@@ -586,16 +607,19 @@ __global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, cons
 }
 
 // Sum the per-block Gram partials in block order, finalize each pair.
+// One warp per (i <= j) pair: lane l sums blocks l, l+32, ..., a fixed
+// shuffle tree sums the lanes, lane 0 finalizes.
 __global__ void k_fc_final(const double* __restrict__ part, int nblk, int F, int Fp,
                            const FcColStat* __restrict__ st, double* __restrict__ out, int* __restrict__ fb_list,
                            int* __restrict__ fb_count, uint8_t* __restrict__ flags) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= F * F) return;
+  const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (e >= F * F) return;  // whole warps exit together
   const int i = e / F, j = e % F;
   if (i > j) return;
   double q[6] = {0, 0, 0, 0, 0, 0};
   // q: n, sx (x'_i m_j), sy (m_i x'_j), sxy, sx2 (x'^2_i m_j), sy2 (m_i x'^2_j)
-  for (int b = 0; b < nblk; ++b) {
+  for (int b = lane; b < nblk; b += 32) {
     const double* P = part + static_cast<size_t>(b) * 4 * Fp * Fp;
     q[0] += P[(0 * Fp + i) * Fp + j];
     q[1] += P[(1 * Fp + i) * Fp + j];
@@ -604,6 +628,14 @@ __global__ void k_fc_final(const double* __restrict__ part, int nblk, int F, int
     q[4] += P[(2 * Fp + i) * Fp + j];
     q[5] += P[(2 * Fp + j) * Fp + i];
   }
+  for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const double v = __shfl_down_sync(kFull, q[k], o);
+      if ((lane & (2 * o - 1)) == 0) q[k] += v;
+    }
+  }
+  if (lane != 0) return;
   double r;
   bool flag = false;
   if (i == j) {
@@ -988,7 +1020,7 @@ int fc_fb_nblk(long long R, int F) {
 
 size_t fc_gram_smem(int Fp, int tasks_per_block) {
   const int slices = 256 / tasks_per_block;
-  return (3 * static_cast<size_t>(kFcRowsChunk) * Fp + static_cast<size_t>(slices) * tasks_per_block * 16) *
+  return (3 * static_cast<size_t>(fc_rows_chunk(Fp)) * Fp + static_cast<size_t>(slices) * tasks_per_block * 16) *
          sizeof(double);
 }
 
@@ -1011,7 +1043,7 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
                                                     w.colpart);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_fc_colfinal<<<(F + 127) / 128, 128, 0, s>>>(w.colpart, w.nblk_cols, F, w.colstat);
+  k_fc_colfinal<<<(F * 32 + 127) / 128, 128, 0, s>>>(w.colpart, w.nblk_cols, F, w.colstat);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const size_t smem = fc_gram_smem(Fp, tasks_per_block);
   dim3 gg(w.nblk_gram, ytiles);
@@ -1028,8 +1060,8 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
   }
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(w.fb_count, 0, sizeof(int), s)) != cudaSuccess) return e;
-  k_fc_final<<<(F * F + 255) / 256, 256, 0, s>>>(w.gram, w.nblk_gram, F, Fp, w.colstat, out, w.fb_list, w.fb_count,
-                                                 flags);
+  k_fc_final<<<(F * F * 32 + 255) / 256, 256, 0, s>>>(w.gram, w.nblk_gram, F, Fp, w.colstat, out, w.fb_list,
+                                                      w.fb_count, flags);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const int maxpairs = F * (F - 1) / 2 > 0 ? F * (F - 1) / 2 : 1;
   const int nblk = fc_fb_nblk(R, F);
