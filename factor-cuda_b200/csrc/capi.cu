@@ -27,7 +27,7 @@ enum Slot : int {
   S_SC_RAW, S_SC_C, S_SC_M, S_SC_ST, S_SC_SUM, S_FB_LIST, S_FB_CNT,
   S_FC_COLPART, S_FC_COLSTAT, S_FC_GRAM, S_FC_FLAGS, S_FC_FBPART,
   S_PC_MU, S_PC_XH, S_PC_XM, S_PC_XL, S_PC_QH, S_PC_QM, S_PC_QL, S_PC_M16, S_PC_X32, S_PC_Q32, S_PC_M32, S_PC_TILES, S_PC_X, S_PC_MASK,
-  S_PC_OUT,
+  S_PC_OUT, S_PC_CPART,
   // streamed panel: three chunk buffers each (upload / compute / download in flight)
   S_PX0, S_PX1, S_PX2, S_PR0, S_PR1, S_PR2, S_PFM0, S_PFM1, S_PFM2, S_PRM0, S_PRM1, S_PRM2,
   S_PRK0, S_PRK1, S_PRK2, S_PIC,
@@ -710,36 +710,32 @@ extern "C" int fcb_dev_stock_corr_prec(const float* d_x, const uint8_t* d_mask, 
   int* dst;
   FCB_TRY(ws.get(S_PC_MU, static_cast<size_t>(Np) * 4, &mu));
   FCB_TRY(ws.get(S_STATUS, 64, &dst));
-  std::vector<int2> tiles;
   if (mode == FCB_PREC_BF16X3) {
     FCB_TRY(ws.get(S_PC_XH, e * 2 * 7, &op.h));
     op.np = Np;
-    for (int ti = 0; ti * kPrecTileTcM < N; ++ti)
-      for (int tj = 0; tj * kPrecTileTcN < N; ++tj)
-        if (tj * kPrecTileTcN + kPrecTileTcN - 1 >= ti * kPrecTileTcM) tiles.push_back(make_int2(ti, tj));
   } else {
     FCB_TRY(ws.get(S_PC_X32, e * 4, &op.x32));
     FCB_TRY(ws.get(S_PC_Q32, e * 4, &op.q32));
     FCB_TRY(ws.get(S_PC_M32, e * 4, &op.m32));
-    for (int ti = 0; ti * kPrecTileFp32 < N; ++ti)
-      for (int tj = ti; tj * kPrecTileFp32 < N; ++tj) tiles.push_back(make_int2(ti, tj));
   }
+  const int ntiles = prec_tile_count(mode == FCB_PREC_BF16X3 ? 0 : 1, N);
   int2* dt;
-  FCB_TRY(ws.get(S_PC_TILES, tiles.size() * sizeof(int2), &dt));
-  FCB_TRY(cudaMemcpyAsync(dt, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
-  FCB_TRY(launch_prec_prep(d_x, d_mask, T, N, Np, Tp, mu, op, s));
+  FCB_TRY(ws.get(S_PC_TILES, static_cast<size_t>(ntiles) * sizeof(int2), &dt));
+  FCB_TRY(launch_prec_tiles(mode == FCB_PREC_BF16X3 ? 0 : 1, N, dt, s));
+  double2* cpart;
+  FCB_TRY(ws.get(S_PC_CPART, static_cast<size_t>(prec_colmean_chunks(T)) * Np * sizeof(double2), &cpart));
+  FCB_TRY(launch_prec_prep(d_x, d_mask, T, N, Np, Tp, mu, cpart, op, s));
   if (mode == FCB_PREC_BF16X3) {
     FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), s));
-    FCB_TRY(launch_corr_bf16x3(op, dt, static_cast<int>(tiles.size()), N, Np, Tp, d_out, dst, s));
-  } else {
-    FCB_TRY(launch_corr_fp32(op, dt, static_cast<int>(tiles.size()), N, Tp, d_out, s));
-  }
-  // the tile list upload reads a host vector: finish it before returning
-  FCB_TRY(cudaStreamSynchronize(s));
-  if (mode == FCB_PREC_BF16X3) {
+    FCB_TRY(launch_corr_bf16x3(op, dt, ntiles, N, Np, Tp, d_out, dst, s));
+    // the kernel's bounded waits report through dst: read it once the stream is done
     int hst = 0;
-    FCB_TRY(cudaMemcpy(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost));
+    FCB_TRY(cudaMemcpyAsync(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FCB_TRY(cudaStreamSynchronize(s));
     if (hst != 0) return FCB_ERR_DEVICE_WAIT;
+  } else {
+    FCB_TRY(launch_corr_fp32(op, dt, ntiles, N, Tp, d_out, s));
+    FCB_TRY(cudaStreamSynchronize(s));
   }
   return FCB_OK;
 }

@@ -783,7 +783,7 @@ __global__ void k_fc_fallback(const TIN* __restrict__ X, const uint8_t* __restri
 }
 
 // Multi-block fallback for large pools: the rows are split into `nblk` fixed
-// ranges; each block forms per-range Kahan partials (threads stride the range,
+// ranges (blockIdx.y); each block forms per-range Kahan partials (threads stride the range,
 // a fixed binary tree merges them), a per-pair kernel merges the ranges in
 // order.  Two passes as in k_fc_fallback: counts / means / min / max, then the
 // centred sums.  Deterministic for a given nblk; agrees with the single-block
@@ -821,9 +821,9 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass1(const TIN* __restric
   __shared__ double sh[5][kFbThreads];
   __shared__ double mm[4][kFbThreads / 32];
   const long long rpb = (R + nblk - 1) / nblk;
-  const long long r0 = blockIdx.x * rpb, r1 = min(R, r0 + rpb);
+  const long long r0 = blockIdx.y * rpb, r1 = min(R, r0 + rpb);
   const int tid = threadIdx.x;
-  for (int slot = blockIdx.y; slot < *fb_count; slot += gridDim.y) {
+  for (int slot = blockIdx.x; slot < *fb_count; slot += gridDim.x) {
     const int e = fb_list[slot];
     const int i = e / F, j = e % F;
     Kahan kx, ky;
@@ -884,7 +884,7 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass1(const TIN* __restric
         mny = fmin(mny, mm[2][w]);
         mxy = fmax(mxy, mm[3][w]);
       }
-      double* P = part + (static_cast<size_t>(slot) * nblk + blockIdx.x) * kFbP1;
+      double* P = part + (static_cast<size_t>(slot) * nblk + blockIdx.y) * kFbP1;
       P[0] = sh[4][0];
       P[1] = sh[0][0];
       P[2] = sh[1][0];
@@ -945,9 +945,9 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass2(const TIN* __restric
                                                             double* __restrict__ part) {
   __shared__ double sh[6][kFbThreads];
   const long long rpb = (R + nblk - 1) / nblk;
-  const long long r0 = blockIdx.x * rpb, r1 = min(R, r0 + rpb);
+  const long long r0 = blockIdx.y * rpb, r1 = min(R, r0 + rpb);
   const int tid = threadIdx.x;
-  for (int slot = blockIdx.y; slot < *fb_count; slot += gridDim.y) {
+  for (int slot = blockIdx.x; slot < *fb_count; slot += gridDim.x) {
     const double* Q = pair + static_cast<size_t>(slot) * 4;
     if (Q[3] != 0.0) continue;  // degenerate: finished by k_fc_fb_mid (uniform per block)
     const int e = fb_list[slot];
@@ -972,7 +972,7 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass2(const TIN* __restric
     sh[5][tid] = c.c;
     __syncthreads();
     fb_tree_kahan(sh, 0, 3);
-    if (tid < kFbP2) part[(static_cast<size_t>(slot) * nblk + blockIdx.x) * kFbP2 + tid] = sh[tid][0];
+    if (tid < kFbP2) part[(static_cast<size_t>(slot) * nblk + blockIdx.y) * kFbP2 + tid] = sh[tid][0];
     __syncthreads();
   }
 }
@@ -1068,8 +1068,10 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
   if (w.fb_part != nullptr && R >= 4096 && nblk > 1) {
     // large pools, caller-provided partials: rows split over nblk blocks per pair
     double* pair = w.fb_part + static_cast<size_t>(maxpairs) * nblk * kFbP1;
+    // pair slots vary fastest, so the blocks of all flagged pairs over one row
+    // range run together and share its columns through L2
     const int ysl = std::max(1, std::min(maxpairs, 2048 / nblk));
-    dim3 g(nblk, ysl);
+    dim3 g(ysl, nblk);
     if (dtype == 0)
       k_fc_fb_pass1<float><<<g, kFbThreads, 0, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, nblk,
                                                      w.fb_list, w.fb_count, w.fb_part);

@@ -53,15 +53,19 @@ constexpr int kTmemCols = 512;                        // 384 used, rounded to a 
 // ---------------------------------------------------------------------------
 // prep: (T,N) f32 + mask -> K-major (Np, Tp) operands
 // ---------------------------------------------------------------------------
-__global__ void k_prec_colmean(const float* __restrict__ X, const uint8_t* __restrict__ mask, int T, int N,
-                               float* __restrict__ mu) {
-  // block (32, 8): 32 columns, 8 date strides; coalesced row reads
+// Column means of the valid cells, in two steps so that enough blocks are in
+// flight: k_prec_colpart sums a chunk of dates per block (block (32, 8): 32
+// columns, 8 date strides, coalesced row reads) into part[chunk][i] = (sum,
+// count); k_prec_colmean adds the chunks in order (deterministic).
+__global__ void k_prec_colpart(const float* __restrict__ X, const uint8_t* __restrict__ mask, int T, int N, int Np,
+                               int tchunk, double2* __restrict__ part) {
   __shared__ double ss[8][33];
   __shared__ double sc[8][33];
   const int i = blockIdx.x * 32 + threadIdx.x;
+  const int t0 = blockIdx.y * tchunk, t1 = min(T, t0 + tchunk);
   double s = 0.0, c = 0.0;
   if (i < N) {
-    for (int t = threadIdx.y; t < T; t += 8) {
+    for (int t = t0 + threadIdx.y; t < t1; t += 8) {
       const size_t e = static_cast<size_t>(t) * N + i;
       const float v = X[e];
       if (finite_f32(v) && (mask == nullptr || mask[e])) {
@@ -78,9 +82,23 @@ __global__ void k_prec_colmean(const float* __restrict__ X, const uint8_t* __res
       s += ss[y][threadIdx.x];
       c += sc[y][threadIdx.x];
     }
-    mu[i] = c > 0 ? static_cast<float>(s / c) : 0.0f;
+    part[static_cast<size_t>(blockIdx.y) * Np + i] = make_double2(s, c);
   }
 }
+
+__global__ void k_prec_colmean(const double2* __restrict__ part, int nchunk, int N, int Np, float* __restrict__ mu) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double s = 0.0, c = 0.0;
+  for (int k = 0; k < nchunk; ++k) {
+    const double2 v = part[static_cast<size_t>(k) * Np + i];
+    s += v.x;
+    c += v.y;
+  }
+  mu[i] = c > 0 ? static_cast<float>(s / c) : 0.0f;
+}
+
+int prec_colmean_chunks(int T) { return T / 64 < 1 ? 1 : (T / 64 > 32 ? 32 : T / 64); }
 
 // Transposing split: one 32x32 (t,i) tile per block.
 __global__ void k_prec_split(const float* __restrict__ X, const uint8_t* __restrict__ mask, const float* __restrict__ mu,
@@ -437,13 +455,51 @@ __global__ void __launch_bounds__(256) k_corr_fp32(const float* __restrict__ X, 
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+// Tile lists on the device (no host vector, no upload).  BF16x3: 128 x 32
+// tiles (ti, tj) that reach the upper triangle, tj >= 4 ti, row-major; row ti
+// starts at ti*ntj - 2 ti (ti-1).  FP32: 64 x 64 tiles tj >= ti; row ti starts
+// at ti*n - ti (ti-1) / 2.  One thread per tile row.
+__global__ void k_prec_tiles(int mode, int N, int2* __restrict__ tiles) {
+  const int ti = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mode == 0) {
+    const int nti = (N + kTcM - 1) / kTcM, ntj = (N + kTcN - 1) / kTcN;
+    if (ti >= nti) return;
+    const long long off = static_cast<long long>(ti) * ntj - 2LL * ti * (ti - 1);
+    for (int tj = 4 * ti; tj < ntj; ++tj) tiles[off + (tj - 4 * ti)] = make_int2(ti, tj);
+  } else {
+    const int n = (N + kPrecTileFp32 - 1) / kPrecTileFp32;
+    if (ti >= n) return;
+    const long long off = static_cast<long long>(ti) * n - static_cast<long long>(ti) * (ti - 1) / 2;
+    for (int tj = ti; tj < n; ++tj) tiles[off + (tj - ti)] = make_int2(ti, tj);
+  }
+}
+
+int prec_tile_count(int mode, int N) {
+  if (mode == 0) {
+    const long long nti = (N + kTcM - 1) / kTcM, ntj = (N + kTcN - 1) / kTcN;
+    return static_cast<int>(nti * ntj - 2 * nti * (nti - 1));
+  }
+  const long long n = (N + kPrecTileFp32 - 1) / kPrecTileFp32;
+  return static_cast<int>(n * (n + 1) / 2);
+}
+
+cudaError_t launch_prec_tiles(int mode, int N, int2* tiles, cudaStream_t s) {
+  const int rows = mode == 0 ? (N + kTcM - 1) / kTcM : (N + kPrecTileFp32 - 1) / kPrecTileFp32;
+  k_prec_tiles<<<(rows + 127) / 128, 128, 0, s>>>(mode, N, tiles);
+  return cudaGetLastError();
+}
+
 size_t prec_tc_smem() { return kTcStages * kStageBytes + 1024 + 256; }
 
 cudaError_t launch_prec_prep(const float* X, const uint8_t* mask, int T, int N, int Np, int Tp, float* mu,
-                             PrecOperands op, cudaStream_t s) {
-  k_prec_colmean<<<(N + 31) / 32, dim3(32, 8), 0, s>>>(X, mask, T, N, mu);
+                             double2* part, PrecOperands op, cudaStream_t s) {
+  const int nchunk = prec_colmean_chunks(T);
+  const int tchunk = (T + nchunk - 1) / nchunk;
+  k_prec_colpart<<<dim3((N + 31) / 32, nchunk), dim3(32, 8), 0, s>>>(X, mask, T, N, Np, tchunk, part);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  k_prec_colmean<<<(N + 255) / 256, 256, 0, s>>>(part, nchunk, N, Np, mu);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   dim3 g((Tp + 31) / 32, (Np + 31) / 32), b(32, 8);
   k_prec_split<<<g, b, 0, s>>>(X, mask, mu, T, N, Tp, op);
   return cudaGetLastError();

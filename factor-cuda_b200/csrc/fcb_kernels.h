@@ -100,8 +100,15 @@ struct PrecOperands {
 // corr_tc.cu
 constexpr int kPrecTileTcM = 128, kPrecTileTcN = 32, kPrecTileFp32 = 64;
 size_t prec_tc_smem();
+// Tile list of a precision form (mode 0 BF16x3, 1 FP32) built on the device;
+// prec_tile_count gives its length.
+int prec_tile_count(int mode, int N);
+cudaError_t launch_prec_tiles(int mode, int N, int2* tiles, cudaStream_t s);
+// Column means (two steps; part: prec_colmean_chunks(T) * Np double2 scratch)
+// and the split operands.
+int prec_colmean_chunks(int T);
 cudaError_t launch_prec_prep(const float* X, const uint8_t* mask, int T, int N, int Np, int Tp, float* mu,
-                             PrecOperands op, cudaStream_t s);
+                             double2* part, PrecOperands op, cudaStream_t s);
 cudaError_t launch_corr_bf16x3(const PrecOperands& op, const int2* tiles, int ntiles, int N, int Np, int Tp,
                                double* out, int* status, cudaStream_t s);
 cudaError_t launch_corr_fp32(const PrecOperands& op, const int2* tiles, int ntiles, int N, int Tp, double* out,
