@@ -27,7 +27,7 @@ enum Slot : int {
   S_SC_RAW, S_SC_C, S_SC_M, S_SC_ST, S_SC_SUM, S_FB_LIST, S_FB_CNT,
   S_FC_COLPART, S_FC_COLSTAT, S_FC_GRAM, S_FC_FLAGS, S_FC_FBPART,
   S_PC_MU, S_PC_XH, S_PC_XM, S_PC_XL, S_PC_QH, S_PC_QM, S_PC_QL, S_PC_M16, S_PC_X32, S_PC_Q32, S_PC_M32, S_PC_TILES, S_PC_X, S_PC_MASK,
-  S_PC_OUT, S_PC_CPART,
+  S_PC_OUT, S_PC_CPART, S_GSCR,
   // streamed panel: three chunk buffers each (upload / compute / download in flight)
   S_PX0, S_PX1, S_PX2, S_PR0, S_PR1, S_PR2, S_PFM0, S_PFM1, S_PFM2, S_PRM0, S_PRM1, S_PRM2,
   S_PRK0, S_PRK1, S_PRK2, S_PIC,
@@ -224,14 +224,23 @@ extern "C" int fcb_dev_cs_rank_f32(const float* d_x, const uint8_t* d_mask, int 
   if (d_x == nullptr || d_out == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
   if (N > (1 << 24)) return FCB_ERR_CAP2;
   if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
-  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (N > kSmemRankCap) {
+    // global-memory path; scratch is stream-ordered (no host synchronisation)
+    const size_t bytes = rank_global_scratch(rank_global_bytes_per_date(0, N, 1, 4, 4), T);
+    void* scr = nullptr;
+    FCB_TRY(cudaMallocAsync(&scr, bytes, s));
+    const cudaError_t e = launch_cs_rank_global(d_x, d_mask, T, N, desc, d_out, static_cast<uint8_t*>(scr), bytes, s);
+    FCB_TRY(cudaFreeAsync(scr, s));
+    return rc(e);
+  }
   static int* d_status = nullptr;  // status sink for the asynchronous variant
   static std::mutex mu;
   {
     std::lock_guard<std::mutex> g(mu);
     if (d_status == nullptr) FCB_TRY(cudaMalloc(&d_status, sizeof(int)));
   }
-  return rc(launch_cs_rank(d_x, d_mask, T, N, desc, d_out, d_status, static_cast<cudaStream_t>(stream)));
+  return rc(launch_cs_rank(d_x, d_mask, T, N, desc, d_out, d_status, s));
 }
 
 extern "C" int fcb_cs_rank_f32(const float* x, const uint8_t* mask, int T, int N, int desc, float* out,
@@ -239,7 +248,6 @@ extern "C" int fcb_cs_rank_f32(const float* x, const uint8_t* mask, int T, int N
   if (x == nullptr || out == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
   if (N > (1 << 24)) return FCB_ERR_CAP2;
   if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
-  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
   WsScope sc(wsp);
   fcb_workspace& ws = *sc.ws;
   FCB_TRY(ws.bind());
@@ -255,7 +263,14 @@ extern "C" int fcb_cs_rank_f32(const float* x, const uint8_t* mask, int T, int N
   FCB_TRY(cudaMemcpyAsync(dx, x, n * 4, cudaMemcpyHostToDevice, s));
   if (mask != nullptr) FCB_TRY(cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, s));
   FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), s));
-  FCB_TRY(launch_cs_rank(dx, dm, T, N, desc, dout, dst, s));
+  if (N > kSmemRankCap) {
+    const size_t bytes = rank_global_scratch(rank_global_bytes_per_date(0, N, 1, 4, 4), T);
+    uint8_t* scr;
+    FCB_TRY(ws.get(S_GSCR, bytes, &scr));
+    FCB_TRY(launch_cs_rank_global(dx, dm, T, N, desc, dout, scr, bytes, s));
+  } else {
+    FCB_TRY(launch_cs_rank(dx, dm, T, N, desc, dout, dst, s));
+  }
   int hst = 0;
   FCB_TRY(cudaMemcpyAsync(out, dout, n * 4, cudaMemcpyDeviceToHost, s));
   FCB_TRY(cudaMemcpyAsync(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -281,7 +296,6 @@ extern "C" int fcb_parameter_scan_f32(const float* x, const uint8_t* mask, int T
   }
   if (N > (1 << 24)) return FCB_ERR_CAP2;
   if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
-  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
   for (int g = 0; g < 4; ++g) {
     if (time_ms) time_ms[g] = 0.0;
     if (time_gpu_ms) time_gpu_ms[g] = 0.0f;
@@ -304,6 +318,10 @@ extern "C" int fcb_parameter_scan_f32(const float* x, const uint8_t* mask, int T
   FCB_TRY(cudaMemcpyAsync(dx, x, n * 4, cudaMemcpyHostToDevice, s));
   if (mask != nullptr) FCB_TRY(cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, s));
   FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), s));
+  const bool global_path = N > kSmemRankCap;
+  uint8_t* scr = nullptr;
+  const size_t scr_bytes = rank_global_scratch(rank_global_bytes_per_date(1, N, 1, 4, 4), T);
+  if (global_path) FCB_TRY(ws.get(S_GSCR, scr_bytes, &scr));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   FCB_TRY(cudaEventCreate(&e0));
   cudaError_t e = cudaEventCreate(&e1);
@@ -317,7 +335,9 @@ extern "C" int fcb_parameter_scan_f32(const float* x, const uint8_t* mask, int T
   };
   e = cudaEventRecord(e0, s);
   const auto t0 = std::chrono::steady_clock::now();
-  cudaError_t le = (e == cudaSuccess) ? launch_param_scan(dx, dm, T, N, so, dst, s) : e;
+  cudaError_t le = (e != cudaSuccess) ? e
+                   : global_path ? launch_param_scan_global(dx, dm, T, N, so, scr, scr_bytes, s)
+                                 : launch_param_scan(dx, dm, T, N, so, dst, s);
   if (le != cudaSuccess) {
     cudaError_t se = cudaStreamSynchronize(s);
     cleanup();
@@ -354,8 +374,13 @@ extern "C" int fcb_parameter_scan_f32(const float* x, const uint8_t* mask, int T
 // rolling_ic (single factor) and the batched panel
 // ---------------------------------------------------------------------------
 template <typename TF, typename TR>
-static int run_rank_ic(const RankIcArgs<TF, TR>& a, int* dst, cudaStream_t s) {
-  return rc(launch_rank_ic<TF, TR>(a, dst, s));
+static int run_rank_ic(const RankIcArgs<TF, TR>& a, int* dst, cudaStream_t s, fcb_workspace& ws) {
+  if (rank_ic_fits_smem<TF, TR>(a.N)) return rc(launch_rank_ic<TF, TR>(a, dst, s));
+  const size_t bytes =
+      rank_global_scratch(rank_global_bytes_per_date(2, a.N, a.F, sizeof(TF), sizeof(TR)), a.T);
+  uint8_t* scr;
+  FCB_TRY(ws.get(S_GSCR, bytes, &scr));
+  return rc(launch_rank_ic_global<TF, TR>(a, scr, bytes, s));
 }
 
 extern "C" int fcb_rolling_ic(const void* f, int fdt, const void* r, int rdt, const uint8_t* fmask,
@@ -367,7 +392,6 @@ extern "C" int fcb_rolling_ic(const void* f, int fdt, const void* r, int rdt, co
   if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
   if ((fdt != FCB_DTYPE_F32 && fdt != FCB_DTYPE_F64) || (rdt != FCB_DTYPE_F32 && rdt != FCB_DTYPE_F64))
     return FCB_ERR_ARG;
-  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
   WsScope sc(wsp);
   fcb_workspace& ws = *sc.ws;
   FCB_TRY(ws.bind());
@@ -397,19 +421,19 @@ extern "C" int fcb_rolling_ic(const void* f, int fdt, const void* r, int rdt, co
   if (fdt == FCB_DTYPE_F32 && rdt == FCB_DTYPE_F32)
     e = run_rank_ic(RankIcArgs<float, float>{static_cast<const float*>(df), static_cast<const float*>(dr), dfm, drm,
                                              1, T, N, min_valid, nullptr, dic, drf, drr},
-                    dst, s);
+                    dst, s, ws);
   else if (fdt == FCB_DTYPE_F32)
     e = run_rank_ic(RankIcArgs<float, double>{static_cast<const float*>(df), static_cast<const double*>(dr), dfm,
                                               drm, 1, T, N, min_valid, nullptr, dic, drf, drr},
-                    dst, s);
+                    dst, s, ws);
   else if (rdt == FCB_DTYPE_F32)
     e = run_rank_ic(RankIcArgs<double, float>{static_cast<const double*>(df), static_cast<const float*>(dr), dfm,
                                               drm, 1, T, N, min_valid, nullptr, dic, drf, drr},
-                    dst, s);
+                    dst, s, ws);
   else
     e = run_rank_ic(RankIcArgs<double, double>{static_cast<const double*>(df), static_cast<const double*>(dr),
                                                dfm, drm, 1, T, N, min_valid, nullptr, dic, drf, drr},
-                    dst, s);
+                    dst, s, ws);
   if (e != 0) return e;
   int hst = 0;
   FCB_TRY(cudaMemcpyAsync(ic, dic, static_cast<size_t>(T) * 8, cudaMemcpyDeviceToHost, s));
@@ -427,7 +451,7 @@ static int panel_args_check(const void* x, const void* r, const double* ic, int 
   if (x == nullptr || r == nullptr || ic == nullptr || F < 1 || T < 1 || N < 1) return FCB_ERR_ARG;
   if (min_valid < 2) return FCB_ERR_CAP4;
   if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
-  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
+  if (N > (1 << 24)) return FCB_ERR_CAP2;
   if (method != 0 && method != 1) return FCB_ERR_ARG;
   return FCB_OK;
 }
@@ -445,7 +469,15 @@ extern "C" int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const u
     if (d_status == nullptr) FCB_TRY(cudaMalloc(&d_status, sizeof(int)));
   }
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr};
-  return rc(launch_rank_ic<float, float>(a, d_status, static_cast<cudaStream_t>(stream)));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (rank_ic_fits_smem<float, float>(N)) return rc(launch_rank_ic<float, float>(a, d_status, s));
+  // global-memory path; scratch is stream-ordered (no host synchronisation)
+  const size_t bytes = rank_global_scratch(rank_global_bytes_per_date(2, N, F, 4, 4), T);
+  void* scr = nullptr;
+  FCB_TRY(cudaMallocAsync(&scr, bytes, s));
+  const cudaError_t e = launch_rank_ic_global<float, float>(a, static_cast<uint8_t*>(scr), bytes, s);
+  FCB_TRY(cudaFreeAsync(scr, s));
+  return rc(e);
 }
 
 // Host panel: dates are streamed in chunks through three buffer sets so that
@@ -475,7 +507,9 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
   if (Tc < 1) Tc = 1;
   if (Tc > T) Tc = T;
   const int nchunk = (T + Tc - 1) / Tc;
-  const bool learned = (method == 1);
+  // learned splitters need the shared-memory kernel; wider sections are ranked
+  // by the global-memory radix path (identical results)
+  const bool learned = (method == 1) && rank_ic_fits_smem<float, float>(N);
   const bool need_ranks = ranks != nullptr || learned;
   float* dx[NB];
   float* dr[NB];
@@ -548,7 +582,8 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
     } else {
       RankIcArgs<float, float> a{dx[j], dr[j], dfm[j], drm[j], F, tc, N, min_valid, drk[j], dic + t0, nullptr, nullptr};
       a.ic_ld = T;
-      FCB_TRY(launch_rank_ic<float, float>(a, dst, s_c));
+      const int e = run_rank_ic(a, dst, s_c, ws);
+      if (e != 0) return e;
     }
     if (learned) {
       ws.since_fit += tc;

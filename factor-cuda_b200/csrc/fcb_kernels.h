@@ -123,6 +123,29 @@ cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const d
 size_t fc_gram_smem(int Fp, int tasks_per_block);
 cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
                                double* out, uint8_t* flags, cudaStream_t s);
+// Global-memory rank path for cross-sections the shared-memory kernels cannot
+// hold (rank_global.cu).  kind 0 cs_rank, 1 parameter_scan, 2 rank+IC: bytes
+// of scratch one date needs; the launchers process dates in chunks that fit
+// the scratch they are given (at least one date's worth).
+size_t rank_global_bytes_per_date(int kind, int N, int F, int ksz_f, int ksz_r);
+cudaError_t launch_cs_rank_global(const float* X, const uint8_t* mask, int T, int N, int desc, float* out,
+                                  uint8_t* scratch, size_t bytes, cudaStream_t s);
+cudaError_t launch_param_scan_global(const float* X, const uint8_t* mask, int T, int N, ScanOut outs,
+                                     uint8_t* scratch, size_t bytes, cudaStream_t s);
+template <typename TF, typename TR>
+cudaError_t launch_rank_ic_global(const RankIcArgs<TF, TR>& a, uint8_t* scratch, size_t bytes, cudaStream_t s);
+// True when the shared-memory rank+IC kernel takes N for these dtypes.
+template <typename TF, typename TR>
+inline bool rank_ic_fits_smem(int N) {
+  return N <= kSmemRankCap && rank_ic_smem<TF, TR>(N) <= kMaxSmemPerBlock;
+}
+inline size_t rank_global_scratch(size_t per_date, int T) {
+  size_t b = per_date * static_cast<size_t>(T);
+  if (b > (size_t(1) << 30)) b = size_t(1) << 30;  // chunks of about 1 GiB
+  if (b < per_date) b = per_date;
+  return b + 8192;
+}
+
 // Persistent rank+IC over (panel, date) items; nt in {256, 512, 1024}.  With
 // occ != nullptr nothing is launched: *occ receives the CTAs per SM that fit.
 template <typename TF, typename TR>

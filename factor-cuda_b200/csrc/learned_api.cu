@@ -219,11 +219,24 @@ int fcb::rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d
   if (F != model->F) return FCB_ERR_ARG;
   if (min_valid < 2) return FCB_ERR_CAP4;
   if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
-  if (N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
+  if (N > (1 << 24)) return FCB_ERR_CAP2;
   static int* d_status = nullptr;
   if (d_status == nullptr) FCB_TRY(cudaMalloc(&d_status, sizeof(int)));
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr,
                              model->table[model->cur], model->zrange[model->cur], cap > 0 ? cap : 64, d_stats,
                              ic_ld};
-  return rc(launch_rank_ic_learned(a, d_status, stream));
+  if (rank_ic_fits_smem<float, float>(N)) return rc(launch_rank_ic_learned(a, d_status, stream));
+  // too wide for the shared-memory kernel: the global-memory radix path ranks
+  // the section (identical results); statistics read outcome 0 (not learned)
+  if (d_stats != nullptr)
+    FCB_TRY(cudaMemsetAsync(d_stats, 0, static_cast<size_t>(F) * T * 4 * sizeof(int), stream));
+  a.cdf_table = nullptr;
+  a.cdf_zrange = nullptr;
+  a.learn_stats = nullptr;
+  const size_t bytes = rank_global_scratch(rank_global_bytes_per_date(2, N, F, 4, 4), T);
+  void* scr = nullptr;
+  FCB_TRY(cudaMallocAsync(&scr, bytes, stream));
+  const cudaError_t e = launch_rank_ic_global<float, float>(a, static_cast<uint8_t*>(scr), bytes, stream);
+  FCB_TRY(cudaFreeAsync(scr, stream));
+  return rc(e);
 }

@@ -80,7 +80,12 @@ void fcb_host_free(void* p);
  * finite && mask; ranks 1..K by ascending value (descending: of -x), ties by
  * column; invalid cells get the quiet NaN 0x7fc00000.
  * Replaces cs_rank_gpu (src/cross_sectional_rank.cuh:90-99).
- * Returns -1 null/dim, -2 N > 2^24, -3 T*N > INT32_MAX. */
+ * Returns -1 null/dim, -2 N > 2^24, -3 T*N > INT32_MAX.
+ * Every N up to the cap is served: sections that fit one CTA's shared memory
+ * (N <= 16384 for cs_rank / parameter_scan; about 11000 f32 and 8192 f64 for
+ * the fused rank + IC entry points) are sorted there, wider ones by a
+ * global-memory radix sort per date with the same results (scratch from the
+ * workspace, or stream-ordered cudaMallocAsync for the fcb_dev_* variants). */
 int fcb_cs_rank_f32(const float* x, const uint8_t* mask, int T, int N, int descending, float* out,
                     fcb_workspace* ws);
 
@@ -189,7 +194,9 @@ int fcb_cdf_grad(const float* params, const float* z, const float* u, int n, flo
  * (NULL = off) receives (F,T,4) ints: outcome (1 learned, 2 bucket overflow,
  * 3 judge rejected, 4 unusable scale; 2-4 fell back to radix), the largest
  * bucket, the sum of squared bucket sizes (the per-date comparison work; m
- * for perfectly even buckets of one) and m, the number of ranked cells. */
+ * for perfectly even buckets of one) and m, the number of ranked cells.
+ * Sections too wide for the shared-memory kernel are ranked by the
+ * global-memory radix path (same results); their statistics read 0. */
 int fcb_dev_rank_ic_panel_learned(const float* d_x, const float* d_r, const uint8_t* d_fmask,
                                   const uint8_t* d_rmask, int F, int T, int N, int min_valid, float* d_ranks,
                                   double* d_ic, const fcb_cdf_model* model, int cap, int* d_stats, void* stream);
@@ -249,7 +256,8 @@ int fcb_dev_factor_corr_noalloc(const void* d_x, int dtype, const uint8_t* d_mas
 typedef struct fcb_batch fcb_batch;
 
 typedef struct fcb_panel {
-  int T, N, F;                 /* N <= 16384 (else FCB_ERR_UNSUPPORTED)          */
+  int T, N, F;                 /* N within one CTA's shared memory (rank + IC: about
+                                  11000 f32, 8192 f64), else FCB_ERR_UNSUPPORTED  */
   const void* X;               /* F factor planes, each (T,N), dtype_x           */
   const void* R;               /* (T,N) forward returns, dtype_r                 */
   const uint8_t* fmask;        /* (T,N) factor mask or NULL                      */

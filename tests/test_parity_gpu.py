@@ -78,8 +78,6 @@ def test_golden_rolling_ic(golden, fcb):
         r = A[c["inputs"][1]]
         if f.ndim == 1:
             f, r = f[None, :], r[None, :]
-        if f.shape[1] > _ic_cap(f.dtype, r.dtype):
-            continue  # covered by the global-memory path tests
         fm = A[c["masks"]["factor_mask"]] if "factor_mask" in c["masks"] else None
         rm = A[c["masks"]["fwd_mask"]] if "fwd_mask" in c["masks"] else None
         got = fcb.rolling_ic_f64(f, r, fm, rm, c["params"]["min_valid"])
