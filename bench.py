@@ -338,19 +338,28 @@ def run_b200(args, rank, world):
     return finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info)
 
 
+# DRAM bytes of one k_rank_ic launch per date at N=5000, F=12, from one ncu capture
+# each at T=600 (profiles/k_rank_ic_learned_T600_N5000_F12.md): dram__bytes_read.sum +
+# dram__bytes_write.sum.  Traffic grows with the number of dates at fixed N and F, so
+# the bench's launch is that times T.
+TRAFFIC_PER_DATE = {"learned": (162.197760e6 + 101.510400e6) / 600,
+                    "radix": (162.098688e6 + 101.336576e6) / 600}
+
+
 def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info=None):
     import torch
     F, T, N = X.shape
     ms_all, e2e_all = ms, (e2e_s if e2e_s is not None else 0.0)
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
+        t = torch.tensor([ms, e2e_s if e2e_s is not None else 0.0], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_all, e2e_all = float(t[0]), float(t[1])
     cells = F * T * N
     peak, peak_kind = measured_peaks()
     bytes_launch = algorithmic_bytes(F, T, N)
     achieved = bytes_launch / (ms / 1e3) / 1e9
+    traffic = TRAFFIC_PER_DATE[args.method] * T if (N, F) == (5000, 12) else None
     res = {
         "metric": METRIC, "value": world * cells / (ms_all / 1e3) / 1e9, "unit": "Gelem/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all,
@@ -366,7 +375,8 @@ def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned
                 "api": "fcb_rank_ic_panel (C ABI, pinned host buffers, date-chunked streaming)",
                 "matches_device_path": e2e_ok},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "traffic_source": "ncu dram bytes at T=600 scaled by T/600" if traffic else None,
                      "kernel": "k_rank_ic", "algorithmic_bytes_per_launch": bytes_launch},
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
