@@ -346,22 +346,34 @@ TRAFFIC_PER_DATE = {"learned": (162.197760e6 + 101.510400e6) / 600,
                     "radix": (162.098688e6 + 101.336576e6) / 600}
 
 
-def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info=None):
+def max_over_ranks(values, device):
+    """Element-wise maximum of a list of floats over every rank of the process
+    group: a replica job is as slow as its slowest rank."""
     import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def job_throughput(world, cells_per_rank, ms_max):
+    """Whole-job Gelem/s of `world` replicas, each ranking `cells_per_rank`
+    cells, timed by the slowest rank."""
+    return world * cells_per_rank / (ms_max / 1e3) / 1e9
+
+
+def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info=None):
     F, T, N = X.shape
     ms_all, e2e_all = ms, (e2e_s if e2e_s is not None else 0.0)
     if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms, e2e_s if e2e_s is not None else 0.0], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_all, e2e_all = float(t[0]), float(t[1])
+        ms_all, e2e_all = max_over_ranks([ms, e2e_all], dev)
     cells = F * T * N
     peak, peak_kind = measured_peaks()
     bytes_launch = algorithmic_bytes(F, T, N)
     achieved = bytes_launch / (ms / 1e3) / 1e9
     traffic = TRAFFIC_PER_DATE[args.method] * T if (N, F) == (5000, 12) else None
     res = {
-        "metric": METRIC, "value": world * cells / (ms_all / 1e3) / 1e9, "unit": "Gelem/s",
+        "metric": METRIC, "value": job_throughput(world, cells, ms_all), "unit": "Gelem/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded stand-in for the 1218x5000x12 corpus panel)",
