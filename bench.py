@@ -486,6 +486,113 @@ def bench_batch(dev, steps=5, warmup=2):
     return res
 
 
+def make_c5_block(dev, g, rng, state, F, Tb, N, start):
+    """One block of Tb dates of the learned-splitter streaming panel, on the
+    device.  Per factor: AR(1) (phi = 0.98) drift of the mean and of the log
+    scale; 70 % of the factors Gaussian, 30 % lognormal(sigma = 0.8); 0.5 %
+    exact duplicates (a cell copies another cell of the same date); stocks
+    missing before a per-stock listing date (10 % of cells on average).
+    `state` carries the drifts from block to block."""
+    import torch
+    nan = float("nan")
+    t_idx = torch.arange(start, start + Tb, device=dev)
+    mu = torch.empty((F, Tb), device=dev)
+    ls = torch.empty((F, Tb), device=dev)
+    m, l = state[0], state[1]
+    for t in range(Tb):
+        m = 0.98 * m + 0.05 * torch.randn(F, generator=g, device=dev)
+        l = 0.98 * l + 0.05 * torch.randn(F, generator=g, device=dev)
+        mu[:, t] = m
+        ls[:, t] = l
+    state[0], state[1] = m, l
+    base = torch.randn((F, Tb, N), generator=g, device=dev)
+    nlog = int(round(0.3 * F))
+    base[F - nlog:] = torch.exp(0.8 * base[F - nlog:])
+    X = (mu[:, :, None] + torch.exp(ls)[:, :, None] * base).float()
+    dup = torch.rand((F, Tb, N), generator=g, device=dev) < 0.005
+    src = torch.randint(0, N, (F, Tb, N), generator=g, device=dev)
+    X = torch.where(dup, torch.gather(X, 2, src), X)
+    listed = t_idx[:, None] >= state[2][None, :]
+    X.masked_fill_(~listed[None], nan)
+    R = 0.03 * torch.nan_to_num(X[0]) + torch.randn((Tb, N), generator=g, device=dev)
+    R.masked_fill_(~listed, nan)
+    return X.contiguous(), R.float().contiguous(), listed.to(torch.uint8), torch.isfinite(R).to(torch.uint8)
+
+
+def bench_c5(dev, T=5000, N=8000, F=128, Tb=250, seed=20261206):
+    """Learned splitters on the streaming configuration (T=5000, N=8000,
+    F=128: 5.12 G cells, 20.5 GB of f32 factors, device-resident in blocks of
+    250 dates).  The CDF networks are fitted on the exact ranks of dates
+    [0, 500) and refitted on every later block's ranks before the next block;
+    every block is ranked by the learned path and by the plain radix path, and
+    the two outputs are compared bit for bit."""
+    import torch
+    import fcb200
+    from fcb200 import _native as nat
+    lib = nat.lib()
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    state = [torch.zeros(F, device=dev), torch.zeros(F, device=dev),
+             torch.from_numpy(rng.integers(0, int(0.2 * T), N)).to(dev)]
+    blocks = [make_c5_block(dev, g, rng, state, F, Tb, N, b * Tb) for b in range(T // Tb)]
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+    ranks_r = torch.empty((F, Tb, N), dtype=torch.float32, device=dev)
+    ranks_l = torch.empty_like(ranks_r)
+    ic_r = torch.empty((F, Tb), dtype=torch.float64, device=dev)
+    ic_l = torch.empty_like(ic_r)
+    stats = torch.zeros((F, Tb, 4), dtype=torch.int32, device=dev)
+    model = fcb200.CdfModel(F, seed=seed)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    t_radix = t_radix_lb = t_learn = t_fit = 0.0
+    exact = True
+    codes = []
+    learned_cells = 0
+    for b, (X, R, fm, rm) in enumerate(blocks):
+        ev[0].record(stream)
+        nat.check(lib.fcb_dev_rank_ic_panel(X.data_ptr(), R.data_ptr(), fm.data_ptr(), rm.data_ptr(), F, Tb, N,
+                                            MIN_VALID, ranks_r.data_ptr(), ic_r.data_ptr(), 0, s), "radix")
+        ev[1].record(stream)
+        if b >= 2:
+            nat.check(lib.fcb_dev_rank_ic_panel_learned(X.data_ptr(), R.data_ptr(), fm.data_ptr(), rm.data_ptr(), F,
+                                                        Tb, N, MIN_VALID, ranks_l.data_ptr(), ic_l.data_ptr(),
+                                                        model.handle, 64, stats.data_ptr(), s), "learned")
+        ev[2].record(stream)
+        # fit on the exact ranks of this block: dates [0, 500) first, then a refit per block
+        if b == 0:
+            model.fit(X, ranks_r, Tb, N, 0, Tb, steps=1500, lr=3e-3, stream=s)
+        else:
+            model.fit(X, ranks_r, Tb, N, 0, Tb, steps=300 if b == 1 else 100, lr=1e-3, stream=s)
+        ev[3].record(stream)
+        torch.cuda.synchronize(dev)
+        t_radix += ev[0].elapsed_time(ev[1])
+        t_fit += ev[2].elapsed_time(ev[3])
+        if b >= 2:
+            t_learn += ev[1].elapsed_time(ev[2])
+            t_radix_lb += ev[0].elapsed_time(ev[1])
+            learned_cells += F * Tb * N
+            exact = exact and bool(torch.equal(ranks_l.view(torch.int32), ranks_r.view(torch.int32))) and \
+                bool(torch.equal(torch.nan_to_num(ic_l, nan=7.0), torch.nan_to_num(ic_r, nan=7.0)))
+            codes.append(stats[..., 0].flatten().cpu().numpy())
+    codes = np.concatenate(codes)
+    res = {"workload": f"learned splitters, streaming: T={T}, N={N}, F={F} ({F * T * N / 1e9:.2f} G cells, "
+                       f"{F * T * N * 4 / 1e9:.1f} GB f32), blocks of {Tb} dates; fit on dates [0, {2 * Tb}), "
+                       f"refit after every block",
+           "learned_gelem_s": learned_cells / (t_learn / 1e3) / 1e9,
+           "radix_gelem_s": F * T * N / (t_radix / 1e3) / 1e9,
+           "speedup_vs_radix": (t_radix_lb / t_learn) if t_learn > 0 else None,
+           "learned_fraction": float((codes == 1).mean()),
+           "fallback_overflow": float((codes == 2).mean()), "fallback_judge": float((codes == 3).mean()),
+           "fallback_scale": float((codes == 4).mean()),
+           "bit_exact_vs_radix": exact, "fit_ms_total": t_fit,
+           "cells_ranked_learned": learned_cells}
+    del blocks
+    torch.cuda.empty_cache()
+    return res
+
+
 def bench_stock_corr(dev, N, T=1218, steps=5, warmup=2):
     """stock_corr precision forms on one (T,N) panel, device-resident:
     BF16x3 tensor-core path vs plain FP32, error against the f64 path."""
@@ -596,6 +703,9 @@ def main():
                     help="run only the stock_corr precision leg at this N (profiling)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-panel leg")
     ap.add_argument("--only-batch", action="store_true", help="run only the batched uneven-panel leg")
+    ap.add_argument("--no-c5", action="store_true", help="skip the learned-splitter streaming leg")
+    ap.add_argument("--only-c5", action="store_true",
+                    help="run only the learned-splitter streaming leg (T=5000, N=8000, F=128)")
     ap.add_argument("--T", type=int, default=T_DEF)
     ap.add_argument("--N", type=int, default=N_DEF)
     ap.add_argument("--F", type=int, default=F_DEF)
@@ -607,6 +717,10 @@ def main():
         import torch
         print(json.dumps(bench_stock_corr(torch.device("cuda", 0), args.only_stock_corr, steps=args.steps,
                                           warmup=args.warmup)))
+        return
+    if args.only_c5:
+        import torch
+        print(json.dumps(bench_c5(torch.device("cuda", 0))))
         return
     if args.only_batch:
         import torch
@@ -641,6 +755,9 @@ def main():
     if not args.no_batch:
         import torch
         res["batch"] = bench_batch(torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+    if not args.no_c5:
+        import torch
+        res["c5_learned_streaming"] = bench_c5(torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
     if rank == 0:
         if not args.no_cpu_baseline:
             X, R, fm, rm = make_panel()
