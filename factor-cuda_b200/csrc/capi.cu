@@ -11,6 +11,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/fcb200.h"
@@ -27,7 +28,7 @@ enum Slot : int {
   S_SC_RAW, S_SC_C, S_SC_M, S_SC_ST, S_SC_SUM, S_FB_LIST, S_FB_CNT,
   S_FC_COLPART, S_FC_COLSTAT, S_FC_GRAM, S_FC_FLAGS, S_FC_FBPART,
   S_PC_MU, S_PC_XH, S_PC_XM, S_PC_XL, S_PC_QH, S_PC_QM, S_PC_QL, S_PC_M16, S_PC_X32, S_PC_Q32, S_PC_M32, S_PC_TILES, S_PC_X, S_PC_MASK,
-  S_PC_OUT, S_PC_CPART, S_GSCR,
+  S_PC_OUT, S_PC_CPART, S_GSCR, S_RICPREP,
   // streamed panel: three chunk buffers each (upload / compute / download in flight)
   S_PX0, S_PX1, S_PX2, S_PR0, S_PR1, S_PR2, S_PFM0, S_PFM1, S_PFM2, S_PRM0, S_PRM1, S_PRM2,
   S_PRK0, S_PRK1, S_PRK2, S_PIC,
@@ -156,6 +157,35 @@ bool is_group_whitelist(cudaError_t e) {
 // ---------------------------------------------------------------------------
 // housekeeping
 // ---------------------------------------------------------------------------
+namespace fcb {
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  cudaMemPool_t pool;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (pools[dev] == nullptr) {
+      cudaMemPoolProps props{};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      e = cudaMemPoolCreate(&pools[dev], &props);
+      if (e != cudaSuccess) return e;
+      uint64_t keep = ~0ull;  // keep freed blocks for the next call
+      e = cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) return e;
+    }
+    pool = pools[dev];
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
+cudaError_t scratch_free(void* p, cudaStream_t s) { return cudaFreeAsync(p, s); }
+}  // namespace fcb
+
 extern "C" fcb_workspace* fcb_workspace_create(void) { return new (std::nothrow) fcb_workspace(); }
 
 extern "C" void fcb_workspace_clear(fcb_workspace* ws) {
@@ -229,9 +259,9 @@ extern "C" int fcb_dev_cs_rank_f32(const float* d_x, const uint8_t* d_mask, int 
     // global-memory path; scratch is stream-ordered (no host synchronisation)
     const size_t bytes = rank_global_scratch(rank_global_bytes_per_date(0, N, 1, 4, 4), T);
     void* scr = nullptr;
-    FCB_TRY(cudaMallocAsync(&scr, bytes, s));
+    FCB_TRY(scratch_alloc(&scr, bytes, s));
     const cudaError_t e = launch_cs_rank_global(d_x, d_mask, T, N, desc, d_out, static_cast<uint8_t*>(scr), bytes, s);
-    FCB_TRY(cudaFreeAsync(scr, s));
+    FCB_TRY(scratch_free(scr, s));
     return rc(e);
   }
   static int* d_status = nullptr;  // status sink for the asynchronous variant
@@ -375,7 +405,17 @@ extern "C" int fcb_parameter_scan_f32(const float* x, const uint8_t* mask, int T
 // ---------------------------------------------------------------------------
 template <typename TF, typename TR>
 static int run_rank_ic(const RankIcArgs<TF, TR>& a, int* dst, cudaStream_t s, fcb_workspace& ws) {
-  if (rank_ic_fits_smem<TF, TR>(a.N)) return rc(launch_rank_ic<TF, TR>(a, dst, s));
+  if (rank_ic_fits_smem<TF, TR>(a.N)) {
+    if constexpr (std::is_same<TF, float>::value && std::is_same<TR, float>::value) {
+      if (a.F >= 2) {
+        // several factors: returns prepared once per date, one CTA per (date, factor)
+        void* prep;
+        FCB_TRY(ws.get(S_RICPREP, ric_prep_bytes(a.T, a.N), &prep));
+        return rc(launch_rank_ic_items<TF, TR>(a, ric_prep_carve(prep, a.T, a.N), false, dst, s));
+      }
+    }
+    return rc(launch_rank_ic<TF, TR>(a, dst, s));
+  }
   const size_t bytes =
       rank_global_scratch(rank_global_bytes_per_date(2, a.N, a.F, sizeof(TF), sizeof(TR)), a.T);
   uint8_t* scr;
@@ -470,13 +510,21 @@ extern "C" int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const u
   }
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (rank_ic_fits_smem<float, float>(N)) return rc(launch_rank_ic<float, float>(a, d_status, s));
+  if (rank_ic_fits_smem<float, float>(N)) {
+    if (F < 2) return rc(launch_rank_ic<float, float>(a, d_status, s));
+    // several factors: returns prepared once per date, one CTA per (date, factor)
+    void* prep = nullptr;
+    FCB_TRY(scratch_alloc(&prep, ric_prep_bytes(T, N), s));
+    const cudaError_t e = launch_rank_ic_items<float, float>(a, ric_prep_carve(prep, T, N), false, d_status, s);
+    FCB_TRY(scratch_free(prep, s));
+    return rc(e);
+  }
   // global-memory path; scratch is stream-ordered (no host synchronisation)
   const size_t bytes = rank_global_scratch(rank_global_bytes_per_date(2, N, F, 4, 4), T);
   void* scr = nullptr;
-  FCB_TRY(cudaMallocAsync(&scr, bytes, s));
+  FCB_TRY(scratch_alloc(&scr, bytes, s));
   const cudaError_t e = launch_rank_ic_global<float, float>(a, static_cast<uint8_t*>(scr), bytes, s);
-  FCB_TRY(cudaFreeAsync(scr, s));
+  FCB_TRY(scratch_free(scr, s));
   return rc(e);
 }
 

@@ -123,6 +123,27 @@ cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const d
 size_t fc_gram_smem(int Fp, int tasks_per_block);
 cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
                                double* out, uint8_t* flags, cudaStream_t s);
+// Returns of each date prepared once for the per-(date, factor) rank + IC
+// kernel (rows 16-byte aligned; see k_ric_returns).
+struct RicPrep {
+  uint16_t* ir;    // (T, ld_ir) column ids of valid returns in key order
+  uint32_t* tie;   // (T, ld_tie) tie-group start bits over the sorted order
+  uint8_t* flags;  // (T, ld_fl) bit 0 returns valid, bit 1 factor mask
+  int* mr;         // (T) valid returns per date
+  int ld_ir, ld_tie, ld_fl;
+};
+size_t ric_prep_bytes(int T, int N);
+// Stream-ordered scratch for the entry points that take no workspace: a
+// library-private memory pool per device that keeps freed blocks cached.
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s);
+cudaError_t scratch_free(void* p, cudaStream_t s);
+RicPrep ric_prep_carve(void* base, int T, int N);
+// Rank + IC as one CTA per (date, factor) after a per-date returns pass:
+// T * F CTAs instead of T, so the last wave of a long panel is short.
+template <typename TF, typename TR>
+cudaError_t launch_rank_ic_items(const RankIcArgs<TF, TR>& a, RicPrep rp, bool learned, int* status,
+                                 cudaStream_t st);
+
 // Global-memory rank path for cross-sections the shared-memory kernels cannot
 // hold (rank_global.cu).  kind 0 cs_rank, 1 parameter_scan, 2 rank+IC: bytes
 // of scratch one date needs; the launchers process dates in chunks that fit

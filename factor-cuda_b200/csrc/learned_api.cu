@@ -225,7 +225,15 @@ int fcb::rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr,
                              model->table[model->cur], model->zrange[model->cur], cap > 0 ? cap : 64, d_stats,
                              ic_ld};
-  if (rank_ic_fits_smem<float, float>(N)) return rc(launch_rank_ic_learned(a, d_status, stream));
+  if (rank_ic_fits_smem<float, float>(N)) {
+    if (F < 2) return rc(launch_rank_ic_learned(a, d_status, stream));
+    // several factors: returns prepared once per date, one CTA per (date, factor)
+    void* prep = nullptr;
+    FCB_TRY(scratch_alloc(&prep, ric_prep_bytes(T, N), stream));
+    const cudaError_t e = launch_rank_ic_items<float, float>(a, ric_prep_carve(prep, T, N), true, d_status, stream);
+    FCB_TRY(scratch_free(prep, stream));
+    return rc(e);
+  }
   // too wide for the shared-memory kernel: the global-memory radix path ranks
   // the section (identical results); statistics read outcome 0 (not learned)
   if (d_stats != nullptr)
@@ -235,8 +243,8 @@ int fcb::rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d
   a.learn_stats = nullptr;
   const size_t bytes = rank_global_scratch(rank_global_bytes_per_date(2, N, F, 4, 4), T);
   void* scr = nullptr;
-  FCB_TRY(cudaMallocAsync(&scr, bytes, stream));
+  FCB_TRY(scratch_alloc(&scr, bytes, stream));
   const cudaError_t e = launch_rank_ic_global<float, float>(a, static_cast<uint8_t*>(scr), bytes, stream);
-  FCB_TRY(cudaFreeAsync(scr, stream));
+  FCB_TRY(scratch_free(scr, stream));
   return rc(e);
 }
