@@ -63,6 +63,50 @@ FCB_DEV T block_reduce_add(T v, T* scratch) {
   return t;
 }
 
+// One pass, three block results: the exclusive prefix sum of c (returned),
+// and the block maximum of mx and sum of c2 (written back).  Warp shuffles,
+// one shared slot per warp and quantity, three barriers.  scan: >= 99 u32.
+FCB_DEV uint32_t block_scan_max_sum(uint32_t c, int& mx, uint32_t& c2, uint32_t* scan) {
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  const unsigned lane = lane_id();
+  const uint32_t inc = warp_inclusive_sum(c);
+  int wm = mx;
+  uint32_t ws = c2;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    wm = max(wm, __shfl_xor_sync(kFull, wm, o));
+    ws += __shfl_xor_sync(kFull, ws, o);
+  }
+  if (lane == 31) scan[w] = inc;
+  if (lane == 0) {
+    scan[32 + w] = static_cast<uint32_t>(wm);
+    scan[64 + w] = ws;
+  }
+  __syncthreads();
+  if (w == 0) {
+    const uint32_t sv = lane < static_cast<unsigned>(nw) ? scan[lane] : 0u;
+    const uint32_t si = warp_inclusive_sum(sv);
+    int mv = lane < static_cast<unsigned>(nw) ? static_cast<int>(scan[32 + lane]) : 0;
+    uint32_t cv = lane < static_cast<unsigned>(nw) ? scan[64 + lane] : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mv = max(mv, __shfl_xor_sync(kFull, mv, o));
+      cv += __shfl_xor_sync(kFull, cv, o);
+    }
+    if (lane < static_cast<unsigned>(nw)) scan[lane] = si - sv;
+    if (lane == 0) {
+      scan[96] = static_cast<uint32_t>(mv);
+      scan[97] = cv;
+    }
+  }
+  __syncthreads();
+  const uint32_t res = scan[w] + inc - c;
+  mx = static_cast<int>(scan[96]);
+  c2 = scan[97];
+  __syncthreads();
+  return res;
+}
+
 // Outcome codes written to the per-(factor,date) statistics.
 constexpr int kLearnOk = 1, kLearnOverflow = 2, kLearnJudge = 3, kLearnScale = 4;
 
@@ -139,13 +183,10 @@ FCB_DEV int learned_sort(uint32_t* kA, uint16_t* iA, uint32_t* kB, uint16_t* iB,
       c2 += v * v;
       mx = max(mx, static_cast<int>(v));
     }
-    mx = block_max_int(mx, reinterpret_cast<int*>(scan));
+    uint32_t run = block_scan_max_sum(c, mx, c2, scan);  // mx, c2 become block totals
     if (max_bucket_out != nullptr) *max_bucket_out = mx;
-    if (mx > cap) return kLearnOverflow;  // uniform across the block
-    c2 = block_reduce_add(c2, scan);
     if (sumsq_out != nullptr) *sumsq_out = static_cast<int>(c2);
-    uint32_t total;
-    uint32_t run = block_exclusive_sum(c, scan, total);
+    if (mx > cap) return kLearnOverflow;  // uniform across the block
     for (int b = b0; b < b1; ++b) {
       const uint32_t v = cnt[b];
       cnt[b] = static_cast<uint16_t>(run);
