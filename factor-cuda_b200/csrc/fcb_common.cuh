@@ -97,6 +97,16 @@ FCB_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t max_polls = (1u 
   return false;
 }
 // dst/src 16-byte aligned, bytes a multiple of 16.
+// Prefetch [src, src + bytes) into L2 (bulk-copy engine, no shared memory,
+// no completion to wait for).  src and bytes are rounded inward to 16 bytes.
+FCB_DEV void bulk_prefetch_l2(const void* src, size_t bytes) {
+  const uintptr_t a0 = (reinterpret_cast<uintptr_t>(src) + 15) & ~uintptr_t(15);
+  const uintptr_t a1 = (reinterpret_cast<uintptr_t>(src) + bytes) & ~uintptr_t(15);
+  if (a1 <= a0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"(static_cast<uint32_t>(a1 - a0))
+               : "memory");
+}
+
 FCB_DEV void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(

@@ -139,24 +139,24 @@ FCB_DEV int learned_sort(uint32_t* kA, uint16_t* iA, uint32_t* kB, uint16_t* iB,
                          uint32_t* bits, const float* tab, float lo, float hi, int cap, double* dscratch,
                          uint32_t* scan, int* max_bucket_out, int* sumsq_out) {
   if (m <= 1) return kLearnOk;
-  // per-date standardisation: mean and mean absolute deviation of the values
-  double s = 0.0;
-  for (int p = threadIdx.x; p < m; p += NT) s += key_to_f32(kA[p]);
-  s = block_reduce_add(s, dscratch);
-  const double mean = s / m;
-  double a = 0.0;
-  for (int p = threadIdx.x; p < m; p += NT) a += fabs(key_to_f32(kA[p]) - mean);
-  a = block_reduce_add(a, dscratch);
-  const double mad = a / m;
+  // per-date standardisation: mean and mean absolute deviation of an evenly
+  // spaced sample of the compacted cells, one per thread (they only shape the
+  // bucket map; the judge below guarantees the order whatever they are)
+  const int S = min(m, NT);
+  const bool smp = static_cast<int>(threadIdx.x) < S;
+  const float sv = smp ? key_to_f32(kA[static_cast<int>((static_cast<long long>(threadIdx.x) * m) / S)]) : 0.0f;
+  const float mean = block_reduce_add(sv, reinterpret_cast<float*>(dscratch)) / static_cast<float>(S);
+  const float mad = block_reduce_add(smp ? fabsf(sv - mean) : 0.0f, reinterpret_cast<float*>(dscratch)) /
+                    static_cast<float>(S);
   BucketMap bm;
   bm.tab = tab;
-  bm.loc = static_cast<float>(mean);
-  bm.inv_scale = static_cast<float>(1.0 / mad);
+  bm.loc = mean;
+  bm.inv_scale = mad > 0.0f ? 1.0f / mad : 0.0f;
   bm.lo = lo;
   bm.inv_dz = static_cast<float>((kCdfKnots - 1) / static_cast<double>(hi - lo));
   bm.B = m;
   bm.Bf = static_cast<float>(m);
-  if (!(mad > 0.0) || !isfinite(bm.loc) || !isfinite(bm.inv_scale) || !(bm.inv_scale > 0.0f) ||
+  if (!(mad > 0.0f) || !isfinite(bm.loc) || !isfinite(bm.inv_scale) || !(bm.inv_scale > 0.0f) ||
       !isfinite(bm.inv_dz) || !(bm.inv_dz > 0.0f))
     return kLearnScale;
   // histogram (packed 16-bit counters); each cell's bucket parked in iB

@@ -614,7 +614,7 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT))
 // run side by side and share its prepared returns in L2).
 template <int NT, int MAXIPT, typename TF, typename TR, bool LEARNED>
 __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT))
-    k_rank_ic_item(RankIcArgs<TF, TR> a, RicPrep rp, int* status) {
+    k_rank_ic_item(RankIcArgs<TF, TR> a, RicPrep rp, int resident, int* status) {
   using KF = typename KeyOf<TF>::type;
   using KR = typename KeyOf<TR>::type;
   constexpr int KSZ = (sizeof(KF) > sizeof(KR)) ? int(sizeof(KF)) : int(sizeof(KR));
@@ -640,6 +640,19 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT))
     // table rows are 4 KB apart from an aligned base: the row lands at sm + L.scratch exactly
     (void)stage_issue(sm + L.scratch, a.cdf_table + static_cast<size_t>(f) * kCdfKnots, kCdfKnots, &bars[4],
                       arm[4]);
+  }
+  // items are dispatched in order: the CTA that starts when this one ends
+  // will take item blockIdx.x + resident -- bring its rows into L2 now
+  if (threadIdx.x == 0 && resident > 0) {
+    const unsigned nx = blockIdx.x + static_cast<unsigned>(resident);
+    if (nx < gridDim.x) {
+      const int tn = static_cast<int>(nx) / a.F, fn = static_cast<int>(nx) % a.F;
+      bulk_prefetch_l2(a.X + (static_cast<size_t>(fn) * a.T + tn) * N, static_cast<size_t>(N) * sizeof(TF));
+      if (fn == 0 || nx == blockIdx.x + static_cast<unsigned>(resident)) {
+        bulk_prefetch_l2(rp.flags + static_cast<size_t>(tn) * rp.ld_fl, static_cast<size_t>(N));
+        bulk_prefetch_l2(rp.ir + static_cast<size_t>(tn) * rp.ld_ir, static_cast<size_t>(N) * 2);
+      }
+    }
   }
   bool ok = stage_wait(&bars[0], ph[0], arm[0]);
   ok = stage_wait(&bars[1], ph[1], arm[1]) && ok;
@@ -894,7 +907,14 @@ static cudaError_t items_nt(const RankIcArgs<TF, TR>& a, RicPrep rp, int* status
   if (e != cudaSuccess) return e;
   const long long grid = static_cast<long long>(a.T) * a.F;
   if (grid > 2147483647LL) return cudaErrorInvalidValue;
-  k_rank_ic_item<NT, 16, TF, TR, LEARNED><<<static_cast<unsigned>(grid), NT, smem, st>>>(a, rp, status);
+  // resident CTAs (the prefetch distance)
+  int occ = 0, dev = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rank_ic_item<NT, 16, TF, TR, LEARNED>, NT, smem) !=
+          cudaSuccess ||
+      cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    occ = sms = 0;
+  k_rank_ic_item<NT, 16, TF, TR, LEARNED><<<static_cast<unsigned>(grid), NT, smem, st>>>(a, rp, occ * sms, status);
   return cudaGetLastError();
 }
 
