@@ -301,7 +301,9 @@ def run_b200(args, rank, world):
 
     # e2e: host entry point, pinned buffers, copies in the timed region
     if args.no_e2e:
-        return finish(args, world, X, R, fm, rm, ms, None, None, clk, spot, dev, learned_info)
+        res = finish(args, world, X, R, fm, rm, ms, None, None, clk, spot, dev, learned_info)
+        res["factor_corr"] = bench_factor_corr(dX, dfm, X, fm, dev, steps=max(3, args.steps // 2))
+        return res
     hX = torch.from_numpy(X).pin_memory()
     hR = torch.from_numpy(R).pin_memory()
     hfm = torch.from_numpy(fm).pin_memory()
@@ -335,7 +337,9 @@ def run_b200(args, rank, world):
     e2e_s = (time.perf_counter() - t0) / args.steps
     lib.fcb_workspace_destroy(ws)
     e2e_ok = bool(np.array_equal(hranks.numpy().view(np.uint32), dranks.cpu().numpy().view(np.uint32)))
-    return finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info)
+    res = finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info)
+    res["factor_corr"] = bench_factor_corr(dX, dfm, X, fm, dev, steps=max(3, args.steps // 2))
+    return res
 
 
 # DRAM bytes of one k_rank_ic launch per date at N=5000, F=12, from one ncu capture
@@ -397,6 +401,49 @@ def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned
     if learned_info is not None:
         res["learned"] = learned_info
     return res
+
+
+def bench_factor_corr(dX, dfm, X, fm, dev, steps=5, warmup=2):
+    """factor_corr of the C2 panel (F factors pooled over the T*N (t, i) rows,
+    factor mask broadcast per column), device-resident factor planes, through
+    fcb_dev_factor_corr; spot-checked against the host entry point on the
+    reference's (T,N,F) layout."""
+    import torch
+    from fcb200 import _native as nat
+    lib = nat.lib()
+    F, T, N = X.shape
+    ws = lib.fcb_workspace_create()
+    out = torch.empty((F, F), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def run():
+        nat.check(lib.fcb_dev_factor_corr(dX.data_ptr(), 0, dfm.data_ptr(), T, N, F, 1, out.data_ptr(), ws,
+                                          stream.cuda_stream), "fcb_dev_factor_corr")
+
+    for _ in range(warmup):
+        run()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        run()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    got = out.cpu().numpy()
+    ref = np.empty((F, F))
+    x3 = np.ascontiguousarray(np.moveaxis(X, 0, -1))
+    nat.check(lib.fcb_factor_corr(nat.ptr(x3), 0, nat.ptr(fm), T, N, F, nat.ptr(ref), None), "fcb_factor_corr")
+    lib.fcb_workspace_destroy(ws)
+    rows = T * N
+    alg_bytes = rows * (4 * F + 1)
+    peak, _ = measured_peaks()
+    same = bool(np.array_equal(np.isnan(got), np.isnan(ref)) and
+                np.nanmax(np.abs(np.nan_to_num(got) - np.nan_to_num(ref))) <= 1e-12)
+    return {"workload": f"factor_corr {F}x{F} over {rows} (t,i) rows, f32 factor planes, factor mask",
+            "ms": ms, "rows_per_s": rows / (ms / 1e3), "algorithmic_gb_s": alg_bytes / (ms / 1e3) / 1e9,
+            "hbm_frac": alg_bytes / (ms / 1e3) / 1e9 / peak, "matches_host_entry_point": same}
 
 
 def make_batch_panels(dev, n=64, F=8, seed=20261205):

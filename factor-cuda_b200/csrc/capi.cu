@@ -723,6 +723,31 @@ extern "C" int fcb_stock_corr(const void* x, int dtype, const uint8_t* mask, int
   return FCB_OK;
 }
 
+extern "C" int fcb_dev_factor_corr(const void* d_x, int dtype, const uint8_t* d_mask, int T, int N, int F,
+                                   int planes, double* d_out, fcb_workspace* wsp, void* stream) {
+  if (d_x == nullptr || d_out == nullptr || T < 1 || N < 1 || F < 1) return FCB_ERR_ARG;
+  if (dtype != FCB_DTYPE_F32 && dtype != FCB_DTYPE_F64) return FCB_ERR_ARG;
+  if (planes != 0 && planes != 1) return FCB_ERR_ARG;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP2;
+  if (F > 128) return FCB_ERR_CAP3;
+  if (wsp == nullptr) return FCB_ERR_ARG;  // scratch comes from a caller-held workspace
+  fcb_workspace& ws = *wsp;
+  FCB_TRY(ws.bind());
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const long long R = static_cast<long long>(T) * N;
+  const int Fp = (F + 3) / 4 * 4;
+  FcWork w{};
+  w.nblk_cols = static_cast<int>(std::min<long long>(592, std::max<long long>(1, R / 2048)));
+  w.nblk_gram = static_cast<int>(std::min<long long>(F <= 32 ? 296 : 148, std::max<long long>(1, R / 1024)));
+  FCB_TRY(ws.get(S_FC_COLPART, static_cast<size_t>(w.nblk_cols) * F * sizeof(FcColPart), &w.colpart));
+  FCB_TRY(ws.get(S_FC_COLSTAT, static_cast<size_t>(F) * sizeof(FcColStat), &w.colstat));
+  FCB_TRY(ws.get(S_FC_GRAM, static_cast<size_t>(w.nblk_gram) * 4 * Fp * Fp * 8, &w.gram));
+  FCB_TRY(ws.get(S_FB_LIST, static_cast<size_t>(F) * F * 4, &w.fb_list));
+  FCB_TRY(ws.get(S_FB_CNT, 64, &w.fb_count));
+  FCB_TRY(ws.get(S_FC_FBPART, fc_fb_part_doubles(R, F) * sizeof(double), &w.fb_part));
+  return rc(launch_factor_corr_strided(d_x, dtype, d_mask, R, F, planes ? 1 : F, planes ? R : 1, w, d_out, nullptr, s));
+}
+
 extern "C" int fcb_factor_corr(const void* x, int dtype, const uint8_t* mask, int T, int N, int F, double* out,
                                uint8_t* fallback_out) {
   if (x == nullptr || out == nullptr || T < 1 || N < 1 || F < 1) return FCB_ERR_ARG;

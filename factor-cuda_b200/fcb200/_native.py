@@ -65,6 +65,7 @@ PROTOTYPES = {
                                     C.POINTER(_i), _p]),
     "fcb_rolling_ic": (_i, [_p, _i, _p, _i, _p, _p, _i, _i, _i, _p, _p, _p, _p]),
     "fcb_factor_corr": (_i, [_p, _i, _p, _i, _i, _i, _p, _p]),
+    "fcb_dev_factor_corr": (_i, [_p, _i, _p, _i, _i, _i, _i, _p, _p, _p]),
     "fcb_stock_corr": (_i, [_p, _i, _p, _i, _i, _p, C.POINTER(_i), C.POINTER(_i)]),
     "fcb_rank_ic_panel": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i, _p]),
     "fcb_dev_rank_ic_panel": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i, _p]),

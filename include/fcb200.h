@@ -122,6 +122,14 @@ int fcb_rolling_ic(const void* f, int f_dtype, const void* r, int r_dtype, const
 int fcb_factor_corr(const void* x, int dtype, const uint8_t* mask, int T, int N, int F, double* out,
                     uint8_t* fallback_out);
 
+/* factor_corr on caller-owned DEVICE buffers, asynchronous on `stream` (NULL =
+ * legacy stream); same kernels and results as fcb_factor_corr.  planes = 0:
+ * d_x is the reference's (T,N,F) panel; planes = 1: F factor planes (F,T,N).
+ * Scratch comes from `ws` (required; calls sharing it must be serialised).
+ * No reference counterpart (device-pointer variant of factor_corr_gpu). */
+int fcb_dev_factor_corr(const void* d_x, int dtype, const uint8_t* d_mask, int T, int N, int F, int planes,
+                        double* d_out, fcb_workspace* ws, void* stream);
+
 /* (N,N) pairwise-complete Pearson of a (T,N) panel over t.  selected_path
  * (NULL = off): 0 fully valid panel, 1 masked panel; fallback_count: pairs
  * recomputed by the two-pass fallback.

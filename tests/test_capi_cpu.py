@@ -57,6 +57,9 @@ def test_contract_errors_without_device(native):
     o = np.zeros(4)
     assert lib.fcb_factor_corr(P(x), 0, None, 1, 1, 129, P(o), None) == -3
     assert lib.fcb_factor_corr(P(x), 0, None, 1 << 16, 1 << 16, 2, P(o), None) == -2
+    assert lib.fcb_dev_factor_corr(P(x), 0, None, 1, 1, 129, 0, P(o), None, None) == -3
+    assert lib.fcb_dev_factor_corr(P(x), 0, None, 2, 2, 2, 0, P(o), None, None) == -1   # workspace required
+    assert lib.fcb_dev_factor_corr(P(x), 0, None, 2, 2, 2, 2, P(o), None, None) == -1   # layout flag
     assert lib.fcb_stock_corr(P(x), 0, None, 1, 46341, P(o), None, None) == -3
     assert lib.fcb_stock_corr(None, 0, None, 1, 2, P(o), None, None) == -1
     st = (C.c_int * 4)()

@@ -248,6 +248,33 @@ def test_factor_corr_large_pool_fallback():
         assert corr_match(out, dO.cpu().numpy())
 
 
+def test_dev_factor_corr_layouts():
+    """The device entry point, in both layouts, equals the host entry point."""
+    import torch
+    from fcb200 import _native as nat
+    rng = np.random.default_rng(33)
+    T, N, F = 40, 900, 6
+    F3 = rng.standard_normal((T, N, F)).astype(np.float32)
+    F3[..., 2] = np.exp(F3[..., 2]) + 3.0
+    F3[rng.random((T, N, F)) < 0.03] = np.nan
+    m8 = (rng.random((T, N)) < 0.9).astype(np.uint8)
+    ref = np.empty((F, F))
+    nat.check(nat.lib().fcb_factor_corr(nat.ptr(F3), 0, nat.ptr(m8), T, N, F, nat.ptr(ref), None), "host")
+    ws = nat.lib().fcb_workspace_create()
+    try:
+        for planes, arr in ((0, F3), (1, np.ascontiguousarray(np.moveaxis(F3, -1, 0)))):
+            dX = torch.from_numpy(arr).cuda()
+            dM = torch.from_numpy(m8).cuda()
+            dO = torch.empty((F, F), dtype=torch.float64, device="cuda")
+            nat.check(nat.lib().fcb_dev_factor_corr(dX.data_ptr(), 0, dM.data_ptr(), T, N, F, planes, dO.data_ptr(), ws,
+                                                    None), "dev")
+            torch.cuda.synchronize()
+            got = dO.cpu().numpy()
+            assert np.array_equal(got.view(np.uint64), ref.view(np.uint64)), planes
+    finally:
+        nat.lib().fcb_workspace_destroy(ws)
+
+
 def test_adapter_end_to_end():
     import fcb200
     rng = np.random.default_rng(1)
