@@ -342,12 +342,13 @@ def run_b200(args, rank, world):
     return res
 
 
-# DRAM bytes of one k_rank_ic launch per date at N=5000, F=12, from one ncu capture
-# each at T=600 (profiles/k_rank_ic_learned_T600_N5000_F12.md): dram__bytes_read.sum +
-# dram__bytes_write.sum.  Traffic grows with the number of dates at fixed N and F, so
-# the bench's launch is that times T.
-TRAFFIC_PER_DATE = {"learned": (162.197760e6 + 101.510400e6) / 600,
-                    "radix": (162.098688e6 + 101.336576e6) / 600}
+# DRAM bytes of one rank + IC step per date at N=5000, F=12 (k_ric_returns +
+# k_rank_ic_item), from one ncu capture each at T=600
+# (profiles/k_rank_ic_item_T600_N5000_F12.md): dram__bytes_read.sum +
+# dram__bytes_write.sum.  Traffic grows with the number of dates at fixed N
+# and F, so the bench's step is that times T.
+TRAFFIC_PER_DATE = {"learned": (153.391360e6 + 103.361792e6 + 18.050048e6) / 600,
+                    "radix": (153.914368e6 + 102.658048e6 + 18.050048e6) / 600}
 
 
 def max_over_ranks(values, device):
@@ -393,7 +394,7 @@ def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "traffic_source": "ncu dram bytes at T=600 scaled by T/600" if traffic else None,
-                     "kernel": "k_rank_ic", "algorithmic_bytes_per_launch": bytes_launch},
+                     "kernel": "k_ric_returns + k_rank_ic_item", "algorithmic_bytes_per_launch": bytes_launch},
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "parity_spot_check": spot,
