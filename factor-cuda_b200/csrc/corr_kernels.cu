@@ -428,13 +428,26 @@ __global__ void k_fc_colpart(const TIN* __restrict__ X, const uint8_t* __restric
   for (int f = threadIdx.y; f < F; f += blockDim.y) {
     Kahan k;
     double cnt = 0.0, mn = kBigPos, mx = -kBigPos;
-    for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-      const double x = static_cast<double>(X[r * sr + f * sf]);
-      if (finite_f64(x) && (mask == nullptr || mask[r] != 0)) {
-        cnt += 1.0;
-        k.add(x);
-        mn = fmin(mn, x);
-        mx = fmax(mx, x);
+    // rows visited in the same order; kU loads in flight before they are added
+    constexpr int kU = 8;
+    for (long long rb = r0 + threadIdx.x; rb < r1; rb += static_cast<long long>(kU) * blockDim.x) {
+      double xv[kU];
+      bool ok[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const long long r = rb + static_cast<long long>(u) * blockDim.x;
+        ok[u] = r < r1;
+        xv[u] = ok[u] ? static_cast<double>(X[r * sr + f * sf]) : 0.0;
+        ok[u] = ok[u] && (mask == nullptr || mask[r] != 0);
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (ok[u] && finite_f64(xv[u])) {
+          cnt += 1.0;
+          k.add(xv[u]);
+          mn = fmin(mn, xv[u]);
+          mx = fmax(mx, xv[u]);
+        }
       }
     }
     // fixed-order warp merge (lanes are threadIdx.x within one warp row)
@@ -828,17 +841,29 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass1(const TIN* __restric
     const int i = e / F, j = e % F;
     Kahan kx, ky;
     double n = 0.0, mnx = kBigPos, mxx = -kBigPos, mny = kBigPos, mxy = -kBigPos;
-    for (long long r = r0 + tid; r < r1; r += kFbThreads) {
-      const double x = static_cast<double>(X[r * sr + i * sf]);
-      const double y = static_cast<double>(X[r * sr + j * sf]);
-      if (finite_f64(x) && finite_f64(y) && (mask == nullptr || mask[r] != 0)) {
-        n += 1.0;
-        kx.add(x);
-        ky.add(y);
-        mnx = fmin(mnx, x);
-        mxx = fmax(mxx, x);
-        mny = fmin(mny, y);
-        mxy = fmax(mxy, y);
+    constexpr int kU = 4;  // rows in flight per thread, added in row order
+    for (long long rb = r0 + tid; rb < r1; rb += static_cast<long long>(kU) * kFbThreads) {
+      double xv[kU], yv[kU];
+      bool ok[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const long long r = rb + static_cast<long long>(u) * kFbThreads;
+        ok[u] = r < r1;
+        xv[u] = ok[u] ? static_cast<double>(X[r * sr + i * sf]) : 0.0;
+        yv[u] = ok[u] ? static_cast<double>(X[r * sr + j * sf]) : 0.0;
+        ok[u] = ok[u] && (mask == nullptr || mask[r] != 0);
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (ok[u] && finite_f64(xv[u]) && finite_f64(yv[u])) {
+          n += 1.0;
+          kx.add(xv[u]);
+          ky.add(yv[u]);
+          mnx = fmin(mnx, xv[u]);
+          mxx = fmax(mxx, xv[u]);
+          mny = fmin(mny, yv[u]);
+          mxy = fmax(mxy, yv[u]);
+        }
       }
     }
     sh[0][tid] = kx.s;
@@ -954,14 +979,26 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass2(const TIN* __restric
     const int i = e / F, j = e % F;
     const double mx = Q[1], my = Q[2];
     Kahan a, b, c;
-    for (long long r = r0 + tid; r < r1; r += kFbThreads) {
-      const double x = static_cast<double>(X[r * sr + i * sf]);
-      const double y = static_cast<double>(X[r * sr + j * sf]);
-      if (finite_f64(x) && finite_f64(y) && (mask == nullptr || mask[r] != 0)) {
-        const double dx = x - mx, dy = y - my;
-        a.add(dx * dx);
-        b.add(dy * dy);
-        c.add(dx * dy);
+    constexpr int kU = 4;  // rows in flight per thread, added in row order
+    for (long long rb = r0 + tid; rb < r1; rb += static_cast<long long>(kU) * kFbThreads) {
+      double xv[kU], yv[kU];
+      bool ok[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const long long r = rb + static_cast<long long>(u) * kFbThreads;
+        ok[u] = r < r1;
+        xv[u] = ok[u] ? static_cast<double>(X[r * sr + i * sf]) : 0.0;
+        yv[u] = ok[u] ? static_cast<double>(X[r * sr + j * sf]) : 0.0;
+        ok[u] = ok[u] && (mask == nullptr || mask[r] != 0);
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (ok[u] && finite_f64(xv[u]) && finite_f64(yv[u])) {
+          const double dx = xv[u] - mx, dy = yv[u] - my;
+          a.add(dx * dx);
+          b.add(dy * dy);
+          c.add(dx * dy);
+        }
       }
     }
     sh[0][tid] = a.s;
