@@ -364,7 +364,7 @@ extern "C" int fcb_batch_create(const fcb_panel* panels, int npanels, int dtype_
     const int F = q.F, Fp = (F + 3) / 4 * 4;
     FcWork& w = b->fcw[i];
     w.nblk_cols = static_cast<int>(std::min<long long>(592, std::max<long long>(1, R / 2048)));
-    w.nblk_gram = static_cast<int>(std::min<long long>(F <= 32 ? 296 : 148, std::max<long long>(1, R / 1024)));
+    w.nblk_gram = fc_gram_blocks(R, F);
     const size_t b_colpart = static_cast<size_t>(w.nblk_cols) * F * sizeof(FcColPart);
     const size_t b_colstat = static_cast<size_t>(F) * sizeof(FcColStat);
     const size_t b_gram = static_cast<size_t>(w.nblk_gram) * 4 * Fp * Fp * sizeof(double);

@@ -738,7 +738,7 @@ extern "C" int fcb_dev_factor_corr(const void* d_x, int dtype, const uint8_t* d_
   const int Fp = (F + 3) / 4 * 4;
   FcWork w{};
   w.nblk_cols = static_cast<int>(std::min<long long>(592, std::max<long long>(1, R / 2048)));
-  w.nblk_gram = static_cast<int>(std::min<long long>(F <= 32 ? 296 : 148, std::max<long long>(1, R / 1024)));
+  w.nblk_gram = fc_gram_blocks(R, F);
   FCB_TRY(ws.get(S_FC_COLPART, static_cast<size_t>(w.nblk_cols) * F * sizeof(FcColPart), &w.colpart));
   FCB_TRY(ws.get(S_FC_COLSTAT, static_cast<size_t>(F) * sizeof(FcColStat), &w.colstat));
   FCB_TRY(ws.get(S_FC_GRAM, static_cast<size_t>(w.nblk_gram) * 4 * Fp * Fp * 8, &w.gram));
@@ -766,7 +766,7 @@ extern "C" int fcb_factor_corr(const void* x, int dtype, const uint8_t* mask, in
   const size_t esz = dtype == FCB_DTYPE_F32 ? 4 : 8;
   FcWork w{};
   w.nblk_cols = static_cast<int>(std::min<long long>(592, std::max<long long>(1, R / 2048)));
-  w.nblk_gram = static_cast<int>(std::min<long long>(F <= 32 ? 296 : 148, std::max<long long>(1, R / 1024)));
+  w.nblk_gram = fc_gram_blocks(R, F);
   void* dx;
   uint8_t* dm = nullptr;
   double* dout;

@@ -527,7 +527,7 @@ __global__ void k_fc_colfinal(const FcColPart* __restrict__ part, int nblk, int 
 __host__ __device__ inline int fc_rows_chunk(int Fp) { return 32 * (64 / Fp > 8 ? 8 : (64 / Fp < 1 ? 1 : 64 / Fp)); }
 
 template <typename TIN>
-__global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+__global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
                                                  long long R, int F, long long sr, long long sf, int Fp,
                                                  long long rows_per_block,
                                                  const FcColStat* __restrict__ st, int tasks_total,
@@ -536,8 +536,7 @@ __global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, cons
   double* sx = fsm;                                  // [chunk][Fp] centred values
   const int chunk = fc_rows_chunk(Fp);
   double* sm = sx + chunk * Fp;                      // [chunk][Fp] validity
-  double* sq = sm + chunk * Fp;                      // [chunk][Fp] squares
-  double* red = sq + chunk * Fp;                     // [slices][tasks_per_block][16]
+  double* red = fsm;  // [slices][tasks_per_block][16], over the staging tile once it is idle
   const int tb = Fp / 4;
   const int task0 = blockIdx.y * tasks_per_block;
   const int ntask = min(tasks_per_block, tasks_total - task0);
@@ -553,7 +552,7 @@ __global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, cons
     fa = (rem / tb) * 4;
     ga = (rem % tb) * 4;
   }
-  double acc[16], prt[16];
+  double acc[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) acc[q] = 0.0;
   const long long r0 = blockIdx.x * rows_per_block;
@@ -576,27 +575,28 @@ __global__ void __launch_bounds__(256) k_fc_gram(const TIN* __restrict__ X, cons
       }
       sx[ei] = v;
       sm[ei] = mv;
-      sq[ei] = v * v;
     }
     __syncthreads();
     if (active) {
-      const double* A = (p == 0) ? sm : (p == 1 ? sx : (p == 2 ? sq : sx));
+      const double* A = (p == 0) ? sm : sx;  // product 2 squares the centred values below
       const double* B = (p == 3) ? sx : sm;
-#pragma unroll
-      for (int q = 0; q < 16; ++q) prt[q] = 0.0;
       for (int rr = my_slice; rr < nr; rr += slices) {
         const double* ar = A + rr * Fp + fa;
         const double* br = B + rr * Fp + ga;
-        const double a0 = ar[0], a1 = ar[1], a2 = ar[2], a3 = ar[3];
+        double a0 = ar[0], a1 = ar[1], a2 = ar[2], a3 = ar[3];
+        if (p == 2) {
+          a0 *= a0;
+          a1 *= a1;
+          a2 *= a2;
+          a3 *= a3;
+        }
         const double b0 = br[0], b1 = br[1], b2 = br[2], b3 = br[3];
         const double av[4] = {a0, a1, a2, a3}, bv[4] = {b0, b1, b2, b3};
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
-          for (int v = 0; v < 4; ++v) prt[u * 4 + v] = fma(av[u], bv[v], prt[u * 4 + v]);
+          for (int v = 0; v < 4; ++v) acc[u * 4 + v] = fma(av[u], bv[v], acc[u * 4 + v]);
       }
-#pragma unroll
-      for (int q = 0; q < 16; ++q) acc[q] += prt[q];
     }
     __syncthreads();
   }
@@ -1057,7 +1057,9 @@ int fc_fb_nblk(long long R, int F) {
 
 size_t fc_gram_smem(int Fp, int tasks_per_block) {
   const int slices = 256 / tasks_per_block;
-  return (3 * static_cast<size_t>(fc_rows_chunk(Fp)) * Fp + static_cast<size_t>(slices) * tasks_per_block * 16) *
+  const size_t stage = 2 * static_cast<size_t>(fc_rows_chunk(Fp)) * Fp;
+  const size_t red = static_cast<size_t>(slices) * tasks_per_block * 16;
+  return (stage > red ? stage : red) *
          sizeof(double);
 }
 

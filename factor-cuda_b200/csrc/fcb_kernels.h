@@ -61,6 +61,15 @@ struct FcWork {
   int* fb_count;       // [1]
   double* fb_part;     // fc_fb_part_doubles(R, F) doubles, or nullptr (single-block fallback)
 };
+// Row blocks of factor_corr's Gram pass: narrow panels (F <= 32) use enough
+// blocks to fill the SMs several times over (their staging tile is small);
+// the same count everywhere keeps single-panel and batched results identical.
+inline int fc_gram_blocks(long long R, int F) {
+  const long long cap = F <= 32 ? 888 : 148;
+  long long nb = R / 1024;
+  if (nb < 1) nb = 1;
+  return static_cast<int>(nb < cap ? nb : cap);
+}
 // Row blocks per flagged pair of the multi-block fallback, and the partials
 // buffer it needs (doubles).
 int fc_fb_nblk(long long R, int F);
