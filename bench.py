@@ -303,6 +303,7 @@ def run_b200(args, rank, world):
     if args.no_e2e:
         res = finish(args, world, X, R, fm, rm, ms, None, None, clk, spot, dev, learned_info)
         res["factor_corr"] = bench_factor_corr(dX, dfm, X, fm, dev, steps=max(3, args.steps // 2))
+        res["c2_stages"] = bench_c2_stages(dX, X, fm, dev, ms, res["factor_corr"]["ms"])
         return res
     hX = torch.from_numpy(X).pin_memory()
     hR = torch.from_numpy(R).pin_memory()
@@ -339,6 +340,7 @@ def run_b200(args, rank, world):
     e2e_ok = bool(np.array_equal(hranks.numpy().view(np.uint32), dranks.cpu().numpy().view(np.uint32)))
     res = finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info)
     res["factor_corr"] = bench_factor_corr(dX, dfm, X, fm, dev, steps=max(3, args.steps // 2))
+    res["c2_stages"] = bench_c2_stages(dX, X, fm, dev, ms, res["factor_corr"]["ms"])
     return res
 
 
@@ -445,6 +447,61 @@ def bench_factor_corr(dX, dfm, X, fm, dev, steps=5, warmup=2):
     return {"workload": f"factor_corr {F}x{F} over {rows} (t,i) rows, f32 factor planes, factor mask",
             "ms": ms, "rows_per_s": rows / (ms / 1e3), "algorithmic_gb_s": alg_bytes / (ms / 1e3) / 1e9,
             "hbm_frac": alg_bytes / (ms / 1e3) / 1e9 / peak, "matches_host_entry_point": same}
+
+
+def bench_c2_stages(dX, X, fm, dev, rank_ic_ms, factor_corr_ms, steps=3):
+    """The C2 pipeline stage by stage on the same panel: cs_rank of every factor
+    plane (device entry point, CUDA events), parameter_scan (4 groups) of every
+    plane (its own device timing, host buffers), and the fused rank + IC and
+    factor_corr legs measured above -- the counterpart of the reference's
+    parameter_scan -> rolling_ic -> factor_corr pipeline figure."""
+    import ctypes as C
+    import torch
+    from fcb200 import _native as nat
+    lib = nat.lib()
+    F, T, N = X.shape
+    dfm = torch.from_numpy(fm).to(dev)
+    out = torch.empty((T, N), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def cs_all():
+        for f in range(F):
+            nat.check(lib.fcb_dev_cs_rank_f32(dX[f].data_ptr(), dfm.data_ptr(), T, N, 0, out.data_ptr(),
+                                              stream.cuda_stream), "fcb_dev_cs_rank_f32")
+
+    cs_all()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        cs_all()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    cs_ms = e0.elapsed_time(e1) / steps
+    # parameter_scan: device time of the fused four-group pass per plane
+    outs = [np.empty((T, N), np.float32) for _ in range(4)]
+    optr = (C.c_void_p * 4)(*[nat.ptr(o) for o in outs])
+    st = (C.c_int * 4)()
+    tg = (C.c_float * 4)()
+    ws = lib.fcb_workspace_create()
+    scan_ms = []
+    for _ in range(2):
+        tot = 0.0
+        for f in range(F):
+            xf = np.ascontiguousarray(X[f])
+            nat.check(lib.fcb_parameter_scan_f32(nat.ptr(xf), nat.ptr(fm), T, N, optr, st, None, tg, None, ws),
+                      "fcb_parameter_scan_f32")
+            tot += sum(float(v) for v in tg)
+        scan_ms.append(tot)
+    lib.fcb_workspace_destroy(ws)
+    scan = min(scan_ms)
+    return {"workload": f"C2 stages on {F} factor planes of {T}x{N}",
+            "cs_rank_ms_all_planes": cs_ms, "parameter_scan_ms_all_planes": scan,
+            "rank_ic_ms_all_planes": rank_ic_ms, "factor_corr_ms": factor_corr_ms,
+            "pipeline_ms": scan + rank_ic_ms + factor_corr_ms,
+            "pipeline": "parameter_scan (4 groups) + cs_rank/rolling_ic (fused, learned) + factor_corr, "
+                        "device-resident kernels"}
 
 
 def make_batch_panels(dev, n=64, F=8, seed=20261205):
