@@ -152,6 +152,20 @@ bool is_group_whitelist(cudaError_t e) {
   return e == cudaErrorInvalidConfiguration || e == cudaErrorLaunchOutOfResources;
 }
 
+// Status word the asynchronous fcb_dev_* entry points hand to kernels with
+// bounded waits (allocated once per process, written only by kernels).
+cudaError_t dev_status_sink(int** out) {
+  static int* d_status = nullptr;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> g(mu);
+  if (d_status == nullptr) {
+    const cudaError_t e = cudaMalloc(&d_status, 64);
+    if (e != cudaSuccess) return e;
+  }
+  *out = d_status;
+  return cudaSuccess;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -264,12 +278,8 @@ extern "C" int fcb_dev_cs_rank_f32(const float* d_x, const uint8_t* d_mask, int 
     FCB_TRY(scratch_free(scr, s));
     return rc(e);
   }
-  static int* d_status = nullptr;  // status sink for the asynchronous variant
-  static std::mutex mu;
-  {
-    std::lock_guard<std::mutex> g(mu);
-    if (d_status == nullptr) FCB_TRY(cudaMalloc(&d_status, sizeof(int)));
-  }
+  int* d_status;
+  FCB_TRY(dev_status_sink(&d_status));
   return rc(launch_cs_rank(d_x, d_mask, T, N, desc, d_out, d_status, s));
 }
 
@@ -400,6 +410,45 @@ extern "C" int fcb_parameter_scan_f32(const float* x, const uint8_t* mask, int T
   return FCB_OK;
 }
 
+extern "C" int fcb_dev_parameter_scan_f32(const float* d_x, const uint8_t* d_mask, int T, int N,
+                                          float* const d_out[4], int group_status[4], const int active[4],
+                                          void* stream) {
+  if (group_status != nullptr)
+    for (int g = 0; g < 4; ++g) group_status[g] = FCB_GROUP_NOT_EXECUTED;
+  if (d_x == nullptr || d_out == nullptr || group_status == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
+  int act[4];
+  ScanOut so{};
+  for (int g = 0; g < 4; ++g) {
+    act[g] = (active == nullptr || active[g]) ? 1 : 0;
+    if (act[g] && d_out[g] == nullptr) return FCB_ERR_ARG;
+    so.out[g] = act[g] ? d_out[g] : nullptr;
+  }
+  if (N > (1 << 24)) return FCB_ERR_CAP2;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t le;
+  if (N > kSmemRankCap) {
+    const size_t bytes = rank_global_scratch(rank_global_bytes_per_date(1, N, 1, 4, 4), T);
+    void* scr = nullptr;
+    FCB_TRY(scratch_alloc(&scr, bytes, s));
+    le = launch_param_scan_global(d_x, d_mask, T, N, so, static_cast<uint8_t*>(scr), bytes, s);
+    FCB_TRY(scratch_free(scr, s));
+  } else {
+    int* d_status;
+    FCB_TRY(dev_status_sink(&d_status));
+    le = launch_param_scan(d_x, d_mask, T, N, so, d_status, s);
+  }
+  if (le != cudaSuccess) {
+    if (!is_group_whitelist(le)) return rc(le);
+    for (int g = 0; g < 4; ++g)
+      if (act[g]) group_status[g] = rc(le);
+    return FCB_OK;  // every active group failed at launch; outputs untouched
+  }
+  for (int g = 0; g < 4; ++g)
+    if (act[g]) group_status[g] = 0;
+  return FCB_OK;
+}
+
 // ---------------------------------------------------------------------------
 // rolling_ic (single factor) and the batched panel
 // ---------------------------------------------------------------------------
@@ -486,6 +535,53 @@ extern "C" int fcb_rolling_ic(const void* f, int fdt, const void* r, int rdt, co
   return check_status(&hst);
 }
 
+template <typename TF, typename TR>
+static int dev_rank_ic(const RankIcArgs<TF, TR>& a, cudaStream_t s) {
+  if (rank_ic_fits_smem<TF, TR>(a.N)) {
+    int* d_status;
+    FCB_TRY(dev_status_sink(&d_status));
+    return rc(launch_rank_ic<TF, TR>(a, d_status, s));
+  }
+  const size_t bytes =
+      rank_global_scratch(rank_global_bytes_per_date(2, a.N, a.F, sizeof(TF), sizeof(TR)), a.T);
+  void* scr = nullptr;
+  FCB_TRY(scratch_alloc(&scr, bytes, s));
+  const cudaError_t e = launch_rank_ic_global<TF, TR>(a, static_cast<uint8_t*>(scr), bytes, s);
+  FCB_TRY(scratch_free(scr, s));
+  return rc(e);
+}
+
+extern "C" int fcb_dev_rolling_ic(const void* d_f, int fdt, const void* d_r, int rdt, const uint8_t* d_fmask,
+                                  const uint8_t* d_rmask, int T, int N, int min_valid, double* d_ic,
+                                  double* d_rank_f, double* d_rank_r, void* stream) {
+  if (d_f == nullptr || d_r == nullptr || d_ic == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
+  if ((d_rank_f == nullptr) != (d_rank_r == nullptr)) return FCB_ERR_ARG;
+  if (min_valid < 2) return FCB_ERR_CAP4;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
+  if ((fdt != FCB_DTYPE_F32 && fdt != FCB_DTYPE_F64) || (rdt != FCB_DTYPE_F32 && rdt != FCB_DTYPE_F64))
+    return FCB_ERR_ARG;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (fdt == FCB_DTYPE_F32 && rdt == FCB_DTYPE_F32)
+    return dev_rank_ic(RankIcArgs<float, float>{static_cast<const float*>(d_f), static_cast<const float*>(d_r),
+                                                d_fmask, d_rmask, 1, T, N, min_valid, nullptr, d_ic, d_rank_f,
+                                                d_rank_r},
+                       s);
+  if (fdt == FCB_DTYPE_F32)
+    return dev_rank_ic(RankIcArgs<float, double>{static_cast<const float*>(d_f), static_cast<const double*>(d_r),
+                                                 d_fmask, d_rmask, 1, T, N, min_valid, nullptr, d_ic, d_rank_f,
+                                                 d_rank_r},
+                       s);
+  if (rdt == FCB_DTYPE_F32)
+    return dev_rank_ic(RankIcArgs<double, float>{static_cast<const double*>(d_f), static_cast<const float*>(d_r),
+                                                 d_fmask, d_rmask, 1, T, N, min_valid, nullptr, d_ic, d_rank_f,
+                                                 d_rank_r},
+                       s);
+  return dev_rank_ic(RankIcArgs<double, double>{static_cast<const double*>(d_f), static_cast<const double*>(d_r),
+                                                d_fmask, d_rmask, 1, T, N, min_valid, nullptr, d_ic, d_rank_f,
+                                                d_rank_r},
+                     s);
+}
+
 static int panel_args_check(const void* x, const void* r, const double* ic, int F, int T, int N, int min_valid,
                             int method) {
   if (x == nullptr || r == nullptr || ic == nullptr || F < 1 || T < 1 || N < 1) return FCB_ERR_ARG;
@@ -502,12 +598,8 @@ extern "C" int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const u
   const int chk = panel_args_check(d_x, d_r, d_ic, F, T, N, min_valid, method);
   if (chk != FCB_OK) return chk;
   if (method != 0) return FCB_ERR_UNSUPPORTED;  // learned: fcb_dev_rank_ic_panel_learned (needs a model)
-  static int* d_status = nullptr;
-  static std::mutex mu;
-  {
-    std::lock_guard<std::mutex> g(mu);
-    if (d_status == nullptr) FCB_TRY(cudaMalloc(&d_status, sizeof(int)));
-  }
+  int* d_status;
+  FCB_TRY(dev_status_sink(&d_status));
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (rank_ic_fits_smem<float, float>(N)) {
@@ -673,12 +765,54 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
 // ---------------------------------------------------------------------------
 // correlations
 // ---------------------------------------------------------------------------
-extern "C" int fcb_stock_corr(const void* x, int dtype, const uint8_t* mask, int T, int N, double* out,
-                              int* selected_path, int* fallback_count) {
+static int stock_corr_check(const void* x, int dtype, const void* out, int T, int N) {
   if (x == nullptr || out == nullptr || T < 1 || N < 1) return FCB_ERR_ARG;
   if (dtype != FCB_DTYPE_F32 && dtype != FCB_DTYPE_F64) return FCB_ERR_ARG;
   if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP2;
   if (static_cast<long long>(N) * N > INT32_MAX) return FCB_ERR_CAP3;
+  return FCB_OK;
+}
+
+extern "C" int fcb_dev_stock_corr(const void* d_x, int dtype, const uint8_t* d_mask, int T, int N, double* d_out,
+                                  int* selected_path, int* fallback_count, fcb_workspace* wsp, void* stream) {
+  const int chk = stock_corr_check(d_x, dtype, d_out, T, N);
+  if (chk != FCB_OK) return chk;
+  if (wsp == nullptr) return FCB_ERR_ARG;  // scratch comes from a caller-held workspace
+  fcb_workspace& ws = *wsp;
+  FCB_TRY(ws.bind());
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int Tp = (T + 31) / 32 * 32;
+  double *xraw, *xc, *mc, *sum;
+  ColStat* st;
+  int *fbl, *fbc;
+  FCB_TRY(ws.get(S_SC_RAW, static_cast<size_t>(N) * Tp * 8, &xraw));
+  FCB_TRY(ws.get(S_SC_C, static_cast<size_t>(N) * Tp * 8, &xc));
+  FCB_TRY(ws.get(S_SC_M, static_cast<size_t>(N) * Tp * 8, &mc));
+  FCB_TRY(ws.get(S_SC_ST, static_cast<size_t>(N) * sizeof(ColStat), &st));
+  FCB_TRY(ws.get(S_SC_SUM, 64, &sum));
+  const size_t upper = static_cast<size_t>(N) * (N - 1) / 2;
+  FCB_TRY(ws.get(S_FB_LIST, (upper > 0 ? upper : 1) * 4, &fbl));
+  FCB_TRY(ws.get(S_FB_CNT, 64, &fbc));
+  FCB_TRY(launch_stock_corr_prep(d_x, dtype, d_mask, T, N, Tp, xraw, xc, mc, st, sum, s));
+  // the domain check and the path flag are read on the host before the Gram pass
+  double hs[3];
+  FCB_TRY(cudaMemcpyAsync(hs, sum, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaStreamSynchronize(s));
+  if (hs[0] > 1e150 || hs[1] < 1e-150) return FCB_ERR_CAP4;
+  if (selected_path) *selected_path = hs[2] != 0.0 ? 0 : 1;
+  FCB_TRY(cudaMemsetAsync(fbc, 0, sizeof(int), s));
+  FCB_TRY(launch_stock_corr_gram(xraw, xc, mc, st, T, N, Tp, d_out, fbl, fbc, s));
+  int hfb = 0;
+  FCB_TRY(cudaMemcpyAsync(&hfb, fbc, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaStreamSynchronize(s));
+  if (fallback_count) *fallback_count = hfb;
+  return FCB_OK;
+}
+
+extern "C" int fcb_stock_corr(const void* x, int dtype, const uint8_t* mask, int T, int N, double* out,
+                              int* selected_path, int* fallback_count) {
+  const int chk = stock_corr_check(x, dtype, out, T, N);
+  if (chk != FCB_OK) return chk;
   fcb_workspace ws;
   struct Rel {
     fcb_workspace& w;
@@ -686,40 +820,45 @@ extern "C" int fcb_stock_corr(const void* x, int dtype, const uint8_t* mask, int
   } rel{ws};
   FCB_TRY(ws.bind());
   cudaStream_t s = ws.stream[0];
-  const int Tp = (T + 31) / 32 * 32;
   const size_t n = static_cast<size_t>(T) * N;
   const size_t esz = dtype == FCB_DTYPE_F32 ? 4 : 8;
   void* dx;
   uint8_t* dm = nullptr;
-  double *xraw, *xc, *mc, *dout, *sum;
-  ColStat* st;
-  int *fbl, *fbc;
+  double* dout;
   FCB_TRY(ws.get(S_X, n * esz, &dx));
   if (mask) FCB_TRY(ws.get(S_MASK, n, &dm));
-  FCB_TRY(ws.get(S_SC_RAW, static_cast<size_t>(N) * Tp * 8, &xraw));
-  FCB_TRY(ws.get(S_SC_C, static_cast<size_t>(N) * Tp * 8, &xc));
-  FCB_TRY(ws.get(S_SC_M, static_cast<size_t>(N) * Tp * 8, &mc));
-  FCB_TRY(ws.get(S_SC_ST, static_cast<size_t>(N) * sizeof(ColStat), &st));
-  FCB_TRY(ws.get(S_SC_SUM, 64, &sum));
   FCB_TRY(ws.get(S_OUT, static_cast<size_t>(N) * N * 8, &dout));
-  const size_t upper = static_cast<size_t>(N) * (N - 1) / 2;
-  FCB_TRY(ws.get(S_FB_LIST, (upper > 0 ? upper : 1) * 4, &fbl));
-  FCB_TRY(ws.get(S_FB_CNT, 64, &fbc));
   FCB_TRY(cudaMemcpyAsync(dx, x, n * esz, cudaMemcpyHostToDevice, s));
   if (mask) FCB_TRY(cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, s));
-  FCB_TRY(launch_stock_corr_prep(dx, dtype, dm, T, N, Tp, xraw, xc, mc, st, sum, s));
-  double hs[3];
-  FCB_TRY(cudaMemcpyAsync(hs, sum, sizeof(hs), cudaMemcpyDeviceToHost, s));
-  FCB_TRY(cudaStreamSynchronize(s));
-  if (hs[0] > 1e150 || hs[1] < 1e-150) return FCB_ERR_CAP4;
-  if (selected_path) *selected_path = hs[2] != 0.0 ? 0 : 1;
-  FCB_TRY(cudaMemsetAsync(fbc, 0, sizeof(int), s));
-  FCB_TRY(launch_stock_corr_gram(xraw, xc, mc, st, T, N, Tp, dout, fbl, fbc, s));
-  int hfb = 0;
+  const int e = fcb_dev_stock_corr(dx, dtype, dm, T, N, dout, selected_path, fallback_count, &ws, s);
+  if (e != FCB_OK) return e;
   FCB_TRY(cudaMemcpyAsync(out, dout, static_cast<size_t>(N) * N * 8, cudaMemcpyDeviceToHost, s));
-  FCB_TRY(cudaMemcpyAsync(&hfb, fbc, sizeof(int), cudaMemcpyDeviceToHost, s));
   FCB_TRY(cudaStreamSynchronize(s));
-  if (fallback_count) *fallback_count = hfb;
+  return FCB_OK;
+}
+
+extern "C" int fcb_dev_corr_domain(const void* d_x, int dtype, const uint8_t* d_mask, int T, int N, int F,
+                                   int planes, int* in_domain, void* stream) {
+  if (d_x == nullptr || in_domain == nullptr || T < 1 || N < 1 || F < 1) return FCB_ERR_ARG;
+  if (dtype != FCB_DTYPE_F32 && dtype != FCB_DTYPE_F64) return FCB_ERR_ARG;
+  if (planes != 0 && planes != 1) return FCB_ERR_ARG;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP2;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const long long R = static_cast<long long>(T) * N;
+  void* scr = nullptr;
+  FCB_TRY(scratch_alloc(&scr, 16, s));
+  unsigned long long* d_ext = static_cast<unsigned long long*>(scr);
+  unsigned long long h_ext[2] = {0ull, 0ull};
+  cudaError_t e = launch_corr_domain(d_x, dtype, d_mask, R, F, planes, d_ext, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_ext, d_ext, sizeof(h_ext), cudaMemcpyDeviceToHost, s);
+  const cudaError_t fe = scratch_free(scr, s);
+  if (e == cudaSuccess) e = fe;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return rc(e);
+  double mx, mn;
+  std::memcpy(&mx, &h_ext[0], 8);
+  std::memcpy(&mn, &h_ext[1], 8);
+  *in_domain = (mx <= 1e150 && mn >= 1e-150) ? 1 : 0;
   return FCB_OK;
 }
 

@@ -411,6 +411,66 @@ cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const d
   return cudaGetLastError();
 }
 
+// Correlation domain extremes over the valid cells of a factor_corr panel.
+// Non-negative doubles order like their bit patterns, so the block results
+// merge with 64-bit integer atomics.
+__global__ void k_corr_domain_init(unsigned long long* ext) {
+  ext[0] = 0ull;                   // +0.0
+  ext[1] = 0x7ff0000000000000ull;  // +inf
+}
+
+template <typename TIN>
+__global__ void __launch_bounds__(256) k_corr_domain(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                     long long R, int F, int planes,
+                                                     unsigned long long* __restrict__ ext) {
+  const long long n = R * F;
+  double mx = 0.0, mn = __longlong_as_double(0x7ff0000000000000ll);
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < n;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const double v = static_cast<double>(X[e]);
+    const long long r = planes ? e % R : e / F;
+    if (finite_f64(v) && (mask == nullptr || mask[r] != 0)) {
+      const double a = fabs(v);
+      mx = fmax(mx, a);
+      if (a != 0.0) mn = fmin(mn, a);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = fmax(mx, __shfl_xor_sync(kFull, mx, o));
+    mn = fmin(mn, __shfl_xor_sync(kFull, mn, o));
+  }
+  __shared__ double smx[8], smn[8];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    smx[w] = mx;
+    smn[w] = mn;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < static_cast<int>(blockDim.x >> 5); ++i) {
+      mx = fmax(mx, smx[i]);
+      mn = fmin(mn, smn[i]);
+    }
+    atomicMax(&ext[0], static_cast<unsigned long long>(__double_as_longlong(mx)));
+    atomicMin(&ext[1], static_cast<unsigned long long>(__double_as_longlong(mn)));
+  }
+}
+
+cudaError_t launch_corr_domain(const void* X, int dtype, const uint8_t* mask, long long R, int F, int planes,
+                               unsigned long long* ext, cudaStream_t s) {
+  k_corr_domain_init<<<1, 1, 0, s>>>(ext);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const long long n = R * F;
+  const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>(148 * 8, (n + 2047) / 2048)));
+  if (dtype == 0)
+    k_corr_domain<float><<<grid, 256, 0, s>>>(static_cast<const float*>(X), mask, R, F, planes, ext);
+  else
+    k_corr_domain<double><<<grid, 256, 0, s>>>(static_cast<const double*>(X), mask, R, F, planes, ext);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // factor_corr: rows r = t*N+i, F <= 128 columns; element (r, f) at
 // X[r*sr + f*sf] -- (sr, sf) = (F, 1) for a (T,N,F) panel (the reference's

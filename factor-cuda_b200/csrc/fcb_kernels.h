@@ -127,6 +127,11 @@ cudaError_t launch_corr_fp32(const PrecOperands& op, const int2* tiles, int ntil
 cudaError_t launch_stock_corr_prep(const void* X, int dtype, const uint8_t* mask, int T, int N, int Tp,
                                    double* Xraw, double* Xc, double* Mc, ColStat* st, double* summary,
                                    cudaStream_t s);
+// max |x| and min nonzero |x| over the valid cells (finite, mask true) of a
+// factor_corr panel, as IEEE bit patterns in ext[0] / ext[1] (0 and +inf when
+// no cell is valid).  planes = 0: (R,F) rows; planes = 1: F planes of R rows.
+cudaError_t launch_corr_domain(const void* X, int dtype, const uint8_t* mask, long long R, int F, int planes,
+                               unsigned long long* ext, cudaStream_t s);
 cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const double* Mc, const ColStat* st, int T,
                                    int N, int Tp, double* out, int* fb_list, int* fb_count, cudaStream_t s);
 size_t fc_gram_smem(int Fp, int tasks_per_block);

@@ -162,6 +162,58 @@ def _domain_check(arr, mask):
 
 
 # ---------------------------------------------------------------------------
+# CUDA-resident inputs: the device entry points of libfcb200 take the tensor's
+# memory directly, so a torch CUDA tensor is never copied to the host and back
+# (the reference adapter does that round trip, fc/_util.py:121-131).
+# ---------------------------------------------------------------------------
+def _is_cuda(x):
+    return _torch is not None and isinstance(x, _torch.Tensor) and x.is_cuda
+
+
+def _dev_input(x, *, name, ndim, dtypes="f32f64", downcast_to=None):
+    x = x.detach()
+    if not _dtype_ok(x.dtype, dtypes):
+        raise ValueError(f"{name} dtype {x.dtype} not in whitelist {{float32,float64}}")
+    ok = x.dim() == ndim if isinstance(ndim, int) else x.dim() in ndim
+    if not ok:
+        raise ValueError(f"{name} must be {ndim}-D, got ndim={x.dim()}")
+    if downcast_to == "float32" and x.dtype == _torch.float64:
+        x = x.to(_torch.float32)  # IEEE round-to-nearest-even, as the host path's astype
+    return f"cuda:{x.device.index}", x.contiguous()
+
+
+def _dev_mask(mask, *, name, T, N, device, allow_none=True):
+    """Strict-bool (T,N) mask as a uint8 view on `device` (None passes through)."""
+    if mask is None:
+        if allow_none:
+            return None
+        raise ValueError(f"{name} is required")
+    if isinstance(mask, np.ndarray):
+        if mask.dtype != np.bool_:
+            raise ValueError(f"{name} must be bool, got {mask.dtype}")
+        mask = _torch.from_numpy(np.ascontiguousarray(mask))
+    elif isinstance(mask, _torch.Tensor):
+        if mask.dtype != _torch.bool:
+            raise ValueError(f"{name} must be bool, got {mask.dtype}")
+    else:
+        raise TypeError(f"{name} must be a bool numpy array or torch.Tensor")
+    if tuple(mask.shape) != (T, N):
+        raise ValueError(f"{name} shape must be (T,N) matching input, got {tuple(mask.shape)}")
+    return mask.detach().to(device).contiguous().view(_torch.uint8)
+
+
+def _stream_of(t):
+    return _torch.cuda.current_stream(t.device).cuda_stream
+
+
+_DT = {"torch.float32": nat.FCB_DTYPE_F32, "torch.float64": nat.FCB_DTYPE_F64}
+
+
+def _dtype_code(t):
+    return _DT[str(t.dtype)]
+
+
+# ---------------------------------------------------------------------------
 # per-shape workspace cache (reference fc/_workspace.py:42-133)
 # ---------------------------------------------------------------------------
 class _WorkspaceCache:
@@ -199,6 +251,7 @@ class _WorkspaceCache:
 _RANK_CACHE = _WorkspaceCache(lambda: nat.fcb().CsRankWorkspace())
 _SCAN_CACHE = _WorkspaceCache(lambda: nat.fcb().CsRankWorkspace())
 _ROLL_CACHE = _WorkspaceCache(lambda: nat.fcb().RollingIcWorkspace())
+_DEV_CACHE = _WorkspaceCache(lambda: Workspace())  # keyed by device index
 
 
 def clear_workspaces():
@@ -216,6 +269,17 @@ def cross_sectional_rank(values, mask=None, descending=False):
     if type(descending) is not bool:
         raise ValueError("descending must be a bool (type(x) is bool), got "
                          f"{type(descending).__name__}")
+    if _is_cuda(values):
+        device, x = _dev_input(values, name="values", ndim=2, downcast_to="float32")
+        T, N = x.shape
+        _require_cuda("cross_sectional_rank")
+        _mask_device(mask, device, "mask")
+        m = _dev_mask(mask, name="mask", T=T, N=N, device=x.device)
+        out = _torch.empty((T, N), dtype=_torch.float32, device=x.device)
+        with _torch.cuda.device(x.device):
+            nat.check(nat.lib().fcb_dev_cs_rank_f32(nat.ptr(x), nat.ptr(m), T, N, int(descending), nat.ptr(out),
+                                                    _stream_of(x)), "cross_sectional_rank")
+        return out
     kind, device, x = _to_numpy(values, name="values", ndim=2, downcast_to="float32")
     T, N = x.shape
     _require_cuda("cross_sectional_rank")
@@ -280,6 +344,8 @@ def parameter_scan(axes, X, mask=None):
     """direction x mask_mode rank scan; results always host numpy
     (fc/parameter_scan.py:62-132).  The active groups come from one fused pass."""
     effective, combos = _normalize_axes(axes)
+    if _is_cuda(X):
+        return _parameter_scan_dev(effective, combos, X, mask)
     _, device, x = _to_numpy(X, name="X", ndim=2, downcast_to="float32")
     T, N = x.shape
     _require_cuda("parameter_scan")
@@ -296,6 +362,48 @@ def parameter_scan(axes, X, mask=None):
     with _SCAN_CACHE.use((T, N)) as ws:
         r = nat.fcb().parameter_scan_f32(x, m, return_timing=True, active_groups=active, workspace=ws)
     elapsed_ms = (time.perf_counter() - t0) * 1e3
+    return _scan_result(effective, combos, r, elapsed_ms)
+
+
+def _parameter_scan_dev(effective, combos, X, mask):
+    """parameter_scan of a CUDA tensor through fcb_dev_parameter_scan_f32: the
+    panel stays on the device; the group results come back as host numpy."""
+    device, x = _dev_input(X, name="X", ndim=2, downcast_to="float32")
+    T, N = x.shape
+    _require_cuda("parameter_scan")
+    if N > (1 << 24):
+        raise ValueError("N > 2^24 (rank precision cap)")
+    any_masked = any(mm == "masked" for _, mm in combos)
+    m = _dev_mask(mask, name="mask", T=T, N=N, device=x.device, allow_none=False) if any_masked else None
+    active = [0, 0, 0, 0]
+    for d, mm in combos:
+        active[_BINDING_INDEX[d][mm]] = 1
+    nact = sum(active)
+    outs = [_torch.empty((T, N), dtype=_torch.float32, device=x.device) if a else None for a in active]
+    optrs = (C.c_void_p * 4)(*[nat.ptr(o) for o in outs])
+    act = (C.c_int * 4)(*active)
+    gst = (C.c_int * 4)()
+    stream = _torch.cuda.current_stream(x.device)
+    with _torch.cuda.device(x.device):
+        e0 = _torch.cuda.Event(enable_timing=True)
+        e1 = _torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        nat.check(nat.lib().fcb_dev_parameter_scan_f32(nat.ptr(x), nat.ptr(m), T, N, optrs, gst, act,
+                                                       stream.cuda_stream), "parameter_scan")
+        e1.record(stream)
+        stream.synchronize()
+        host_ms = (time.perf_counter() - t0) * 1e3
+        gpu_ms = e0.elapsed_time(e1)
+    st = [int(v) for v in gst]
+    r = {"groups": [o.cpu().numpy() if (o is not None and st[g] == 0) else None for g, o in enumerate(outs)],
+         "group_status": st,
+         "time_ms": [host_ms / nact if st[g] == 0 else 0.0 for g in range(4)],
+         "time_gpu_ms": [gpu_ms / nact if st[g] == 0 else 0.0 for g in range(4)]}
+    return _scan_result(effective, combos, r, host_ms)
+
+
+def _scan_result(effective, combos, r, elapsed_ms):
     groups = []
     for gi, (d, mm) in enumerate(combos):
         g = _BINDING_INDEX[d][mm]
@@ -330,6 +438,8 @@ def rolling_ic(factor, forward_returns, factor_mask=None, fwd_mask=None, min_val
         raise ValueError("min_valid must be an integer (bool rejected)")
     if min_valid < 2:
         raise ValueError("min_valid must be >= 2")
+    if _is_cuda(factor) and _is_cuda(forward_returns) and factor.device == forward_returns.device:
+        return _rolling_ic_dev(factor, forward_returns, factor_mask, fwd_mask, min_valid, device)
     kf, df, f = _to_numpy(factor, name="factor", ndim=2)
     kr, dr, r = _to_numpy(forward_returns, name="forward_returns", ndim=2)
     T, N = f.shape
@@ -351,10 +461,35 @@ def rolling_ic(factor, forward_returns, factor_mask=None, fwd_mask=None, min_val
     return _torch.as_tensor(res, device=_torch.device(df))
 
 
+def _rolling_ic_dev(factor, forward_returns, factor_mask, fwd_mask, min_valid, device):
+    """rolling_ic of two CUDA tensors through fcb_dev_rolling_ic; (T,) f64 on their device."""
+    df, f = _dev_input(factor, name="factor", ndim=2)
+    _, r = _dev_input(forward_returns, name="forward_returns", ndim=2)
+    T, N = f.shape
+    if tuple(r.shape) != (T, N):
+        raise ValueError(f"factor and forward_returns shapes must match (T,N), got {tuple(f.shape)} vs "
+                         f"{tuple(r.shape)}")
+    _mask_device(factor_mask, df, "factor_mask")
+    _mask_device(fwd_mask, df, "fwd_mask")
+    fm = _dev_mask(factor_mask, name="factor_mask", T=T, N=N, device=f.device)
+    rm = _dev_mask(fwd_mask, name="fwd_mask", T=T, N=N, device=f.device)
+    if device == "cpu":
+        raise NotImplementedError("fcb200 has no CPU backend; use the reference adapter for device='cpu'")
+    _require_cuda("rolling_ic")
+    ic = _torch.empty((T,), dtype=_torch.float64, device=f.device)
+    with _torch.cuda.device(f.device):
+        nat.check(nat.lib().fcb_dev_rolling_ic(nat.ptr(f), _dtype_code(f), nat.ptr(r), _dtype_code(r), nat.ptr(fm),
+                                               nat.ptr(rm), T, N, min_valid, nat.ptr(ic), None, None,
+                                               _stream_of(f)), "rolling_ic")
+    return ic
+
+
 def factor_corr(data, mask=None, names=None, backend="cuda"):
     """(F,F) pooled pairwise-complete correlation (fc/correlation.py:52-72)."""
     if backend not in ("cpu", "cuda"):
         raise ValueError(f"backend must be 'cpu' or 'cuda', got {backend!r}")
+    if _is_cuda(data):
+        return _factor_corr_dev(data, mask, names, backend)
     kind, device, arr = _to_numpy(data, name="data", ndim=3)
     T, N, F = arr.shape
     if names is not None and len(names) != F:
@@ -372,10 +507,66 @@ def factor_corr(data, mask=None, names=None, backend="cuda"):
     return res if kind == "numpy" else _make_output(res, kind, device)
 
 
+def _factor_corr_dev(data, mask, names, backend):
+    """factor_corr of a CUDA (T,N,F) tensor through fcb_dev_factor_corr; (F,F) f64 on its device."""
+    device, x = _dev_input(data, name="data", ndim=3)
+    T, N, F = x.shape
+    if names is not None and len(names) != F:
+        raise ValueError(f"names length {len(names)} must equal F={F}")
+    if backend == "cpu":
+        raise NotImplementedError("fcb200 has no CPU backend; use the reference adapter for backend='cpu'")
+    _require_cuda("factor_corr backend='cuda'")
+    _mask_device(mask, device, "mask")
+    m = _dev_mask(mask, name="mask", T=T, N=N, device=x.device)
+    if F > 128:
+        raise ValueError("F > 128 (factor pair grid cap)")
+    out = _torch.empty((F, F), dtype=_torch.float64, device=x.device)
+    stream = _torch.cuda.current_stream(x.device)
+    with _torch.cuda.device(x.device):
+        if x.dtype == _torch.float64:  # f32 panels always lie inside the domain
+            ok = C.c_int(0)
+            nat.check(nat.lib().fcb_dev_corr_domain(nat.ptr(x), nat.FCB_DTYPE_F64, nat.ptr(m), T, N, F, 0,
+                                                    C.byref(ok), stream.cuda_stream), "factor_corr domain")
+            if not ok.value:
+                raise ValueError(DOMAIN_MSG)
+        with _DEV_CACHE.use(x.device.index) as ws:
+            rc = nat.lib().fcb_dev_factor_corr(nat.ptr(x), _dtype_code(x), nat.ptr(m), T, N, F, 0, nat.ptr(out),
+                                               ws.handle, stream.cuda_stream)
+            stream.synchronize()  # the workspace's scratch is free again once this returns
+    if rc != 0:  # the reference binding maps every failure to RuntimeError
+        raise RuntimeError(f"factor_corr: error {rc} ({nat.status_string(rc)})")
+    return out
+
+
+def _stock_corr_dev(data, mask, backend):
+    """stock_corr of a CUDA (T,N) tensor through fcb_dev_stock_corr; (N,N) f64 on its device."""
+    device, x = _dev_input(data, name="data", ndim=2)
+    T, N = x.shape
+    if backend == "cpu":
+        raise NotImplementedError("fcb200 has no CPU backend; use the reference adapter for backend='cpu'")
+    _require_cuda("stock_corr backend='cuda'")
+    _mask_device(mask, device, "mask")
+    m = _dev_mask(mask, name="mask", T=T, N=N, device=x.device)
+    if int(N) * N > (1 << 31) - 1:
+        raise ValueError("N*N exceeds INT32_MAX (output grid cap, N <= 46340)")
+    out = _torch.empty((N, N), dtype=_torch.float64, device=x.device)
+    stream = _torch.cuda.current_stream(x.device)
+    with _torch.cuda.device(x.device), _DEV_CACHE.use(x.device.index) as ws:
+        rc = nat.lib().fcb_dev_stock_corr(nat.ptr(x), _dtype_code(x), nat.ptr(m), T, N, nat.ptr(out), None, None,
+                                          ws.handle, stream.cuda_stream)
+        stream.synchronize()
+    if rc == -4:
+        raise ValueError(DOMAIN_MSG)
+    nat.check(rc, "stock_corr")
+    return out
+
+
 def stock_corr(data, mask=None, backend="cuda"):
     """(N,N) pairwise-complete correlation over t (fc/correlation.py:75-93)."""
     if backend not in ("cpu", "cuda"):
         raise ValueError(f"backend must be 'cpu' or 'cuda', got {backend!r}")
+    if _is_cuda(data):
+        return _stock_corr_dev(data, mask, backend)
     kind, device, arr = _to_numpy(data, name="data", ndim=2)
     T, N = arr.shape
     if backend == "cpu":

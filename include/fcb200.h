@@ -161,9 +161,45 @@ int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const uint8_t* d_f
                           int F, int T, int N, int min_valid, float* d_ranks, double* d_ic, int method,
                           void* stream);
 
-/* Device-pointer cs_rank (asynchronous on `stream`). */
+/* ------------------------------------------- device-resident fc.* calls ---
+ * The fc.* operators on caller-owned DEVICE buffers, issued on `stream`
+ * (cudaStream_t, NULL = legacy stream), with the same arguments, kernels,
+ * results and status codes as the host entry points above.  They remove the
+ * device -> host -> device round trip the reference adapter makes for
+ * CUDA-resident inputs (fc/_util.py:121-131).  Scratch is either stream-ordered
+ * (cudaMallocAsync from a per-device pool) or taken from `ws` where the
+ * signature has one; calls sharing a workspace must be serialised. */
+
+/* cs_rank (asynchronous). */
 int fcb_dev_cs_rank_f32(const float* d_x, const uint8_t* d_mask, int T, int N, int descending, float* d_out,
                         void* stream);
+
+/* parameter_scan (asynchronous).  group_status is filled on the host when
+ * the call returns: 0 for every active group that was launched, the
+ * whitelisted launch error (9 / 701) for a group whose launch failed, -100 for
+ * inactive groups.  Timing is left to the caller (events on `stream`). */
+int fcb_dev_parameter_scan_f32(const float* d_x, const uint8_t* d_mask, int T, int N, float* const d_out[4],
+                               int group_status[4], const int active[4], void* stream);
+
+/* rolling_ic (asynchronous); f / r f32 or f64; d_rank_f / d_rank_r (NULL =
+ * off) receive the (T,N) f64 joint-set ranks, 0 elsewhere. */
+int fcb_dev_rolling_ic(const void* d_f, int f_dtype, const void* d_r, int r_dtype, const uint8_t* d_fmask,
+                       const uint8_t* d_rmask, int T, int N, int min_valid, double* d_ic, double* d_rank_f,
+                       double* d_rank_r, void* stream);
+
+/* stock_corr into a device (N,N) f64 buffer.  Synchronises `stream` twice:
+ * the domain check and the path flag are read on the host before the Gram
+ * pass, and fallback_count after it.  Scratch from `ws` (required). */
+int fcb_dev_stock_corr(const void* d_x, int dtype, const uint8_t* d_mask, int T, int N, double* d_out,
+                       int* selected_path, int* fallback_count, fcb_workspace* ws, void* stream);
+
+/* Correlation domain precondition of a device factor_corr panel (layout as
+ * fcb_dev_factor_corr): *in_domain = 1 when max|x| <= 1e150 and every nonzero
+ * |x| >= 1e-150 over the valid cells (finite, mask true), else 0.  The
+ * reference adapter runs this check on the host before factor_corr_gpu
+ * (fc/correlation.py:16-49).  Synchronises `stream`. */
+int fcb_dev_corr_domain(const void* d_x, int dtype, const uint8_t* d_mask, int T, int N, int F, int planes,
+                        int* in_domain, void* stream);
 
 /* ---------------------------------------------------- learned splitters ---
  * No reference counterpart (a new form of the rank path).  A model holds one

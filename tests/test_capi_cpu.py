@@ -69,6 +69,38 @@ def test_contract_errors_without_device(native):
     assert lib.fcb_status_string(-4).decode()
 
 
+def test_device_entry_contract_errors_without_device(native):
+    """The fcb_dev_* variants of the fc.* calls reject bad arguments with the
+    host entry points' codes before they touch a device."""
+    lib = native.lib()
+    P = native.ptr
+    x = np.zeros(4, np.float32)
+    o = np.zeros(4)
+    st = (C.c_int * 4)()
+    outs = (C.c_void_p * 4)(P(x), P(x), P(x), P(x))
+    assert lib.fcb_dev_parameter_scan_f32(P(x), None, 1, (1 << 24) + 1, outs, st, None, None) == -2
+    assert list(st) == [-100] * 4
+    assert lib.fcb_dev_parameter_scan_f32(P(x), None, 1 << 16, 1 << 16, outs, st, None, None) == -3
+    assert lib.fcb_dev_parameter_scan_f32(None, None, 2, 2, outs, st, None, None) == -1
+    nulls = (C.c_void_p * 4)(P(x), None, P(x), P(x))
+    assert lib.fcb_dev_parameter_scan_f32(P(x), None, 2, 2, nulls, st, None, None) == -1   # active group, no output
+    only0 = (C.c_int * 4)(1, 0, 0, 0)
+    assert lib.fcb_dev_parameter_scan_f32(P(x), None, 1, (1 << 24) + 1, nulls, st, only0, None) == -2
+    assert lib.fcb_dev_rolling_ic(P(x), 0, P(x), 0, None, None, 2, 2, 1, P(o), None, None, None) == -4
+    assert lib.fcb_dev_rolling_ic(P(x), 0, P(x), 0, None, None, 1 << 16, 1 << 16, 30, P(o), None, None, None) == -3
+    assert lib.fcb_dev_rolling_ic(P(x), 2, P(x), 0, None, None, 2, 2, 30, P(o), None, None, None) == -1
+    assert lib.fcb_dev_rolling_ic(P(x), 0, P(x), 0, None, None, 2, 2, 30, P(o), P(o), None, None) == -1
+    assert lib.fcb_dev_stock_corr(P(x), 0, None, 1, 46341, P(o), None, None, None, None) == -3
+    assert lib.fcb_dev_stock_corr(P(x), 0, None, 1 << 16, 1 << 16, P(o), None, None, None, None) == -2
+    assert lib.fcb_dev_stock_corr(P(x), 0, None, 2, 2, P(o), None, None, None, None) == -1  # workspace required
+    ok = C.c_int(7)
+    assert lib.fcb_dev_corr_domain(P(x), 0, None, 2, 2, 2, 2, C.byref(ok), None) == -1      # layout flag
+    assert lib.fcb_dev_corr_domain(P(x), 3, None, 2, 2, 2, 0, C.byref(ok), None) == -1      # dtype
+    assert lib.fcb_dev_corr_domain(P(x), 1, None, 1 << 16, 1 << 16, 2, 0, C.byref(ok), None) == -2
+    assert lib.fcb_dev_corr_domain(P(x), 1, None, 2, 2, 2, 0, None, None) == -1
+    assert ok.value == 7
+
+
 def test_batch_contract_errors_without_device(native):
     """fcb_batch_create rejects bad panels with the single-panel codes before
     it touches a device; the default configuration is the documented one."""
