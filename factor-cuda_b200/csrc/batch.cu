@@ -21,10 +21,16 @@
 // from the default configuration it tries each knob's alternatives in turn
 // (coordinate descent), keeps a change when the graph replay gets faster, and
 // can remember the winner per batch signature in a small text cache file.
+// Each group's shared memory is sized for its widest section, so one panel
+// just above an occupancy step costs the whole group a resident CTA per SM;
+// besides fixed steps, the group boundaries tried are those steps (the widest
+// N that keeps each occupancy level), found from the occupancy calculator
+// over the batch's range of N.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <iterator>
 #include <new>
 #include <string>
 #include <vector>
@@ -280,6 +286,44 @@ int bind_device(const fcb_batch& b) {
   return dev == b.device ? FCB_OK : FCB_ERR_ARG;
 }
 
+// Resident CTAs per SM of the persistent kernel of block size nt with its
+// shared memory sized for sections of N cells (0 when it does not fit).
+int occ_at(const fcb_batch& b, int nt, int N, int* occ) {
+  *occ = 0;
+  const size_t smem = (b.dtx == FCB_DTYPE_F32) ? rank_ic_batch_smem<float, float>(nt, N)
+                                               : rank_ic_batch_smem<double, double>(nt, N);
+  if (smem > kMaxSmemPerBlock) return FCB_OK;
+  if (b.dtx == FCB_DTYPE_F32)
+    return rcode(launch_rank_ic_batch<float, float>(nt, b.learned,
+                                                    static_cast<const RankIcArgs<float, float>*>(b.d_args), nullptr,
+                                                    0, nullptr, 0, smem, nullptr, nullptr, occ));
+  return rcode(launch_rank_ic_batch<double, double>(nt, false, static_cast<const RankIcArgs<double, double>*>(b.d_args),
+                                                    nullptr, 0, nullptr, 0, smem, nullptr, nullptr, occ));
+}
+
+// Class boundaries worth measuring: for each occupancy level block size nt
+// reaches on [lo, hi], the largest N that still keeps it.  A class sized for
+// one cell more runs one resident CTA per SM fewer for all of its items.
+int occupancy_cliffs(const fcb_batch& b, int nt, int lo, int hi, std::vector<int>* out) {
+  int cur = std::max(1, lo);
+  while (cur <= hi) {
+    int o = 0;
+    int r = occ_at(b, nt, cur, &o);
+    if (r != FCB_OK) return r;
+    if (o < 1) break;
+    int a = cur, z = hi;  // occupancy does not grow with N: bisect for its last N
+    while (a < z) {
+      const int mid = a + (z - a + 1) / 2;
+      int om = 0;
+      if ((r = occ_at(b, nt, mid, &om)) != FCB_OK) return r;
+      if (om >= o) a = mid; else z = mid - 1;
+    }
+    out->push_back(a);
+    cur = a + 1;
+  }
+  return FCB_OK;
+}
+
 bool valid_cfg(const fcb_batch_config& c) {
   return c.nt_small_max >= 1 && c.nt_small_max <= 4096 && c.nt_mid_max > c.nt_small_max && c.nt_mid_max <= 8192 &&
          c.ctas_per_sm >= 0 && (c.concurrent == 0 || c.concurrent == 1) && (c.order == 0 || c.order == 1) &&
@@ -511,7 +555,7 @@ std::string signature(const fcb_batch& b) {
     work[k] += item_work(q) * q.T;
   }
   char buf[512];
-  int n = std::snprintf(buf, sizeof(buf), "fcb-batch-v1 n=%zu dt=%d/%d l=%d", b.p.size(), b.dtx, b.dtr,
+  int n = std::snprintf(buf, sizeof(buf), "fcb-batch-v2 n=%zu dt=%d/%d l=%d", b.p.size(), b.dtx, b.dtr,
                         b.learned ? 1 : 0);
   for (int k = 0; k < kClasses; ++k)
     n += std::snprintf(buf + n, sizeof(buf) - n, " c%d=%lld:%lld:%.3e", k, cnt[k], mx[k], work[k]);
@@ -596,10 +640,31 @@ extern "C" int fcb_batch_autotune(fcb_batch* b, int reps, const char* cache_path
     c.order = o;
     if ((r = consider(c)) != FCB_OK) return r;
   }
-  for (int v : small_opts) {
+  // class boundaries: fixed steps plus the occupancy cliffs inside the
+  // batch's range of section widths
+  int nmin = 1 << 30, nmax = 0;
+  for (const fcb_panel& q : b->p) {
+    nmin = std::min(nmin, q.N);
+    nmax = std::max(nmax, q.N);
+  }
+  std::vector<int> small_c(std::begin(small_opts), std::end(small_opts));
+  if ((r = occupancy_cliffs(*b, 256, nmin, std::min(nmax, 4096), &small_c)) != FCB_OK) return r;
+  std::sort(small_c.begin(), small_c.end());
+  small_c.erase(std::unique(small_c.begin(), small_c.end()), small_c.end());
+  for (int v : small_c) {
     fcb_batch_config c = best;
     if (c.nt_small_max == v) continue;
     c.nt_small_max = v;
+    if ((r = consider(c)) != FCB_OK) return r;
+  }
+  std::vector<int> mid_c{8192};
+  if ((r = occupancy_cliffs(*b, 512, best.nt_small_max + 1, std::min(nmax, 8192), &mid_c)) != FCB_OK) return r;
+  std::sort(mid_c.begin(), mid_c.end());
+  mid_c.erase(std::unique(mid_c.begin(), mid_c.end()), mid_c.end());
+  for (int v : mid_c) {
+    fcb_batch_config c = best;
+    if (c.nt_mid_max == v) continue;
+    c.nt_mid_max = v;
     if ((r = consider(c)) != FCB_OK) return r;
   }
   for (int v : cps_opts) {

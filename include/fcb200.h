@@ -344,7 +344,9 @@ int fcb_batch_run_per_panel(fcb_batch* b, void* stream);
  * in any run since the last call did not land. */
 int fcb_batch_status(fcb_batch* b);
 /* Measures the batch under alternative configurations (coordinate descent,
- * `reps` replays each) and keeps the fastest.  cache_path (or NULL): a text
+ * `reps` replays each) and keeps the fastest; the size-class boundaries tried
+ * include the occupancy steps of each block size within the batch's range of
+ * N.  cache_path (or NULL): a text
  * file of "signature<TAB>config ms" lines; a batch whose signature is found
  * takes that configuration without measuring (returns 1), a measured winner is
  * appended.  Returns 0 after measuring. */
