@@ -110,34 +110,19 @@ FCB_DEV uint32_t block_scan_max_sum(uint32_t c, int& mx, uint32_t& c2, uint32_t*
 // Outcome codes written to the per-(factor,date) statistics.
 constexpr int kLearnOk = 1, kLearnOverflow = 2, kLearnJudge = 3, kLearnScale = 4;
 
-// Start and end of the bucket holding sorted position q, from the bitmap of
-// bucket starts (bit p set <=> a non-empty bucket starts at p; bit 0 is always
-// set).  Buckets hold at most `cap` (<= 64) cells, so each scan is short.
-FCB_DEV void bucket_bounds(const uint32_t* bits, int q, int m, int& lo, int& hi) {
-  int w = q >> 5;
-  const int sh = q & 31;
-  uint32_t x = bits[w] & (0xFFFFFFFFu >> (31 - sh));  // starts at or before q
-  while (x == 0u) x = bits[--w];
-  lo = w * 32 + 31 - __clz(x);
-  w = q >> 5;
-  x = (sh == 31) ? 0u : (bits[w] & (0xFFFFFFFFu << (sh + 1)));  // starts after q
-  while (x == 0u && (w + 1) * 32 < m) x = bits[++w];
-  hi = (x != 0u) ? min(m, w * 32 + __ffs(x) - 1) : m;
-}
-
 // Sort the m compacted pairs (kA, iA) with the bucket map.  On success the
 // sorted sequence is in (kA, iA) and the return is kLearnOk.  kLearnOverflow /
 // kLearnScale leave (kA, iA) untouched; kLearnJudge leaves them permuted (the
 // caller must rebuild them before falling back).
 //   cnt:   u16 array of at least m+2 entries, 4-byte aligned (bucket counters)
-//   bits:  u32 bitmap of at least m/32+2 words (bucket starts)
-//   fscratch: >= 32 doubles; scan: >= 33 u32.
+//   fscratch: >= 32 doubles; scan: >= 99 u32.
 // The bucket of each cell is evaluated once (histogram pass) and parked in iB,
-// which is idle until the scatter; the scatter reads it back into registers.
+// which is idle until the scatter; the scatter reads it back into registers
+// and each thread keeps its cells' buckets and slots there for the ranking.
 template <int NT, int MAXIPT>
 FCB_DEV int learned_sort(uint32_t* kA, uint16_t* iA, uint32_t* kB, uint16_t* iB, int m, uint16_t* cnt,
-                         uint32_t* bits, const float* tab, float lo, float hi, int cap, double* dscratch,
-                         uint32_t* scan, int* max_bucket_out, int* sumsq_out) {
+                         const float* tab, float lo, float hi, int cap, double* dscratch, uint32_t* scan,
+                         int* max_bucket_out, int* sumsq_out) {
   if (m <= 1) return kLearnOk;
   // per-date standardisation: mean and mean absolute deviation of an evenly
   // spaced sample of the compacted cells, one per thread (they only shape the
@@ -160,9 +145,7 @@ FCB_DEV int learned_sort(uint32_t* kA, uint16_t* iA, uint32_t* kB, uint16_t* iB,
       !isfinite(bm.inv_dz) || !(bm.inv_dz > 0.0f))
     return kLearnScale;
   // histogram (packed 16-bit counters); each cell's bucket parked in iB
-  const int nwords = (m >> 5) + 2;
   for (int b = threadIdx.x; b < (m + 2) / 2; b += NT) reinterpret_cast<uint32_t*>(cnt)[b] = 0u;
-  for (int w = threadIdx.x; w < nwords; w += NT) bits[w] = 0u;
   __syncthreads();
   for (int p = threadIdx.x; p < m; p += NT) {
     const int b = bm(kA[p]);
@@ -171,7 +154,7 @@ FCB_DEV int learned_sort(uint32_t* kA, uint16_t* iA, uint32_t* kB, uint16_t* iB,
   }
   __syncthreads();
   // exclusive scan of the counts -> bucket starts (in place), largest bucket,
-  // sum of squared sizes, bitmap of bucket starts
+  // sum of squared sizes
   {
     const int per = (m + NT - 1) / NT;
     const int b0 = threadIdx.x * per, b1 = min(m, b0 + per);
@@ -190,48 +173,56 @@ FCB_DEV int learned_sort(uint32_t* kA, uint16_t* iA, uint32_t* kB, uint16_t* iB,
     for (int b = b0; b < b1; ++b) {
       const uint32_t v = cnt[b];
       cnt[b] = static_cast<uint16_t>(run);
-      if (v != 0u) atomicOr(&bits[run >> 5], 1u << (run & 31));
       run += v;
     }
     __syncthreads();
   }
-  // scatter into bucket slots (order inside a bucket is arbitrary)
-  {
-    uint32_t breg[(MAXIPT + 1) / 2];
+  // scatter into bucket slots (order inside a bucket is arbitrary); each
+  // thread keeps the bucket and the slot of each of its cells, two per word
+  uint32_t breg[(MAXIPT + 1) / 2], sreg[(MAXIPT + 1) / 2];
 #pragma unroll
-    for (int j = 0; j < MAXIPT; j += 2) {
-      const int p0 = threadIdx.x + j * NT, p1 = p0 + NT;
-      const uint32_t b0 = p0 < m ? iB[p0] : 0u;
-      const uint32_t b1 = (j + 1 < MAXIPT && p1 < m) ? iB[p1] : 0u;
-      breg[j >> 1] = b0 | (b1 << 16);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < MAXIPT; ++j) {
-      const int p = threadIdx.x + j * NT;
-      if (p < m) {
-        const int b = static_cast<int>((breg[j >> 1] >> ((j & 1) * 16)) & 0xFFFFu);
-        const uint32_t pos = packed_inc(cnt, b);
-        kB[pos] = kA[p];
-        iB[pos] = iA[p];
-      }
-    }
-    __syncthreads();
+  for (int j = 0; j < MAXIPT; j += 2) {
+    const int p0 = threadIdx.x + j * NT, p1 = p0 + NT;
+    const uint32_t b0 = p0 < m ? iB[p0] : 0u;
+    const uint32_t b1 = (j + 1 < MAXIPT && p1 < m) ? iB[p1] : 0u;
+    breg[j >> 1] = b0 | (b1 << 16);
+    sreg[j >> 1] = 0u;
   }
-  // rank inside the bucket by (key, column): keys first, column ids on ties
-  for (int q = threadIdx.x; q < m; q += NT) {
-    const uint32_t key = kB[q];
-    const uint16_t id = iB[q];
-    int lo_b, hi_b;
-    bucket_bounds(bits, q, m, lo_b, hi_b);
-    int r = 0;
-    for (int s2 = lo_b; s2 < hi_b; ++s2) {
-      const uint32_t k2 = kB[s2];
-      r += (k2 < key) ? 1 : 0;
-      if (k2 == key) r += (iB[s2] < id) ? 1 : 0;
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < MAXIPT; ++j) {
+    const int p = threadIdx.x + j * NT;
+    if (p < m) {
+      const int b = static_cast<int>((breg[j >> 1] >> ((j & 1) * 16)) & 0xFFFFu);
+      const uint32_t pos = packed_inc(cnt, b);
+      kB[pos] = kA[p];
+      iB[pos] = iA[p];
+      sreg[j >> 1] |= pos << ((j & 1) * 16);
     }
-    kA[lo_b + r] = key;
-    iA[lo_b + r] = id;
+  }
+  __syncthreads();
+  // rank inside the bucket by (key, column): keys first, column ids on ties.
+  // After the scatter cnt[b] is the end of bucket b, and bucket b starts
+  // where bucket b - 1 ends (the buckets tile [0, m) in order).
+#pragma unroll
+  for (int j = 0; j < MAXIPT; ++j) {
+    const int p = threadIdx.x + j * NT;
+    if (p < m) {
+      const int b = static_cast<int>((breg[j >> 1] >> ((j & 1) * 16)) & 0xFFFFu);
+      const int pos = static_cast<int>((sreg[j >> 1] >> ((j & 1) * 16)) & 0xFFFFu);
+      const int lo_b = b > 0 ? static_cast<int>(cnt[b - 1]) : 0;
+      const int hi_b = static_cast<int>(cnt[b]);
+      const uint32_t key = kB[pos];
+      const uint16_t id = iB[pos];
+      int r = 0;
+      for (int s2 = lo_b; s2 < hi_b; ++s2) {
+        const uint32_t k2 = kB[s2];
+        r += (k2 < key) ? 1 : 0;
+        if (k2 == key) r += (iB[s2] < id) ? 1 : 0;
+      }
+      kA[lo_b + r] = key;
+      iA[lo_b + r] = id;
+    }
   }
   __syncthreads();
   // judge: strictly increasing (key, column) over the whole row

@@ -365,24 +365,16 @@ FCB_DEV bool rank_ic_factor(const RankIcArgs<TF, TR>& a, const int t, const int 
   uint16_t* ifs = i0;
   bool sorted = false;
   if (LEARNED && a.cdf_table != nullptr) {
-    // the radix histogram and digit-base regions are idle here: they hold
-    // this factor's table and the bitmap of bucket starts
-    using S = SortScratch<NT>;
+    // the radix histogram region is idle here: it holds this factor's table
     float* tab = reinterpret_cast<float*>(sm + L.scratch);
-    constexpr size_t kTabBytes = kCdfKnots * sizeof(float);
-    static_assert(S::hist_bytes >= kTabBytes, "table must fit the histogram region");
-    static_assert(S::hist_bytes >= kTabBytes + (NT * MAXIPT / 32 + 2) * 4 ||
-                      S::base_bytes >= (NT * MAXIPT / 32 + 2) * 4,
-                  "bucket-start bitmap must fit an idle region");
-    uint32_t* bits = reinterpret_cast<uint32_t*>(
-        sm + L.scratch + (S::hist_bytes >= kTabBytes + (NT * MAXIPT / 32 + 2) * 4 ? kTabBytes : S::hist_bytes));
+    static_assert(SortScratch<NT>::hist_bytes >= kCdfKnots * sizeof(float), "table must fit the histogram region");
     if (!table_staged) {
       for (int k = threadIdx.x; k < kCdfKnots; k += NT) tab[k] = a.cdf_table[static_cast<size_t>(f) * kCdfKnots + k];
       __syncthreads();
     }
     int mb = 0, ss = 0;
     const int st = learned_sort<NT, MAXIPT>(reinterpret_cast<uint32_t*>(kf0), i0, reinterpret_cast<uint32_t*>(kf1),
-                                            i1, mf, RR, bits, tab, a.cdf_zrange[2 * f], a.cdf_zrange[2 * f + 1],
+                                            i1, mf, RR, tab, a.cdf_zrange[2 * f], a.cdf_zrange[2 * f + 1],
                                             a.learn_cap, reinterpret_cast<double*>(scan64), scan, &mb, &ss);
     if (a.learn_stats != nullptr && threadIdx.x == 0) {
       int* o = a.learn_stats + (static_cast<size_t>(f) * T + t) * 4;
