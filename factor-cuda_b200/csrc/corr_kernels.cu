@@ -585,6 +585,43 @@ __global__ void k_fc_colfinal(const FcColPart* __restrict__ part, int nblk, int 
 // Rows staged per step: 32 for F >= 64, more for narrower panels so that the
 // staged tile stays near 48 KB (fewer barriers per row, two blocks per SM).
 __host__ __device__ inline int fc_rows_chunk(int Fp) { return 32 * (64 / Fp > 8 ? 8 : (64 / Fp < 1 ? 1 : 64 / Fp)); }
+// Staged tile layout: column f of the centred values at sx[f * pitch + row],
+// the validity tile at the same offsets from sm.  pitch = chunk + 1 is odd, so
+// column f starts on bank pair 2f (mod 32) and consecutive rows of a column
+// are consecutive words; sm starts 2 doubles past a 16-double boundary (bank
+// offset 4), so the columns {c, c+4, c+8} of both tiles that one load of a
+// warp touches, on one row or on two adjacent rows, fall in distinct banks.
+__host__ __device__ inline int fc_stage_pitch(int Fp) { return fc_rows_chunk(Fp) + 1; }
+// Tasks (4x4 tiles) of the Gram pass: the symmetric products n and sxy need
+// only the tiles on or above the diagonal (k_fc_final reads (i, j) with
+// i <= j), sx and sx2 need all tb x tb tiles (read as (i, j) and (j, i)).
+// Order: n upper tiles, sx, sx2, sxy upper tiles.
+__host__ __device__ inline int fc_gram_tasks(int tb) { return tb * (tb + 1) + 2 * tb * tb; }
+FCB_DEV void fc_gram_task(int tk, int tb, int& p, int& fa, int& ga) {
+  const int ntri = tb * (tb + 1) / 2, nsq = tb * tb;
+  int k;
+  if (tk < ntri) {
+    p = 0;
+    k = tk;
+  } else if (tk < ntri + 2 * nsq) {
+    p = tk < ntri + nsq ? 1 : 2;
+    const int rem = tk - ntri - (p - 1) * nsq;
+    fa = (rem / tb) * 4;
+    ga = (rem % tb) * 4;
+    return;
+  } else {
+    p = 3;
+    k = tk - ntri - 2 * nsq;
+  }
+  int a = 0;
+  while (k >= tb - a) {  // row a of the upper triangle holds tiles (a, a .. tb-1)
+    k -= tb - a;
+    ++a;
+  }
+  fa = a * 4;
+  ga = (a + k) * 4;
+}
+__host__ __device__ inline int fc_stage_sm_offset(int Fp) { return (Fp * fc_stage_pitch(Fp) + 15) / 16 * 16 + 2; }
 
 template <typename TIN>
 __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
@@ -593,9 +630,10 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
                                                  const FcColStat* __restrict__ st, int tasks_total,
                                                  int tasks_per_block, double* __restrict__ part) {
   extern __shared__ __align__(16) double fsm[];
-  double* sx = fsm;                                  // [chunk][Fp] centred values
   const int chunk = fc_rows_chunk(Fp);
-  double* sm = sx + chunk * Fp;                      // [chunk][Fp] validity
+  const int pitch = fc_stage_pitch(Fp);
+  double* sx = fsm;                                  // [Fp][pitch] centred values
+  double* sm = sx + fc_stage_sm_offset(Fp);          // [Fp][pitch] validity
   double* red = fsm;  // [slices][tasks_per_block][16], over the staging tile once it is idle
   const int tb = Fp / 4;
   const int task0 = blockIdx.y * tasks_per_block;
@@ -605,13 +643,7 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
   const int my_slice = threadIdx.x / tasks_per_block;
   const bool active = (my_slice < slices) && (my_task < ntask);
   int p = 0, fa = 0, ga = 0;
-  if (active) {
-    const int tk = task0 + my_task;
-    p = tk / (tb * tb);
-    const int rem = tk % (tb * tb);
-    fa = (rem / tb) * 4;
-    ga = (rem % tb) * 4;
-  }
+  if (active) fc_gram_task(task0 + my_task, tb, p, fa, ga);
   double acc[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) acc[q] = 0.0;
@@ -623,7 +655,7 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
       // consecutive threads read consecutive elements of X in either layout
       const int rr = (sf == 1) ? e / Fp : e % chunk;
       const int f = (sf == 1) ? e % Fp : e / chunk;
-      const int ei = rr * Fp + f;
+      const int ei = f * pitch + rr;
       double v = 0.0, mv = 0.0;
       if (rr < nr && f < F) {
         const long long r = c0 + rr;
@@ -641,16 +673,16 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
       const double* A = (p == 0) ? sm : sx;  // product 2 squares the centred values below
       const double* B = (p == 3) ? sx : sm;
       for (int rr = my_slice; rr < nr; rr += slices) {
-        const double* ar = A + rr * Fp + fa;
-        const double* br = B + rr * Fp + ga;
-        double a0 = ar[0], a1 = ar[1], a2 = ar[2], a3 = ar[3];
+        const double* ar = A + fa * pitch + rr;
+        const double* br = B + ga * pitch + rr;
+        double a0 = ar[0], a1 = ar[pitch], a2 = ar[2 * pitch], a3 = ar[3 * pitch];
         if (p == 2) {
           a0 *= a0;
           a1 *= a1;
           a2 *= a2;
           a3 *= a3;
         }
-        const double b0 = br[0], b1 = br[1], b2 = br[2], b3 = br[3];
+        const double b0 = br[0], b1 = br[pitch], b2 = br[2 * pitch], b3 = br[3 * pitch];
         const double av[4] = {a0, a1, a2, a3}, bv[4] = {b0, b1, b2, b3};
 #pragma unroll
         for (int u = 0; u < 4; ++u)
@@ -671,10 +703,9 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
     const int tk = e / 16, q = e % 16;
     double s = 0.0;
     for (int sl = 0; sl < slices; ++sl) s += red[(static_cast<size_t>(sl) * tasks_per_block + tk) * 16 + q];
-    const int gt = task0 + tk;
-    const int pp = gt / (tb * tb);
-    const int rem = gt % (tb * tb);
-    const int f = (rem / tb) * 4 + q / 4, g = (rem % tb) * 4 + q % 4;
+    int pp = 0, f0 = 0, g0 = 0;
+    fc_gram_task(task0 + tk, tb, pp, f0, g0);
+    const int f = f0 + q / 4, g = g0 + q % 4;
     part[((static_cast<size_t>(blockIdx.x) * 4 + pp) * Fp + f) * Fp + g] = s;
   }
 }
@@ -1117,7 +1148,7 @@ int fc_fb_nblk(long long R, int F) {
 
 size_t fc_gram_smem(int Fp, int tasks_per_block) {
   const int slices = 256 / tasks_per_block;
-  const size_t stage = 2 * static_cast<size_t>(fc_rows_chunk(Fp)) * Fp;
+  const size_t stage = static_cast<size_t>(fc_stage_sm_offset(Fp)) + static_cast<size_t>(Fp) * fc_stage_pitch(Fp);
   const size_t red = static_cast<size_t>(slices) * tasks_per_block * 16;
   return (stage > red ? stage : red) *
          sizeof(double);
@@ -1128,7 +1159,7 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
                                        cudaStream_t s) {
   const int Fp = (F + 3) / 4 * 4;
   const int tb = Fp / 4;
-  const int tasks_total = 4 * tb * tb;
+  const int tasks_total = fc_gram_tasks(tb);
   const int tasks_per_block = tasks_total <= 256 ? tasks_total : 256;
   const int ytiles = (tasks_total + tasks_per_block - 1) / tasks_per_block;
   const long long rpb_cols = (R + w.nblk_cols - 1) / w.nblk_cols;
