@@ -582,9 +582,13 @@ __global__ void k_fc_colfinal(const FcColPart* __restrict__ part, int nblk, int 
 // 2 sx2=(x'^2,m), 3 sxy=(x',x').  Each thread owns a 4x4 (f,g) tile of one
 // product and a slice of the staged rows; slices are summed in shared memory
 // in a fixed order at the end of the block.
-// Rows staged per step: 32 for F >= 64, more for narrower panels so that the
-// staged tile stays near 48 KB (fewer barriers per row, two blocks per SM).
-__host__ __device__ inline int fc_rows_chunk(int Fp) { return 32 * (64 / Fp > 8 ? 8 : (64 / Fp < 1 ? 1 : 64 / Fp)); }
+// Rows staged per step: 16 for F > 64, 32 for F in (32, 64], more for
+// narrower panels (fewer barriers per row); with the raw-copy double buffer
+// the block stays under 75 KB of shared memory for every F <= 128 and both
+// input widths, so three blocks fit an SM.
+__host__ __device__ inline int fc_rows_chunk(int Fp) {
+  return Fp > 64 ? 16 : 32 * (64 / Fp > 8 ? 8 : (64 / Fp < 1 ? 1 : 64 / Fp));
+}
 // Staged tile layout: column f of the centred values at sx[f * pitch + row],
 // the validity tile at the same offsets from sm.  pitch = chunk + 1 is odd, so
 // column f starts on bank pair 2f (mod 32) and consecutive rows of a column
@@ -622,6 +626,23 @@ FCB_DEV void fc_gram_task(int tk, int tb, int& p, int& fa, int& ga) {
   ga = (a + k) * 4;
 }
 __host__ __device__ inline int fc_stage_sm_offset(int Fp) { return (Fp * fc_stage_pitch(Fp) + 15) / 16 * 16 + 2; }
+// Doubles before the raw-copy buffers: the staged tiles, or the slice
+// reduction buffer that reuses them after the row loop, whichever is larger.
+__host__ __device__ inline size_t fc_gram_raw_offset(int Fp, int tasks_per_block) {
+  const size_t stage = static_cast<size_t>(fc_stage_sm_offset(Fp)) + static_cast<size_t>(Fp) * fc_stage_pitch(Fp);
+  const size_t red = static_cast<size_t>(256 / tasks_per_block) * tasks_per_block * 16;
+  return ((stage > red ? stage : red) + 1) / 2 * 2;  // 16-byte aligned
+}
+
+// Asynchronous global -> shared copies of single elements (cp.async, L1
+// allocating); each thread waits for its own groups, a barrier publishes them.
+template <int BYTES>
+FCB_DEV void cp_async_elem(void* smem, const void* gmem) {
+  static_assert(BYTES == 4 || BYTES == 8, "element copies are 4 or 8 bytes");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(smem)), "l"(gmem), "n"(BYTES) : "memory");
+}
+FCB_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+FCB_DEV void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 template <typename TIN>
 __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
@@ -649,18 +670,53 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
   for (int q = 0; q < 16; ++q) acc[q] = 0.0;
   const long long r0 = blockIdx.x * rows_per_block;
   const long long r1 = min(R, r0 + rows_per_block);
-  for (long long c0 = r0; c0 < r1; c0 += chunk) {
-    const int nr = static_cast<int>(min(static_cast<long long>(chunk), r1 - c0));
+  // Row chunks are pipelined: while chunk k is centred and multiplied, the raw
+  // elements of chunk k + 1 are in flight into the other raw buffer
+  // (cp.async) and its mask bytes in a register.
+  TIN* raw[2];
+  raw[0] = reinterpret_cast<TIN*>(fsm + fc_gram_raw_offset(Fp, tasks_per_block));
+  raw[1] = raw[0] + chunk * Fp;
+  uint8_t* smask = reinterpret_cast<uint8_t*>(raw[1] + chunk * Fp);
+  auto issue = [&](long long cs, TIN* dst) {
+    const int nrs = static_cast<int>(min(static_cast<long long>(chunk), r1 - cs));
     for (int e = threadIdx.x; e < chunk * Fp; e += 256) {
       // consecutive threads read consecutive elements of X in either layout
+      const int rr = (sf == 1) ? e / Fp : e % chunk;
+      const int f = (sf == 1) ? e % Fp : e / chunk;
+      if (rr < nrs && f < F) cp_async_elem<sizeof(TIN)>(dst + e, X + (cs + rr) * sr + f * sf);
+    }
+  };
+  auto mask_of = [&](long long cs) -> uint8_t {
+    const long long r = cs + threadIdx.x;
+    return (mask == nullptr || threadIdx.x >= chunk || r >= r1) ? uint8_t(1) : mask[r];
+  };
+  uint8_t m_cur = 1;
+  if (r0 < r1) {
+    issue(r0, raw[0]);
+    m_cur = mask_of(r0);
+  }
+  cp_async_commit();
+  int it = 0;
+  for (long long c0 = r0; c0 < r1; c0 += chunk, ++it) {
+    const int nr = static_cast<int>(min(static_cast<long long>(chunk), r1 - c0));
+    uint8_t m_next = 1;
+    if (c0 + chunk < r1) {
+      issue(c0 + chunk, raw[(it + 1) & 1]);
+      m_next = mask_of(c0 + chunk);
+    }
+    cp_async_commit();
+    if (threadIdx.x < chunk) smask[threadIdx.x] = m_cur;
+    cp_async_wait_prev();  // this thread's copies of chunk `it` have landed
+    __syncthreads();
+    const TIN* rb = raw[it & 1];
+    for (int e = threadIdx.x; e < chunk * Fp; e += 256) {
       const int rr = (sf == 1) ? e / Fp : e % chunk;
       const int f = (sf == 1) ? e % Fp : e / chunk;
       const int ei = f * pitch + rr;
       double v = 0.0, mv = 0.0;
       if (rr < nr && f < F) {
-        const long long r = c0 + rr;
-        const double x = static_cast<double>(X[r * sr + f * sf]);
-        if (finite_f64(x) && (mask == nullptr || mask[r] != 0)) {
+        const double x = static_cast<double>(rb[e]);
+        if (finite_f64(x) && smask[rr] != 0) {
           v = x - st[f].mean;
           mv = 1.0;
         }
@@ -691,6 +747,7 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
       }
     }
     __syncthreads();
+    m_cur = m_next;
   }
   // reduce slices in fixed order
   if (active) {
@@ -1146,12 +1203,9 @@ int fc_fb_nblk(long long R, int F) {
   return static_cast<int>(std::max<long long>(nb, 1));
 }
 
-size_t fc_gram_smem(int Fp, int tasks_per_block) {
-  const int slices = 256 / tasks_per_block;
-  const size_t stage = static_cast<size_t>(fc_stage_sm_offset(Fp)) + static_cast<size_t>(Fp) * fc_stage_pitch(Fp);
-  const size_t red = static_cast<size_t>(slices) * tasks_per_block * 16;
-  return (stage > red ? stage : red) *
-         sizeof(double);
+size_t fc_gram_smem(int Fp, int tasks_per_block, int elem_bytes) {
+  const size_t raw = 2 * static_cast<size_t>(fc_rows_chunk(Fp)) * Fp * elem_bytes + fc_rows_chunk(Fp);
+  return fc_gram_raw_offset(Fp, tasks_per_block) * sizeof(double) + (raw + 15) / 16 * 16;
 }
 
 cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* mask, long long R, int F,
@@ -1175,7 +1229,7 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
   if (e != cudaSuccess) return e;
   k_fc_colfinal<<<(F * 32 + 127) / 128, 128, 0, s>>>(w.colpart, w.nblk_cols, F, w.colstat);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const size_t smem = fc_gram_smem(Fp, tasks_per_block);
+  const size_t smem = fc_gram_smem(Fp, tasks_per_block, dtype == 0 ? 4 : 8);
   dim3 gg(w.nblk_gram, ytiles);
   if (dtype == 0) {
     e = cudaFuncSetAttribute(k_fc_gram<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));

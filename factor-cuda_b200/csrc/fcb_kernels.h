@@ -134,7 +134,7 @@ cudaError_t launch_corr_domain(const void* X, int dtype, const uint8_t* mask, lo
                                unsigned long long* ext, cudaStream_t s);
 cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const double* Mc, const ColStat* st, int T,
                                    int N, int Tp, double* out, int* fb_list, int* fb_count, cudaStream_t s);
-size_t fc_gram_smem(int Fp, int tasks_per_block);
+size_t fc_gram_smem(int Fp, int tasks_per_block, int elem_bytes);
 cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
                                double* out, uint8_t* flags, cudaStream_t s);
 // Returns of each date prepared once for the per-(date, factor) rank + IC

@@ -215,6 +215,24 @@ def test_factor_corr_random(fcp):
     assert np.array_equal(got, fcp.factor_corr_f64(F3.astype(np.float64), m), equal_nan=True)
 
 
+@pytest.mark.parametrize("F", [33, 64, 65, 128])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_factor_corr_wide_panels(fcp, F, dtype):
+    """Wide panels up to the F <= 128 cap: the Gram pass stages fewer rows
+    per step above F = 64 and splits its tiles over several block rows."""
+    rng = np.random.default_rng(F)
+    T, N = 12, 700
+    F3 = rng.standard_normal((T, N, F))
+    F3[..., 1] += 0.5 * F3[..., 0]
+    F3[..., 2] = np.exp(F3[..., 2]) + 50.0          # far-from-zero mean: the cancellation fallback
+    F3[..., F - 1] = 3.0                            # constant factor
+    F3[rng.random((T, N, F)) < 0.03] = np.nan
+    F3 = F3.astype(dtype)
+    m = rng.random((T, N)) < 0.93
+    got = fcp.factor_corr_f64(F3, m)
+    assert corr_match(got, O.factor_corr(F3, m))
+
+
 def test_factor_corr_large_pool_fallback():
     """Pairs the cancellation gate flags on a large pool (200k rows) take the
     multi-block two-pass fallback: same results as the oracle (<= 1e-12) and
