@@ -92,6 +92,47 @@ FCB_DEV uint32_t chunk_prefix(int m, Pred pred, int& b, int& e, uint32_t* scan, 
   return block_exclusive_sum(c, scan, total);
 }
 
+// The rank + IC epilogue's block results in one reduction round: the sum of
+// joint rank products and the first / last joint positions on the returns
+// and factor sides (integer sums and extrema: any order gives the same
+// result).  scratch: >= 32 * 24 bytes, idle between the two barriers' callers.
+struct IcEnds {
+  unsigned long long sum;
+  int rfirst, rlast, ffirst, flast;
+};
+
+FCB_DEV IcEnds block_reduce_ends(IcEnds v, uint8_t* scratch) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.sum += __shfl_xor_sync(kFull, v.sum, o);
+    v.rfirst = min(v.rfirst, __shfl_xor_sync(kFull, v.rfirst, o));
+    v.rlast = max(v.rlast, __shfl_xor_sync(kFull, v.rlast, o));
+    v.ffirst = min(v.ffirst, __shfl_xor_sync(kFull, v.ffirst, o));
+    v.flast = max(v.flast, __shfl_xor_sync(kFull, v.flast, o));
+  }
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  unsigned long long* s64 = reinterpret_cast<unsigned long long*>(scratch);
+  int* si = reinterpret_cast<int*>(scratch + 32 * sizeof(unsigned long long));
+  if (lane_id() == 0) {
+    s64[w] = v.sum;
+    si[w] = v.rfirst;
+    si[32 + w] = v.rlast;
+    si[64 + w] = v.ffirst;
+    si[96 + w] = v.flast;
+  }
+  __syncthreads();
+  IcEnds r{0ull, 0x7fffffff, -1, 0x7fffffff, -1};
+  for (int i = 0; i < nw; ++i) {
+    r.sum += s64[i];
+    r.rfirst = min(r.rfirst, si[i]);
+    r.rlast = max(r.rlast, si[32 + i]);
+    r.ffirst = min(r.ffirst, si[64 + i]);
+    r.flast = max(r.flast, si[96 + i]);
+  }
+  __syncthreads();
+  return r;
+}
+
 FCB_DEV void store_row_f32(float* __restrict__ dst, const float* __restrict__ src, int n) {
   // dst and src share the same 16-byte phase whenever N % 4 == 0 and the
   // panel is 16-aligned; fall back to scalar stores otherwise.
@@ -400,23 +441,9 @@ FCB_DEV bool rank_ic_factor(const RankIcArgs<TF, TR>& a, const int t, const int 
   }
   if (!sorted) block_radix_sort<NT, MAXIPT, KF>(kf0, i0, kf1, i1, mf, sm + L.scratch, &kfs, &ifs);
 
-  // returns side: joint ranks in return order, first/last joint position
-  int b, e;
-  uint32_t mj;
-  uint32_t c = chunk_prefix(mr, [&](int p) { return flags[IR[p]] == 7u; }, b, e, scan, mj);
-  int rfirst = 0x7fffffff, rlast = -1;
-  for (int p = b; p < e; ++p) {
-    const int i = IR[p];
-    if (flags[i] == 7u) {
-      RR[i] = static_cast<uint16_t>(++c);
-      rfirst = min(rfirst, p);
-      rlast = max(rlast, p);
-    }
-  }
-  rfirst = block_min_int(rfirst, reinterpret_cast<int*>(scan));
-  rlast = block_max_int(rlast, reinterpret_cast<int*>(scan));
-
-  // factor side: cs ranks, joint ranks, sum of rank products
+  // the idle key buffer receives the cs ranks; cells left out of the factor's
+  // valid set keep the quiet NaN (the barriers inside the two prefix counts
+  // below order these stores before the rank stores)
   float* rbuf = reinterpret_cast<float*>(kfs == kf0 ? kf1 : kf0);
   const bool want_ranks = a.ranks_out != nullptr;
   if (want_ranks) {
@@ -429,36 +456,52 @@ FCB_DEV bool rank_ic_factor(const RankIcArgs<TF, TR>& a, const int t, const int 
       a.rank_r_out[frow + i] = 0.0;
     }
   }
-  __syncthreads();
+
+  // returns side: joint ranks in return order, first/last joint position
+  int b, e;
+  uint32_t mj;
+  uint32_t c = chunk_prefix(mr, [&](int p) { return flags[IR[p]] == 7u; }, b, e, scan, mj);
+  IcEnds ends{0ull, 0x7fffffff, -1, 0x7fffffff, -1};
+  for (int p = b; p < e; ++p) {
+    const int i = IR[p];
+    if (flags[i] == 7u) {
+      RR[i] = static_cast<uint16_t>(++c);
+      ends.rfirst = min(ends.rfirst, p);
+      ends.rlast = max(ends.rlast, p);
+    }
+  }
+
+  // factor side: cs ranks, joint ranks, sum of rank products (the prefix
+  // count's barriers also publish RR)
   uint32_t mj2;
   uint32_t cf = chunk_prefix(mf, [&](int p) { return flags[ifs[p]] == 7u; }, b, e, scan, mj2);
   long long sum = 0;
-  int ffirst = 0x7fffffff, flast = -1;
   for (int p = b; p < e; ++p) {
     const int i = ifs[p];
     if (want_ranks) rbuf[i] = static_cast<float>(p + 1);
     if (flags[i] == 7u) {
       ++cf;
       sum += static_cast<long long>(cf) * RR[i];
-      ffirst = min(ffirst, p);
-      flast = max(flast, p);
+      ends.ffirst = min(ends.ffirst, p);
+      ends.flast = max(ends.flast, p);
       if (a.rank_f_out != nullptr) {
         a.rank_f_out[frow + i] = static_cast<double>(cf);
         a.rank_r_out[frow + i] = static_cast<double>(RR[i]);
       }
     }
   }
-  sum = block_sum<unsigned long long>(static_cast<unsigned long long>(sum), scan64);
-  ffirst = block_min_int(ffirst, reinterpret_cast<int*>(scan));
-  flast = block_max_int(flast, reinterpret_cast<int*>(scan));
+  ends.sum = static_cast<unsigned long long>(sum);
+  // the sort scratch is idle here (the learned table too)
+  ends = block_reduce_ends(ends, sm + L.scratch);
+  const int ffirst = ends.ffirst, flast = ends.flast;
   // block-collective: do the joint returns at rfirst and rlast share a key?
-  const bool rconst = same_ret_group(rfirst, rlast);
+  const bool rconst = same_ret_group(ends.rfirst, ends.rlast);
   if (threadIdx.x == 0) {
     double ic = __longlong_as_double(0x7ff8000000000000ll);
     const long long m = static_cast<long long>(mj);
     if (m >= a.min_valid && m >= 2) {
       const bool fconst = kfs[ffirst] == kfs[flast];
-      if (!fconst && !rconst) ic = spearman_from_sum(m, sum);
+      if (!fconst && !rconst) ic = spearman_from_sum(m, static_cast<long long>(ends.sum));
     }
     a.ic_out[static_cast<size_t>(f) * (a.ic_ld > 0 ? a.ic_ld : T) + t] = ic;
   }
