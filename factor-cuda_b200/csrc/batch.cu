@@ -68,6 +68,10 @@ struct fcb_batch {
   int2* d_items = nullptr;         // items grouped by class
   size_t items_cap = 0;
   int* d_ctr = nullptr;            // queue heads [kClasses]
+  // per-panel arm (f32): each panel's prepared returns for the per-(date,
+  // factor) path that the single-panel entry points take with F >= 2
+  void* d_prep_mem = nullptr;
+  std::vector<RicPrep> preps;
   int* d_status = nullptr;
   std::vector<FcWork> fcw;
   std::vector<void*> fc_mem;
@@ -94,6 +98,7 @@ struct fcb_batch {
     cudaFree(d_args);
     cudaFree(d_items);
     cudaFree(d_ctr);
+    cudaFree(d_prep_mem);
     cudaFree(d_status);
     for (void* m : fc_mem) cudaFree(m);
     fc_mem.clear();
@@ -110,6 +115,7 @@ struct fcb_batch {
     d_args = nullptr;
     d_items = nullptr;
     d_ctr = nullptr;
+    d_prep_mem = nullptr;
     d_status = nullptr;
   }
 };
@@ -433,6 +439,20 @@ extern "C" int fcb_batch_create(const fcb_panel* panels, int npanels, int dtype_
     c8 += 256;
     w.fb_part = reinterpret_cast<double*>(c8);
   }
+  if (dtype_x == FCB_DTYPE_F32) {
+    // prepared returns for the per-panel arm (ric_prep_bytes per panel, 256-byte aligned)
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    size_t total = 0;
+    for (int i = 0; i < npanels; ++i) total += al(ric_prep_bytes(panels[i].T, panels[i].N));
+    e = cudaMalloc(&b->d_prep_mem, total);
+    if (e != cudaSuccess) return fail(rcode(e));
+    b->preps.resize(npanels);
+    uint8_t* c8 = static_cast<uint8_t*>(b->d_prep_mem);
+    for (int i = 0; i < npanels; ++i) {
+      b->preps[i] = ric_prep_carve(c8, panels[i].T, panels[i].N);
+      c8 += al(ric_prep_bytes(panels[i].T, panels[i].N));
+    }
+  }
   const int r = (dtype_x == FCB_DTYPE_F32) ? upload_args<float, float>(*b) : upload_args<double, double>(*b);
   if (r != FCB_OK) return fail(r);
   *out = b;
@@ -485,14 +505,20 @@ extern "C" int fcb_batch_run_per_panel(fcb_batch* b, void* stream) {
       a.min_valid = b->min_valid;
       a.ranks_out = q.ranks_out;
       a.ic_out = q.ic_out;
-      if (q.model != nullptr) {
+      const bool lrn = q.model != nullptr;
+      if (lrn) {
         a.cdf_table = q.model->table[q.model->cur];
         a.cdf_zrange = q.model->zrange[q.model->cur];
         a.learn_cap = b->cfg.learn_cap > 0 ? b->cfg.learn_cap : 64;
-        FCB_BTRY(launch_rank_ic_learned(a, b->d_status, s));
-      } else {
-        FCB_BTRY(launch_rank_ic<float, float>(a, b->d_status, s));
       }
+      // as the single-panel entry points: several factors go through the
+      // prepared returns and per-(date, factor) items, one factor per date
+      if (a.F >= 2)
+        FCB_BTRY(launch_rank_ic_items<float, float>(a, b->preps[i], lrn, b->d_status, s));
+      else if (lrn)
+        FCB_BTRY(launch_rank_ic_learned(a, b->d_status, s));
+      else
+        FCB_BTRY(launch_rank_ic<float, float>(a, b->d_status, s));
     } else {
       RankIcArgs<double, double> a{};
       a.X = static_cast<const double*>(q.X);

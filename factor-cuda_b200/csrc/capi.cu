@@ -152,19 +152,6 @@ bool is_group_whitelist(cudaError_t e) {
   return e == cudaErrorInvalidConfiguration || e == cudaErrorLaunchOutOfResources;
 }
 
-// Status word the asynchronous fcb_dev_* entry points hand to kernels with
-// bounded waits (allocated once per process, written only by kernels).
-cudaError_t dev_status_sink(int** out) {
-  static int* d_status = nullptr;
-  static std::mutex mu;
-  std::lock_guard<std::mutex> g(mu);
-  if (d_status == nullptr) {
-    const cudaError_t e = cudaMalloc(&d_status, 64);
-    if (e != cudaSuccess) return e;
-  }
-  *out = d_status;
-  return cudaSuccess;
-}
 
 }  // namespace
 
@@ -198,6 +185,33 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
   return cudaMallocFromPoolAsync(p, bytes, pool, s);
 }
 cudaError_t scratch_free(void* p, cudaStream_t s) { return cudaFreeAsync(p, s); }
+
+// Status word the asynchronous fcb_dev_* entry points hand to kernels with
+// bounded waits: one per device, allocated and zeroed on the first call made
+// with that device current; kernels only ever set it, fcb_dev_status reads and
+// clears it.
+cudaError_t dev_status_sink(int** out) {
+  static std::mutex mu;
+  static int* sinks[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(mu);
+  if (sinks[dev] == nullptr) {
+    int* p = nullptr;
+    e = cudaMalloc(&p, 64);
+    if (e != cudaSuccess) return e;
+    e = cudaMemset(p, 0, 64);
+    if (e != cudaSuccess) {
+      cudaFree(p);
+      return e;
+    }
+    sinks[dev] = p;
+  }
+  *out = sinks[dev];
+  return cudaSuccess;
+}
 }  // namespace fcb
 
 extern "C" fcb_workspace* fcb_workspace_create(void) { return new (std::nothrow) fcb_workspace(); }
@@ -226,6 +240,17 @@ extern "C" int fcb_workspace_learned_state(const fcb_workspace* ws, int* ready, 
   if (fits) *fits = ws->fits;
   if (learned_chunks) *learned_chunks = ws->learned_chunks;
   return FCB_OK;
+}
+
+extern "C" int fcb_dev_status(void) {
+  int* d = nullptr;
+  FCB_TRY(dev_status_sink(&d));
+  FCB_TRY(cudaDeviceSynchronize());
+  int h = 0;
+  FCB_TRY(cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h == 0) return FCB_OK;
+  FCB_TRY(cudaMemset(d, 0, sizeof(int)));
+  return FCB_ERR_DEVICE_WAIT;
 }
 
 extern "C" int fcb_version(void) { return 10000; }

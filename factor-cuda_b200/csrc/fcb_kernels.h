@@ -151,6 +151,8 @@ size_t ric_prep_bytes(int T, int N);
 // library-private memory pool per device that keeps freed blocks cached.
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s);
 cudaError_t scratch_free(void* p, cudaStream_t s);
+// Per-device status word of the asynchronous entry points (capi.cu).
+cudaError_t dev_status_sink(int** out);
 RicPrep ric_prep_carve(void* base, int T, int N);
 // Rank + IC as one CTA per (date, factor) after a per-date returns pass:
 // T * F CTAs instead of T, so the last wave of a long panel is short.

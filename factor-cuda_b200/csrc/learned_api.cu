@@ -220,8 +220,8 @@ int fcb::rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d
   if (min_valid < 2) return FCB_ERR_CAP4;
   if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
   if (N > (1 << 24)) return FCB_ERR_CAP2;
-  static int* d_status = nullptr;
-  if (d_status == nullptr) FCB_TRY(cudaMalloc(&d_status, sizeof(int)));
+  int* d_status = nullptr;
+  FCB_TRY(dev_status_sink(&d_status));
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr,
                              model->table[model->cur], model->zrange[model->cur], cap > 0 ? cap : 64, d_stats,
                              ic_ld};

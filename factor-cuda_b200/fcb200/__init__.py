@@ -35,7 +35,7 @@ except Exception:  # pragma: no cover
 __version__ = "1.0.0"
 __all__ = ["cross_sectional_rank", "factor_plane", "factor_corr", "stock_corr", "rolling_ic",
            "parameter_scan", "rank_ic_panel", "Workspace", "CdfModel", "Batch", "clear_workspaces",
-           "__version__"]
+           "check_device", "__version__"]
 
 _WHITELIST = (np.float32, np.float64)
 DOMAIN_MSG = ("correlation domain violation: max|x| > 1e150 or a nonzero |x| < 1e-150 "
@@ -200,6 +200,13 @@ def _dev_mask(mask, *, name, T, N, device, allow_none=True):
     if tuple(mask.shape) != (T, N):
         raise ValueError(f"{name} shape must be (T,N) matching input, got {tuple(mask.shape)}")
     return mask.detach().to(device).contiguous().view(_torch.uint8)
+
+
+def check_device():
+    """Synchronise the current CUDA device and raise ``RuntimeError`` if a
+    bounded device-side wait in an asynchronous call (the CUDA-tensor route)
+    gave up since the last check; the condition is cleared by the check."""
+    nat.check(nat.lib().fcb_dev_status(), "device status")
 
 
 def _stream_of(t):

@@ -170,6 +170,15 @@ int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const uint8_t* d_f
  * (cudaMallocAsync from a per-device pool) or taken from `ws` where the
  * signature has one; calls sharing a workspace must be serialised. */
 
+/* Bounded device-side waits in the asynchronous entry points (a staged copy
+ * that did not land) set a status word of the current device instead of
+ * returning a code.  fcb_dev_status synchronises the current device, returns
+ * FCB_ERR_DEVICE_WAIT (and clears the word) if any such wait gave up since the
+ * last check, else FCB_OK.  The word is allocated on a device's first
+ * asynchronous call (before any stream capture on that device).  No reference
+ * counterpart: the reference's entry points are all synchronous. */
+int fcb_dev_status(void);
+
 /* cs_rank (asynchronous). */
 int fcb_dev_cs_rank_f32(const float* d_x, const uint8_t* d_mask, int T, int N, int descending, float* d_out,
                         void* stream);

@@ -189,6 +189,17 @@ def test_device_inputs_validation(fc):
         fc.rolling_ic(dx, dx, device="cpu")
 
 
+def test_device_status_after_async_calls(fc):
+    """The asynchronous route reports bounded-wait failures through a
+    per-device status word; after ordinary calls it reads clear."""
+    x, m = _panel(20, 3000, 12)
+    dx, dm = torch.from_numpy(x).to(DEV), torch.from_numpy(m).to(DEV)
+    fc.cross_sectional_rank(dx, dm)
+    fc.rolling_ic(dx, dx * 0.5 + 1.0, dm, None)
+    fc.check_device()
+    fc.check_device()
+
+
 def test_device_inputs_follow_the_stream(fc):
     """Work is issued on the caller's current stream: a result read on that
     stream after the call sees the finished ranks without a device sync."""
