@@ -674,7 +674,35 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
   int Tc = static_cast<int>((64ull << 20) / (per_date > 0 ? per_date : 1));
   if (Tc < 1) Tc = 1;
   if (Tc > T) Tc = T;
-  const int nchunk = (T + Tc - 1) / Tc;
+  // Chunk schedule: the first upload and the last compute + download overlap
+  // nothing, so the chunks ramp up from Tc/8 at the start and back down to
+  // Tc/8 at the end (Tc/8, Tc/4, Tc/2, Tc, ..., Tc, Tc/2, Tc/4, Tc/8) when the
+  // panel is long enough; shorter panels take uniform chunks of Tc.
+  std::vector<int> chunk_t0, chunk_tc;
+  {
+    const int r1 = std::max(1, Tc / 8), r2 = std::max(1, Tc / 4), r3 = std::max(1, Tc / 2);
+    const int ramp = r1 + r2 + r3;
+    std::vector<int> sizes;
+    if (Tc >= 8 && T >= 2 * ramp + Tc) {
+      sizes = {r1, r2, r3};
+      int mid = T - 2 * ramp;
+      while (mid > 0) {
+        const int c = std::min(Tc, mid);
+        sizes.push_back(c);
+        mid -= c;
+      }
+      sizes.insert(sizes.end(), {r3, r2, r1});
+    } else {
+      for (int t = 0; t < T; t += Tc) sizes.push_back(std::min(Tc, T - t));
+    }
+    int t = 0;
+    for (int c : sizes) {
+      chunk_t0.push_back(t);
+      chunk_tc.push_back(c);
+      t += c;
+    }
+  }
+  const int nchunk = static_cast<int>(chunk_tc.size());
   // learned splitters need the shared-memory kernel; wider sections are ranked
   // by the global-memory radix path (identical results)
   const bool learned = (method == 1) && rank_ic_fits_smem<float, float>(N);
@@ -729,8 +757,8 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
   FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), s_c));
   for (int c = 0; c < nchunk; ++c) {
     const int j = c % NB;
-    const int t0 = c * Tc;
-    const int tc = (t0 + Tc <= T) ? Tc : (T - t0);
+    const int t0 = chunk_t0[c];
+    const int tc = chunk_tc[c];
     const size_t cnn = static_cast<size_t>(tc) * N;
     if (c >= NB) FCB_TRY(cudaStreamWaitEvent(s_in, ev_out[j], 0));  // buffer set j drained
     // one strided copy moves this date range of all F factor panels

@@ -126,9 +126,12 @@ def test_learned_rank_ic_bit_exact_and_beats_no_network(nat):
 def test_host_panel_learned_equals_radix(nat):
     import fcb200
     F, T, N = 6, 1500, 8000
-    # the host entry point streams date chunks of about 64 MB of factor input:
-    # 349 dates here, so 5 chunks per call and a refit after every 250 dates
-    nchunk = -(-T // max(1, (64 << 20) // (F * N * 4)))
+    # the host entry point streams date chunks of about 64 MB of factor input
+    # (Tc = 349 dates here), ramped at both ends: Tc/8, Tc/4, Tc/2, Tc, ...,
+    # Tc, Tc/2, Tc/4, Tc/8; a refit follows every 250 dates
+    Tc = min(T, max(1, (64 << 20) // (F * N * 4)))
+    ramp = max(1, Tc // 8) + max(1, Tc // 4) + max(1, Tc // 2)
+    nchunk = 6 + -(-(T - 2 * ramp) // Tc) if (Tc >= 8 and T >= 2 * ramp + Tc) else -(-T // Tc)
     assert nchunk >= 4
     X, R, fm, rm = drift_panel(F, T, N, seed=9)
     r0, ic0 = fcb200.rank_ic_panel(X, R, fm, rm, min_valid=30, method="radix")
