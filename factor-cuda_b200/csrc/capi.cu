@@ -253,6 +253,21 @@ extern "C" int fcb_dev_status(void) {
   return FCB_ERR_DEVICE_WAIT;
 }
 
+extern "C" int fcb_selftest_bounded_wait(int arrive, int max_polls) {
+  if (max_polls < 1) return FCB_ERR_ARG;
+  int* d = nullptr;
+  FCB_TRY(cudaMalloc(&d, sizeof(int)));
+  struct Free {
+    int* p;
+    ~Free() { cudaFree(p); }
+  } fr{d};
+  FCB_TRY(cudaMemset(d, 0, sizeof(int)));
+  FCB_TRY(launch_wait_probe(arrive != 0, static_cast<uint32_t>(max_polls), d, nullptr));
+  int h = 0;
+  FCB_TRY(cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost));
+  return h != 0 ? FCB_ERR_DEVICE_WAIT : FCB_OK;
+}
+
 extern "C" int fcb_version(void) { return 10000; }
 
 extern "C" int fcb_device_count(void) {

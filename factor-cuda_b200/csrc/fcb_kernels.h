@@ -153,6 +153,9 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s);
 cudaError_t scratch_free(void* p, cudaStream_t s);
 // Per-device status word of the asynchronous entry points (capi.cu).
 cudaError_t dev_status_sink(int** out);
+// One block waiting (at most max_polls polls) on a barrier that completes
+// only if `arrive`; sets *status on timeout (selftest.cu).
+cudaError_t launch_wait_probe(bool arrive, uint32_t max_polls, int* status, cudaStream_t s);
 RicPrep ric_prep_carve(void* base, int T, int N);
 // Rank + IC as one CTA per (date, factor) after a per-date returns pass:
 // T * F CTAs instead of T, so the last wave of a long panel is short.

@@ -70,6 +70,7 @@ PROTOTYPES = {
     "fcb_rank_ic_panel": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i, _p]),
     "fcb_dev_rank_ic_panel": (_i, [_p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i, _p]),
     "fcb_dev_status": (_i, []),
+    "fcb_selftest_bounded_wait": (_i, [_i, _i]),
     "fcb_dev_cs_rank_f32": (_i, [_p, _p, _i, _i, _i, _p, _p]),
     "fcb_dev_parameter_scan_f32": (_i, [_p, _p, _i, _i, C.POINTER(_p), C.POINTER(_i), C.POINTER(_i), _p]),
     "fcb_dev_rolling_ic": (_i, [_p, _i, _p, _i, _p, _p, _i, _i, _i, _p, _p, _p, _p]),

@@ -179,6 +179,13 @@ int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const uint8_t* d_f
  * counterpart: the reference's entry points are all synchronous. */
 int fcb_dev_status(void);
 
+/* Self-test of the bounded-wait path (no reference counterpart): one block
+ * waits, for at most max_polls polls, on a shared-memory barrier that is
+ * completed only when arrive != 0 (otherwise it expects a transfer that is
+ * never issued).  Returns FCB_ERR_DEVICE_WAIT when the wait ran out, FCB_OK
+ * when it completed; the device stays usable either way.  Synchronous. */
+int fcb_selftest_bounded_wait(int arrive, int max_polls);
+
 /* cs_rank (asynchronous). */
 int fcb_dev_cs_rank_f32(const float* d_x, const uint8_t* d_mask, int T, int N, int descending, float* d_out,
                         void* stream);

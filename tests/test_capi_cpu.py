@@ -93,6 +93,7 @@ def test_device_entry_contract_errors_without_device(native):
     assert lib.fcb_dev_stock_corr(P(x), 0, None, 1, 46341, P(o), None, None, None, None) == -3
     assert lib.fcb_dev_stock_corr(P(x), 0, None, 1 << 16, 1 << 16, P(o), None, None, None, None) == -2
     assert lib.fcb_dev_stock_corr(P(x), 0, None, 2, 2, P(o), None, None, None, None) == -1  # workspace required
+    assert lib.fcb_selftest_bounded_wait(0, 0) == -1   # poll limit must be positive
     ok = C.c_int(7)
     assert lib.fcb_dev_corr_domain(P(x), 0, None, 2, 2, 2, 2, C.byref(ok), None) == -1      # layout flag
     assert lib.fcb_dev_corr_domain(P(x), 3, None, 2, 2, 2, 0, C.byref(ok), None) == -1      # dtype

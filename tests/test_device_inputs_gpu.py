@@ -200,6 +200,21 @@ def test_device_status_after_async_calls(fc):
     fc.check_device()
 
 
+def test_bounded_wait_runs_out_and_reports(fc):
+    """A wait on a barrier that nothing completes ends after its poll limit
+    with FCB_ERR_DEVICE_WAIT (no hang, no fault); the context stays usable:
+    a completed wait and an ordinary call succeed right after."""
+    from fcb200 import _native as nat
+    lib = nat.lib()
+    assert lib.fcb_selftest_bounded_wait(0, 2000) == nat.FCB_ERR_DEVICE_WAIT
+    assert lib.fcb_selftest_bounded_wait(1, 2000) == 0
+    assert lib.fcb_selftest_bounded_wait(0, 0) == -1
+    x, m = _panel(5, 700, 3)
+    got = fc.cross_sectional_rank(torch.from_numpy(x).to(DEV), torch.from_numpy(m).to(DEV)).cpu().numpy()
+    assert bitwise_f32(got, O.cs_rank(x, m))
+    fc.check_device()
+
+
 def test_device_inputs_follow_the_stream(fc):
     """Work is issued on the caller's current stream: a result read on that
     stream after the call sees the finished ranks without a device sync."""
