@@ -480,36 +480,43 @@ cudaError_t launch_corr_domain(const void* X, int dtype, const uint8_t* mask, lo
 // Per-block column partials over a contiguous row range: count, Kahan sum,
 // min, max.  Rows are visited in increasing order within each thread's
 // strided slice; partials are merged in a fixed order by k_fc_colfinal.
-template <typename TIN>
+template <typename TIN, bool UNIT_ROWS>
 __global__ void k_fc_colpart(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
                              long long sr, long long sf, long long rows_per_block, FcColPart* __restrict__ part) {
   const long long r0 = blockIdx.x * rows_per_block;
   const long long r1 = min(R, r0 + rows_per_block);
   for (int f = threadIdx.y; f < F; f += blockDim.y) {
     Kahan k;
-    double cnt = 0.0, mn = kBigPos, mx = -kBigPos;
+    // count, min and max in the input's own type (exact: the values are the
+    // same after the widening); only the Kahan sum needs FP64
+    long long cnt_i = 0;
+    TIN mn_t = KeyOf<TIN>::max_finite(), mx_t = -KeyOf<TIN>::max_finite();
+    const TIN* col = X + f * sf;
     // rows visited in the same order; kU loads in flight before they are added
     constexpr int kU = 8;
     for (long long rb = r0 + threadIdx.x; rb < r1; rb += static_cast<long long>(kU) * blockDim.x) {
-      double xv[kU];
+      TIN xv[kU];
       bool ok[kU];
 #pragma unroll
       for (int u = 0; u < kU; ++u) {
         const long long r = rb + static_cast<long long>(u) * blockDim.x;
         ok[u] = r < r1;
-        xv[u] = ok[u] ? static_cast<double>(X[r * sr + f * sf]) : 0.0;
+        xv[u] = ok[u] ? col[UNIT_ROWS ? r : r * sr] : TIN(0);
         ok[u] = ok[u] && (mask == nullptr || mask[r] != 0);
       }
 #pragma unroll
       for (int u = 0; u < kU; ++u) {
-        if (ok[u] && finite_f64(xv[u])) {
-          cnt += 1.0;
-          k.add(xv[u]);
-          mn = fmin(mn, xv[u]);
-          mx = fmax(mx, xv[u]);
+        if (ok[u] && KeyOf<TIN>::finite(xv[u])) {
+          ++cnt_i;
+          k.add(static_cast<double>(xv[u]));
+          mn_t = xv[u] < mn_t ? xv[u] : mn_t;
+          mx_t = xv[u] > mx_t ? xv[u] : mx_t;
         }
       }
     }
+    double cnt = static_cast<double>(cnt_i);
+    double mn = cnt_i > 0 ? static_cast<double>(mn_t) : kBigPos;
+    double mx = cnt_i > 0 ? static_cast<double>(mx_t) : -kBigPos;
     // fixed-order warp merge (lanes are threadIdx.x within one warp row)
     for (int o = 1; o < 32; o <<= 1) {
       const double os = __shfl_down_sync(kFull, k.s, o), oc = __shfl_down_sync(kFull, k.c, o);
@@ -1219,12 +1226,19 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
   const long long rpb_cols = (R + w.nblk_cols - 1) / w.nblk_cols;
   const long long rpb_gram = (R + w.nblk_gram - 1) / w.nblk_gram;
   dim3 cb(32, 8);
-  if (dtype == 0)
-    k_fc_colpart<float><<<w.nblk_cols, cb, 0, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, rpb_cols,
-                                                   w.colpart);
+  // factor planes (rows at unit stride) take the instantiation without the row-stride product
+  if (dtype == 0 && sr == 1)
+    k_fc_colpart<float, true><<<w.nblk_cols, cb, 0, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, rpb_cols,
+                                                         w.colpart);
+  else if (dtype == 0)
+    k_fc_colpart<float, false><<<w.nblk_cols, cb, 0, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf,
+                                                          rpb_cols, w.colpart);
+  else if (sr == 1)
+    k_fc_colpart<double, true><<<w.nblk_cols, cb, 0, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf,
+                                                          rpb_cols, w.colpart);
   else
-    k_fc_colpart<double><<<w.nblk_cols, cb, 0, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf, rpb_cols,
-                                                    w.colpart);
+    k_fc_colpart<double, false><<<w.nblk_cols, cb, 0, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf,
+                                                           rpb_cols, w.colpart);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_fc_colfinal<<<(F * 32 + 127) / 128, 128, 0, s>>>(w.colpart, w.nblk_cols, F, w.colstat);

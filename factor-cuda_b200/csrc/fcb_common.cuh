@@ -47,12 +47,14 @@ template <> struct KeyOf<float> {
   using type = uint32_t;
   static FCB_DEV uint32_t key(float v) { return key_f32(v); }
   static FCB_DEV bool finite(float v) { return finite_f32(v); }
+  static FCB_DEV float max_finite() { return __FLT_MAX__; }
   static constexpr uint32_t invalid = kInvalidKey32;
 };
 template <> struct KeyOf<double> {
   using type = unsigned long long;
   static FCB_DEV unsigned long long key(double v) { return key_f64(v); }
   static FCB_DEV bool finite(double v) { return finite_f64(v); }
+  static FCB_DEV double max_finite() { return __DBL_MAX__; }
   static constexpr unsigned long long invalid = kInvalidKey64;
 };
 
