@@ -684,13 +684,29 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
   raw[0] = reinterpret_cast<TIN*>(fsm + fc_gram_raw_offset(Fp, tasks_per_block));
   raw[1] = raw[0] + chunk * Fp;
   uint8_t* smask = reinterpret_cast<uint8_t*>(raw[1] + chunk * Fp);
+  // Element e of a staged chunk is (row rr, factor f): rr = e / Fp, f = e % Fp
+  // for the (rows, F) layout, rr = e % chunk, f = e / chunk for factor planes,
+  // so that consecutive threads read consecutive elements of X either way.
+  // Each thread walks e = tid, tid + 256, ...: one division up front, then a
+  // constant step with a carry.
+  const bool planes = sf != 1;
+  const int inner = planes ? chunk : Fp;  // extent of the fast index
+  const int e0_in = threadIdx.x % inner, e0_out = threadIdx.x / inner;
+  const int step_in = 256 % inner, step_out = 256 / inner;
   auto issue = [&](long long cs, TIN* dst) {
     const int nrs = static_cast<int>(min(static_cast<long long>(chunk), r1 - cs));
+    const TIN* base = X + cs * sr;
+    int a = e0_in, b = e0_out;  // (fast, slow) index of element e
     for (int e = threadIdx.x; e < chunk * Fp; e += 256) {
-      // consecutive threads read consecutive elements of X in either layout
-      const int rr = (sf == 1) ? e / Fp : e % chunk;
-      const int f = (sf == 1) ? e % Fp : e / chunk;
-      if (rr < nrs && f < F) cp_async_elem<sizeof(TIN)>(dst + e, X + (cs + rr) * sr + f * sf);
+      const int rr = planes ? a : b;
+      const int f = planes ? b : a;
+      if (rr < nrs && f < F) cp_async_elem<sizeof(TIN)>(dst + e, base + rr * sr + f * sf);
+      a += step_in;
+      b += step_out;
+      if (a >= inner) {
+        a -= inner;
+        ++b;
+      }
     }
   };
   auto mask_of = [&](long long cs) -> uint8_t {
@@ -716,9 +732,16 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
     cp_async_wait_prev();  // this thread's copies of chunk `it` have landed
     __syncthreads();
     const TIN* rb = raw[it & 1];
+    int a = e0_in, b = e0_out;
     for (int e = threadIdx.x; e < chunk * Fp; e += 256) {
-      const int rr = (sf == 1) ? e / Fp : e % chunk;
-      const int f = (sf == 1) ? e % Fp : e / chunk;
+      const int rr = planes ? a : b;
+      const int f = planes ? b : a;
+      a += step_in;
+      b += step_out;
+      if (a >= inner) {
+        a -= inner;
+        ++b;
+      }
       const int ei = f * pitch + rr;
       double v = 0.0, mv = 0.0;
       if (rr < nr && f < F) {
