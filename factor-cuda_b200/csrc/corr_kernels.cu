@@ -1104,27 +1104,43 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass1(const TIN* __restric
 
 // Per flagged pair: merge the pass-1 ranges in order -> (n, mean x, mean y,
 // degenerate flag) in pair[slot*4 ..]; a degenerate pair is finished here.
+// One warp per flagged pair: the lanes load up to 32 range partials at once and
+// every lane merges them in range order from shuffled copies (the same
+// sequence of operations as a single thread walking the ranges), so the
+// merged values do not depend on the warp; lane 0 writes.
 __global__ void k_fc_fb_mid(int F, int nblk, const int* __restrict__ fb_list, const int* __restrict__ fb_count,
                             const double* __restrict__ part, double* __restrict__ pair, double* __restrict__ out) {
-  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= *fb_count) return;
+  const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (slot >= *fb_count) return;  // whole warps exit together
   Kahan kx, ky;
   double n = 0.0, mnx = kBigPos, mxx = -kBigPos, mny = kBigPos, mxy = -kBigPos;
-  for (int b = 0; b < nblk; ++b) {
+  for (int b0 = 0; b0 < nblk; b0 += 32) {
+    double v[kFbP1];
+    const int b = b0 + lane;
     const double* P = part + (static_cast<size_t>(slot) * nblk + b) * kFbP1;
-    Kahan o;
-    o.s = P[1];
-    o.c = P[2];
-    kx.merge(o);
-    o.s = P[3];
-    o.c = P[4];
-    ky.merge(o);
-    n += P[0];
-    mnx = fmin(mnx, P[5]);
-    mxx = fmax(mxx, P[6]);
-    mny = fmin(mny, P[7]);
-    mxy = fmax(mxy, P[8]);
+#pragma unroll
+    for (int q = 0; q < kFbP1; ++q) v[q] = b < nblk ? P[q] : 0.0;
+    const int nb = min(32, nblk - b0);
+    for (int l = 0; l < nb; ++l) {
+      double w[kFbP1];
+#pragma unroll
+      for (int q = 0; q < kFbP1; ++q) w[q] = __shfl_sync(kFull, v[q], l);
+      Kahan o;
+      o.s = w[1];
+      o.c = w[2];
+      kx.merge(o);
+      o.s = w[3];
+      o.c = w[4];
+      ky.merge(o);
+      n += w[0];
+      mnx = fmin(mnx, w[5]);
+      mxx = fmax(mxx, w[6]);
+      mny = fmin(mny, w[7]);
+      mxy = fmax(mxy, w[8]);
+    }
   }
+  if (lane != 0) return;
   const bool degenerate = (n < 2.0 || mnx == mxx || mny == mxy);
   double* Q = pair + static_cast<size_t>(slot) * 4;
   Q[0] = n;
@@ -1192,26 +1208,39 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass2(const TIN* __restric
   }
 }
 
+// Pass-2 partials merged per flagged pair, one warp per pair as in k_fc_fb_mid.
 __global__ void k_fc_fb_final(int F, int nblk, const int* __restrict__ fb_list, const int* __restrict__ fb_count,
                               const double* __restrict__ pair, const double* __restrict__ part,
                               double* __restrict__ out) {
-  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= *fb_count) return;
+  const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (slot >= *fb_count) return;  // whole warps exit together
   if (pair[static_cast<size_t>(slot) * 4 + 3] != 0.0) return;
   Kahan a, b, c;
-  for (int k = 0; k < nblk; ++k) {
+  for (int k0 = 0; k0 < nblk; k0 += 32) {
+    double v[kFbP2];
+    const int k = k0 + lane;
     const double* P = part + (static_cast<size_t>(slot) * nblk + k) * kFbP2;
-    Kahan o;
-    o.s = P[0];
-    o.c = P[1];
-    a.merge(o);
-    o.s = P[2];
-    o.c = P[3];
-    b.merge(o);
-    o.s = P[4];
-    o.c = P[5];
-    c.merge(o);
+#pragma unroll
+    for (int q = 0; q < kFbP2; ++q) v[q] = k < nblk ? P[q] : 0.0;
+    const int nk = min(32, nblk - k0);
+    for (int l = 0; l < nk; ++l) {
+      double w[kFbP2];
+#pragma unroll
+      for (int q = 0; q < kFbP2; ++q) w[q] = __shfl_sync(kFull, v[q], l);
+      Kahan o;
+      o.s = w[0];
+      o.c = w[1];
+      a.merge(o);
+      o.s = w[2];
+      o.c = w[3];
+      b.merge(o);
+      o.s = w[4];
+      o.c = w[5];
+      c.merge(o);
+    }
   }
+  if (lane != 0) return;
   const int e = fb_list[slot];
   const int i = e / F, j = e % F;
   const double r = safe_pearson(c.s - c.c, a.s - a.c, b.s - b.c);
@@ -1300,7 +1329,7 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
       k_fc_fb_pass1<double><<<g, kFbThreads, 0, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf, nblk,
                                                       w.fb_list, w.fb_count, w.fb_part);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_fc_fb_mid<<<(maxpairs + 127) / 128, 128, 0, s>>>(F, nblk, w.fb_list, w.fb_count, w.fb_part, pair, out);
+    k_fc_fb_mid<<<(maxpairs * 32 + 127) / 128, 128, 0, s>>>(F, nblk, w.fb_list, w.fb_count, w.fb_part, pair, out);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (dtype == 0)
       k_fc_fb_pass2<float><<<g, kFbThreads, 0, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, nblk,
@@ -1309,7 +1338,7 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
       k_fc_fb_pass2<double><<<g, kFbThreads, 0, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf, nblk,
                                                       w.fb_list, w.fb_count, pair, w.fb_part);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_fc_fb_final<<<(maxpairs + 127) / 128, 128, 0, s>>>(F, nblk, w.fb_list, w.fb_count, pair, w.fb_part, out);
+    k_fc_fb_final<<<(maxpairs * 32 + 127) / 128, 128, 0, s>>>(F, nblk, w.fb_list, w.fb_count, pair, w.fb_part, out);
     return cudaGetLastError();
   }
   if (dtype == 0)
