@@ -70,6 +70,7 @@ struct fcb_batch {
   int* d_ctr = nullptr;            // queue heads [kClasses]
   // per-panel arm (f32): each panel's prepared returns for the per-(date,
   // factor) path that the single-panel entry points take with F >= 2
+  // (allocated by the first fcb_batch_run_per_panel)
   void* d_prep_mem = nullptr;
   std::vector<RicPrep> preps;
   int* d_status = nullptr;
@@ -439,20 +440,6 @@ extern "C" int fcb_batch_create(const fcb_panel* panels, int npanels, int dtype_
     c8 += 256;
     w.fb_part = reinterpret_cast<double*>(c8);
   }
-  if (dtype_x == FCB_DTYPE_F32) {
-    // prepared returns for the per-panel arm (ric_prep_bytes per panel, 256-byte aligned)
-    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    size_t total = 0;
-    for (int i = 0; i < npanels; ++i) total += al(ric_prep_bytes(panels[i].T, panels[i].N));
-    e = cudaMalloc(&b->d_prep_mem, total);
-    if (e != cudaSuccess) return fail(rcode(e));
-    b->preps.resize(npanels);
-    uint8_t* c8 = static_cast<uint8_t*>(b->d_prep_mem);
-    for (int i = 0; i < npanels; ++i) {
-      b->preps[i] = ric_prep_carve(c8, panels[i].T, panels[i].N);
-      c8 += al(ric_prep_bytes(panels[i].T, panels[i].N));
-    }
-  }
   const int r = (dtype_x == FCB_DTYPE_F32) ? upload_args<float, float>(*b) : upload_args<double, double>(*b);
   if (r != FCB_OK) return fail(r);
   *out = b;
@@ -490,6 +477,20 @@ extern "C" int fcb_batch_run_per_panel(fcb_batch* b, void* stream) {
   if (b == nullptr) return FCB_ERR_ARG;
   int r = bind_device(*b);
   if (r != FCB_OK) return r;
+  if (b->dtx == FCB_DTYPE_F32 && b->d_prep_mem == nullptr) {
+    // prepared returns for the per-(date, factor) path, allocated on the first
+    // per-panel run (ric_prep_bytes per panel, 256-byte aligned)
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    size_t total = 0;
+    for (const fcb_panel& q : b->p) total += al(ric_prep_bytes(q.T, q.N));
+    FCB_BTRY(cudaMalloc(&b->d_prep_mem, total));
+    b->preps.resize(b->p.size());
+    uint8_t* c8 = static_cast<uint8_t*>(b->d_prep_mem);
+    for (size_t i = 0; i < b->p.size(); ++i) {
+      b->preps[i] = ric_prep_carve(c8, b->p[i].T, b->p[i].N);
+      c8 += al(ric_prep_bytes(b->p[i].T, b->p[i].N));
+    }
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   for (size_t i = 0; i < b->p.size(); ++i) {
     const fcb_panel& q = b->p[i];
