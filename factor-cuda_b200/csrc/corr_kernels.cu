@@ -321,49 +321,77 @@ __global__ void __launch_bounds__(256, 2)
   (void)full;
 }
 
-// Two-pass Pearson of one pair over its joint valid rows, serial in row
-// order (exact replica of the Kahan-mean two-pass reference).
-FCB_DEV double two_pass_serial(const double* xi, const double* mi, const double* xj, const double* mj, int T,
-                               size_t stride_x, size_t stride_m) {
+// Two-pass Pearson of one pair over its joint valid dates, serial in date
+// order (the Kahan-mean two-pass reference's exact sequence of operations).
+// One thread per pair: the dates are read kU at a time, all loads issued
+// before they are used, so each step does not wait on its own loads; the
+// values are then consumed in date order.
+template <int kU>
+FCB_DEV double two_pass_serial(const double* __restrict__ xi, const double* __restrict__ mi,
+                               const double* __restrict__ xj, const double* __restrict__ mj, int T) {
   double n = 0.0, mnx = kBigPos, mxx = -kBigPos, mny = kBigPos, mxy = -kBigPos;
   Kahan kx, ky;
-  for (int t = 0; t < T; ++t) {
-    if (mi[t * stride_m] != 0.0 && mj[t * stride_m] != 0.0) {
-      const double x = xi[t * stride_x], y = xj[t * stride_x];
-      n += 1.0;
-      kx.add(x);
-      ky.add(y);
-      mnx = fmin(mnx, x);
-      mxx = fmax(mxx, x);
-      mny = fmin(mny, y);
-      mxy = fmax(mxy, y);
+  for (int t0 = 0; t0 < T; t0 += kU) {
+    double a[kU], b[kU], x[kU], y[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int t = t0 + u;
+      const bool in = t < T;
+      a[u] = in ? mi[t] : 0.0;
+      b[u] = in ? mj[t] : 0.0;
+      x[u] = in ? xi[t] : 0.0;
+      y[u] = in ? xj[t] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      if (a[u] != 0.0 && b[u] != 0.0) {
+        n += 1.0;
+        kx.add(x[u]);
+        ky.add(y[u]);
+        mnx = fmin(mnx, x[u]);
+        mxx = fmax(mxx, x[u]);
+        mny = fmin(mny, y[u]);
+        mxy = fmax(mxy, y[u]);
+      }
     }
   }
   if (n < 2.0) return dnan();
   if (mnx == mxx || mny == mxy) return dnan();
   const double mx = kx.s / n, my = ky.s / n;
-  double sxx, syy, sxy;
-  if (T > kTwoPassKahanT) {
-    Kahan a, b, c;
-    for (int t = 0; t < T; ++t)
-      if (mi[t * stride_m] != 0.0 && mj[t * stride_m] != 0.0) {
-        const double dx = xi[t * stride_x] - mx, dy = xj[t * stride_x] - my;
-        a.add(dx * dx);
-        b.add(dy * dy);
-        c.add(dx * dy);
+  const bool kahan = T > kTwoPassKahanT;
+  Kahan ka, kb, kc;
+  double sxx = 0.0, syy = 0.0, sxy = 0.0;
+  for (int t0 = 0; t0 < T; t0 += kU) {
+    double a[kU], b[kU], x[kU], y[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int t = t0 + u;
+      const bool in = t < T;
+      a[u] = in ? mi[t] : 0.0;
+      b[u] = in ? mj[t] : 0.0;
+      x[u] = in ? xi[t] : 0.0;
+      y[u] = in ? xj[t] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      if (a[u] != 0.0 && b[u] != 0.0) {
+        const double dx = x[u] - mx, dy = y[u] - my;
+        if (kahan) {
+          ka.add(dx * dx);
+          kb.add(dy * dy);
+          kc.add(dx * dy);
+        } else {
+          sxx += dx * dx;
+          syy += dy * dy;
+          sxy += dx * dy;
+        }
       }
-    sxx = a.s - a.c;
-    syy = b.s - b.c;
-    sxy = c.s - c.c;
-  } else {
-    sxx = syy = sxy = 0.0;
-    for (int t = 0; t < T; ++t)
-      if (mi[t * stride_m] != 0.0 && mj[t * stride_m] != 0.0) {
-        const double dx = xi[t * stride_x] - mx, dy = xj[t * stride_x] - my;
-        sxx += dx * dx;
-        syy += dy * dy;
-        sxy += dx * dy;
-      }
+    }
+  }
+  if (kahan) {
+    sxx = ka.s - ka.c;
+    syy = kb.s - kb.c;
+    sxy = kc.s - kc.c;
   }
   return safe_pearson(sxy, sxx, syy);
 }
@@ -375,8 +403,8 @@ __global__ void k_sc_fallback(const double* __restrict__ Xraw, const double* __r
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
     const int cell = fb_list[k];
     const int i = cell / N, j = cell % N;
-    const double r = two_pass_serial(Xraw + static_cast<size_t>(i) * Tp, Mc + static_cast<size_t>(i) * Tp,
-                                     Xraw + static_cast<size_t>(j) * Tp, Mc + static_cast<size_t>(j) * Tp, T, 1, 1);
+    const double r = two_pass_serial<8>(Xraw + static_cast<size_t>(i) * Tp, Mc + static_cast<size_t>(i) * Tp,
+                                        Xraw + static_cast<size_t>(j) * Tp, Mc + static_cast<size_t>(j) * Tp, T);
     out[static_cast<size_t>(i) * N + j] = r;
     out[static_cast<size_t>(j) * N + i] = r;
   }
