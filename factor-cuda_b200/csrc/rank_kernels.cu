@@ -632,15 +632,15 @@ __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT))
   block_radix_sort<NT, MAXIPT, KR>(kr0, i0, kr1, i1, mr, sm + L.scratch, &krs, &irs);
   uint16_t* gir = rp.ir + static_cast<size_t>(t) * rp.ld_ir;
   for (int p = threadIdx.x; p < mr; p += NT) gir[p] = irs[p];
+  // tie-start bits, one word per warp step: lane k tests sorted position
+  // w * 32 + k (consecutive keys across the lanes, no bank conflicts)
   uint32_t* gtie = rp.tie + static_cast<size_t>(t) * rp.ld_tie;
   const int nw = (N + 31) / 32;
-  for (int w = threadIdx.x; w < nw; w += NT) {
-    uint32_t bitsw = 0u;
-    for (int k = 0; k < 32; ++k) {
-      const int p = w * 32 + k;
-      if (p < mr && (p == 0 || krs[p] != krs[p - 1])) bitsw |= 1u << k;
-    }
-    gtie[w] = bitsw;
+  for (int w = static_cast<int>(threadIdx.x >> 5); w < nw; w += NT / 32) {  // uniform per warp
+    const int p = w * 32 + static_cast<int>(threadIdx.x & 31);
+    const bool start = p < mr && (p == 0 || krs[p] != krs[p - 1]);
+    const uint32_t bitsw = __ballot_sync(kFull, start);
+    if ((threadIdx.x & 31) == 0) gtie[w] = bitsw;
   }
   if (threadIdx.x == 0) rp.mr[t] = mr;
 }
