@@ -482,13 +482,13 @@ extern "C" int fcb_batch_run_per_panel(fcb_batch* b, void* stream) {
     // per-panel run (ric_prep_bytes per panel, 256-byte aligned)
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     size_t total = 0;
-    for (const fcb_panel& q : b->p) total += al(ric_prep_bytes(q.T, q.N));
+    for (const fcb_panel& q : b->p) total += al(ric_prep_bytes(q.T, q.N, q.F));
     FCB_BTRY(cudaMalloc(&b->d_prep_mem, total));
     b->preps.resize(b->p.size());
     uint8_t* c8 = static_cast<uint8_t*>(b->d_prep_mem);
     for (size_t i = 0; i < b->p.size(); ++i) {
-      b->preps[i] = ric_prep_carve(c8, b->p[i].T, b->p[i].N);
-      c8 += al(ric_prep_bytes(b->p[i].T, b->p[i].N));
+      b->preps[i] = ric_prep_carve(c8, b->p[i].T, b->p[i].N, b->p[i].F);
+      c8 += al(ric_prep_bytes(b->p[i].T, b->p[i].N, b->p[i].F));
     }
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -514,8 +514,8 @@ extern "C" int fcb_batch_run_per_panel(fcb_batch* b, void* stream) {
       }
       // as the single-panel entry points: several factors go through the
       // prepared returns and per-(date, factor) items, one factor per date
-      if (a.F >= 2)
-        FCB_BTRY(launch_rank_ic_items<float, float>(a, b->preps[i], lrn, b->d_status, s));
+      if (a.F >= 2 && ric_items_fit(a.N))
+        FCB_BTRY(launch_rank_ic_items(a, b->preps[i], lrn, s));
       else if (lrn)
         FCB_BTRY(launch_rank_ic_learned(a, b->d_status, s));
       else

@@ -28,7 +28,7 @@ enum Slot : int {
   S_SC_RAW, S_SC_C, S_SC_M, S_SC_ST, S_SC_SUM, S_FB_LIST, S_FB_CNT,
   S_FC_COLPART, S_FC_COLSTAT, S_FC_GRAM, S_FC_FLAGS, S_FC_FBPART,
   S_PC_MU, S_PC_XH, S_PC_XM, S_PC_XL, S_PC_QH, S_PC_QM, S_PC_QL, S_PC_M16, S_PC_X32, S_PC_Q32, S_PC_M32, S_PC_TILES, S_PC_X, S_PC_MASK,
-  S_PC_OUT, S_PC_CPART, S_GSCR, S_RICPREP,
+  S_PC_OUT, S_PC_CPART, S_GSCR, S_RICPREP, S_FCT_WORK,
   // streamed panel: three chunk buffers each (upload / compute / download in flight)
   S_PX0, S_PX1, S_PX2, S_PR0, S_PR1, S_PR2, S_PFM0, S_PFM1, S_PFM2, S_PRM0, S_PRM1, S_PRM2,
   S_PRK0, S_PRK1, S_PRK2, S_PIC,
@@ -496,11 +496,11 @@ template <typename TF, typename TR>
 static int run_rank_ic(const RankIcArgs<TF, TR>& a, int* dst, cudaStream_t s, fcb_workspace& ws) {
   if (rank_ic_fits_smem<TF, TR>(a.N)) {
     if constexpr (std::is_same<TF, float>::value && std::is_same<TR, float>::value) {
-      if (a.F >= 2) {
+      if (a.F >= 2 && ric_items_fit(a.N) && a.rank_f_out == nullptr) {
         // several factors: returns prepared once per date, one CTA per (date, factor)
         void* prep;
-        FCB_TRY(ws.get(S_RICPREP, ric_prep_bytes(a.T, a.N), &prep));
-        return rc(launch_rank_ic_items<TF, TR>(a, ric_prep_carve(prep, a.T, a.N), false, dst, s));
+        FCB_TRY(ws.get(S_RICPREP, ric_prep_bytes(a.T, a.N, a.F), &prep));
+        return rc(launch_rank_ic_items(a, ric_prep_carve(prep, a.T, a.N, a.F), false, s));
       }
     }
     return rc(launch_rank_ic<TF, TR>(a, dst, s));
@@ -643,11 +643,11 @@ extern "C" int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const u
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (rank_ic_fits_smem<float, float>(N)) {
-    if (F < 2) return rc(launch_rank_ic<float, float>(a, d_status, s));
+    if (F < 2 || !ric_items_fit(N)) return rc(launch_rank_ic<float, float>(a, d_status, s));
     // several factors: returns prepared once per date, one CTA per (date, factor)
     void* prep = nullptr;
-    FCB_TRY(scratch_alloc(&prep, ric_prep_bytes(T, N), s));
-    const cudaError_t e = launch_rank_ic_items<float, float>(a, ric_prep_carve(prep, T, N), false, d_status, s);
+    FCB_TRY(scratch_alloc(&prep, ric_prep_bytes(T, N, F), s));
+    const cudaError_t e = launch_rank_ic_items(a, ric_prep_carve(prep, T, N, F), false, s);
     FCB_TRY(scratch_free(prep, s));
     return rc(e);
   }
@@ -999,6 +999,60 @@ extern "C" int fcb_factor_corr(const void* x, int dtype, const uint8_t* mask, in
     FCB_TRY(cudaMemcpyAsync(fallback_out, dflags, static_cast<size_t>(F) * F, cudaMemcpyDeviceToHost, s));
   FCB_TRY(cudaStreamSynchronize(s));
   return FCB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// factor_corr precision form (BF16x3 tensor cores, FP64 finalize)
+// ---------------------------------------------------------------------------
+extern "C" int fcb_dev_factor_corr_bf16x3(const float* d_x, const uint8_t* d_mask, int T, int N, int F, int planes,
+                                          double* d_out, fcb_workspace* wsp, void* stream) {
+  if (d_x == nullptr || d_out == nullptr || T < 1 || N < 1 || F < 1) return FCB_ERR_ARG;
+  if (planes != 0 && planes != 1) return FCB_ERR_ARG;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP2;
+  if (F > 128) return FCB_ERR_CAP3;
+  if (F > kFcTcMaxF) return FCB_ERR_UNSUPPORTED;
+  if (wsp == nullptr) return FCB_ERR_ARG;  // scratch comes from a caller-held workspace
+  fcb_workspace& ws = *wsp;
+  FCB_TRY(ws.bind());
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const long long R = static_cast<long long>(T) * N;
+  void* work;
+  int* d_status;
+  FCB_TRY(ws.get(S_FCT_WORK, fc_tc_work_bytes(F), &work));
+  FCB_TRY(dev_status_sink(&d_status));
+  return rc(launch_factor_corr_bf16x3(d_x, d_mask, R, F, planes ? 1 : F, planes ? R : 1, work, d_out, d_status, s));
+}
+
+extern "C" int fcb_factor_corr_bf16x3(const float* x, const uint8_t* mask, int T, int N, int F, double* out,
+                                      fcb_workspace* wsp) {
+  if (x == nullptr || out == nullptr || T < 1 || N < 1 || F < 1) return FCB_ERR_ARG;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP2;
+  if (F > 128) return FCB_ERR_CAP3;
+  if (F > kFcTcMaxF) return FCB_ERR_UNSUPPORTED;
+  WsScope sc(wsp);
+  fcb_workspace& ws = *sc.ws;
+  FCB_TRY(ws.bind());
+  cudaStream_t s = ws.stream[0];
+  const long long R = static_cast<long long>(T) * N;
+  float* dx;
+  uint8_t* dm = nullptr;
+  double* dout;
+  void* work;
+  int* dst;
+  FCB_TRY(ws.get(S_X, static_cast<size_t>(R) * F * 4, &dx));
+  if (mask) FCB_TRY(ws.get(S_MASK, static_cast<size_t>(R), &dm));
+  FCB_TRY(ws.get(S_OUT, static_cast<size_t>(F) * F * 8, &dout));
+  FCB_TRY(ws.get(S_FCT_WORK, fc_tc_work_bytes(F), &work));
+  FCB_TRY(ws.get(S_STATUS, 64, &dst));
+  FCB_TRY(cudaMemsetAsync(dst, 0, sizeof(int), s));
+  FCB_TRY(cudaMemcpyAsync(dx, x, static_cast<size_t>(R) * F * 4, cudaMemcpyHostToDevice, s));
+  if (mask) FCB_TRY(cudaMemcpyAsync(dm, mask, static_cast<size_t>(R), cudaMemcpyHostToDevice, s));
+  FCB_TRY(launch_factor_corr_bf16x3(dx, dm, R, F, F, 1, work, dout, dst, s));
+  FCB_TRY(cudaMemcpyAsync(out, dout, static_cast<size_t>(F) * F * 8, cudaMemcpyDeviceToHost, s));
+  int hst = 0;
+  FCB_TRY(cudaMemcpyAsync(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FCB_TRY(cudaStreamSynchronize(s));
+  return check_status(&hst);
 }
 
 // ---------------------------------------------------------------------------

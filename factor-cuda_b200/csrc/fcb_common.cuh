@@ -58,6 +58,21 @@ template <> struct KeyOf<double> {
   static constexpr unsigned long long invalid = kInvalidKey64;
 };
 
+// Spearman IC from exact integer sums.  The joint-set ranks of both sides are
+// permutations of 1..m, so sum r = m(m+1)/2 and sum r^2 = m(m+1)(2m+1)/6 and
+// only S = sum r_f r_r depends on the data: 4 sxy = 4S - m(m+1)^2 and
+// 4 sxx = 4 syy = m(m^2-1)/3 are exact integers.  The reference's two-pass
+// f64 Pearson on integer ranks is exact before the same finalize
+// (sxy/sqrt(sxx))/sqrt(syy) (src/rolling_ic.cu:232-304), so the results are
+// bit-identical.
+FCB_DEV double spearman_from_sum(long long m, long long sum_rr) {
+  const long long s4 = 4 * sum_rr - m * (m + 1) * (m + 1);  // 4*sxy
+  const long long q4 = m * (m * m - 1) / 3;                // 4*sxx == 4*syy
+  const double sxy = static_cast<double>(s4) * 0.25;
+  const double sxx = static_cast<double>(q4) * 0.25;
+  return (sxy / sqrt(sxx)) / sqrt(sxx);
+}
+
 FCB_DEV unsigned lane_id() { return threadIdx.x & 31u; }
 FCB_DEV unsigned lanemask_lt() {
   unsigned m;

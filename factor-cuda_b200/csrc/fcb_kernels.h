@@ -138,15 +138,26 @@ size_t fc_gram_smem(int Fp, int tasks_per_block, int elem_bytes);
 cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
                                double* out, uint8_t* flags, cudaStream_t s);
 // Returns of each date prepared once for the per-(date, factor) rank + IC
-// kernel (rows 16-byte aligned; see k_ric_returns).
+// kernels (rank_ic_bucket.cu).  word[t*ld + i]: bits 0-13 the position of
+// stock i in the stable ascending order of the date's valid returns, bits
+// 14-27 the position where its tie group starts, bit 28 returns valid, bit 29
+// factor mask (N <= 16384; rows 16-byte aligned).  fb_count / fb_items: the
+// sections (t*F + f) the learned kernel hands to the radix kernel.
 struct RicPrep {
-  uint16_t* ir;    // (T, ld_ir) column ids of valid returns in key order
-  uint32_t* tie;   // (T, ld_tie) tie-group start bits over the sorted order
-  uint8_t* flags;  // (T, ld_fl) bit 0 returns valid, bit 1 factor mask
-  int* mr;         // (T) valid returns per date
-  int ld_ir, ld_tie, ld_fl;
+  uint32_t* word;
+  int* fb_count;
+  int* fb_items;
+  int ld;
 };
-size_t ric_prep_bytes(int T, int N);
+size_t ric_prep_bytes(int T, int N, int F);
+RicPrep ric_prep_carve(void* base, int T, int N, int F);
+// True when the per-(date, factor) kernels take N (f32 factors and returns).
+bool ric_items_fit(int N);
+// Rank + IC of F >= 1 f32 factor panels against one f32 returns panel: the
+// returns pass, then one CTA per (date, factor) -- learned splitters (with the
+// radix kernel taking the sections they hand back) or radix.  Requires
+// rank_f_out == rank_r_out == nullptr.
+cudaError_t launch_rank_ic_items(const RankIcArgs<float, float>& a, RicPrep rp, bool learned, cudaStream_t st);
 // Stream-ordered scratch for the entry points that take no workspace: a
 // library-private memory pool per device that keeps freed blocks cached.
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s);
@@ -156,13 +167,6 @@ cudaError_t dev_status_sink(int** out);
 // One block waiting (at most max_polls polls) on a barrier that completes
 // only if `arrive`; sets *status on timeout (selftest.cu).
 cudaError_t launch_wait_probe(bool arrive, uint32_t max_polls, int* status, cudaStream_t s);
-RicPrep ric_prep_carve(void* base, int T, int N);
-// Rank + IC as one CTA per (date, factor) after a per-date returns pass:
-// T * F CTAs instead of T, so the last wave of a long panel is short.
-template <typename TF, typename TR>
-cudaError_t launch_rank_ic_items(const RankIcArgs<TF, TR>& a, RicPrep rp, bool learned, int* status,
-                                 cudaStream_t st);
-
 // Global-memory rank path for cross-sections the shared-memory kernels cannot
 // hold (rank_global.cu).  kind 0 cs_rank, 1 parameter_scan, 2 rank+IC: bytes
 // of scratch one date needs; the launchers process dates in chunks that fit
@@ -194,6 +198,13 @@ template <typename TF, typename TR>
 cudaError_t launch_rank_ic_batch(int nt, bool learned, const RankIcArgs<TF, TR>* panels, const int2* items,
                                  int nitems, int* counter, int grid, size_t smem, int* status, cudaStream_t st,
                                  int* occ);
+// factor_corr precision form (fc_tc.cu): BF16x3 tcgen05 moment products over
+// the R pooled rows, split over one CTA per SM, FP64 finalize.  F <= kFcTcMaxF;
+// element (r, f) at X[r*sr + f*sf]; work: fc_tc_work_bytes(F) bytes.
+constexpr int kFcTcMaxF = 16;
+size_t fc_tc_work_bytes(int F);
+cudaError_t launch_factor_corr_bf16x3(const float* X, const uint8_t* mask, long long R, int F, long long sr,
+                                      long long sf, void* work, double* out, int* status, cudaStream_t s);
 // Same with element (r, f) at X[r*sr + f*sf].
 cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* mask, long long R, int F,
                                        long long sr, long long sf, FcWork& w, double* out, uint8_t* flags,

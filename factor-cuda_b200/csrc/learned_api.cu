@@ -155,6 +155,33 @@ extern "C" int fcb_cdf_model_fit(fcb_cdf_model* m, const float* d_x, const float
   return FCB_OK;
 }
 
+// Refits that overlap ranking: the samples are drawn on the ranking stream
+// (they read the ranks just produced), the training and the tabulation run on
+// another stream into the idle table slot, and the caller makes that slot
+// current (fcb_cdf_model_swap) once the training stream has passed it.
+extern "C" int fcb_cdf_model_sample(fcb_cdf_model* m, const float* d_x, const float* d_ranks, int T, int N, int t0,
+                                    int tcount, void* stream) {
+  if (m == nullptr || d_x == nullptr || d_ranks == nullptr || T < 1 || N < 1 || tcount < 1 || t0 < 0 ||
+      t0 + tcount > T)
+    return FCB_ERR_ARG;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
+  FCB_TRY(fcb::cdf_model_features(m, d_x, d_ranks, T, N, t0, tcount, static_cast<cudaStream_t>(stream)));
+  return FCB_OK;
+}
+
+extern "C" int fcb_cdf_model_train(fcb_cdf_model* m, int steps, float lr, int into_idle, void* stream) {
+  if (m == nullptr || steps < 0 || !(lr > 0.0f) || m->nsamp < 1) return FCB_ERR_ARG;
+  FCB_TRY(fcb::cdf_model_train_tabulate(m, steps, lr, into_idle ? (m->cur ^ 1) : m->cur,
+                                        static_cast<cudaStream_t>(stream)));
+  return FCB_OK;
+}
+
+extern "C" int fcb_cdf_model_swap(fcb_cdf_model* m) {
+  if (m == nullptr) return FCB_ERR_ARG;
+  m->cur ^= 1;
+  return FCB_OK;
+}
+
 extern "C" int fcb_cdf_model_state(const fcb_cdf_model* m, float* params, float* zrange, float* table, float* loss) {
   if (m == nullptr) return FCB_ERR_ARG;
   const size_t P = kCdfParams;
@@ -226,11 +253,11 @@ int fcb::rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d
                              model->table[model->cur], model->zrange[model->cur], cap > 0 ? cap : 64, d_stats,
                              ic_ld};
   if (rank_ic_fits_smem<float, float>(N)) {
-    if (F < 2) return rc(launch_rank_ic_learned(a, d_status, stream));
+    if (F < 2 || !ric_items_fit(N)) return rc(launch_rank_ic_learned(a, d_status, stream));
     // several factors: returns prepared once per date, one CTA per (date, factor)
     void* prep = nullptr;
-    FCB_TRY(scratch_alloc(&prep, ric_prep_bytes(T, N), stream));
-    const cudaError_t e = launch_rank_ic_items<float, float>(a, ric_prep_carve(prep, T, N), true, d_status, stream);
+    FCB_TRY(scratch_alloc(&prep, ric_prep_bytes(T, N, F), stream));
+    const cudaError_t e = launch_rank_ic_items(a, ric_prep_carve(prep, T, N, F), true, stream);
     FCB_TRY(scratch_free(prep, stream));
     return rc(e);
   }

@@ -95,9 +95,16 @@ void check_rc(int rc, const char* fn) {
                            fcb_status_string(rc) + ")");
 }
 
-fcb_workspace* ws_ptr(py::object w) {
+// The workspace argument must be the handle class the function is bound to
+// (CsRankWorkspace for cs_rank / parameter_scan, RollingIcWorkspace for
+// rolling_ic); any other object raises TypeError, as a typed pybind11
+// parameter would.
+template <typename W>
+fcb_workspace* ws_ptr(py::object w, const char* expected) {
   if (w.is_none()) return nullptr;
-  return py::cast<Workspace&>(w).ws;
+  if (!py::isinstance<W>(w))
+    throw py::type_error(std::string("workspace must be a ") + expected + " or None");
+  return py::cast<W&>(w).ws;
 }
 
 void check_2d(const py::array& a, const char* name, py::ssize_t& T, py::ssize_t& N) {
@@ -116,7 +123,7 @@ py::array_t<float> cs_rank_f32(py::object X, py::object mask, bool descending, p
   if (static_cast<int64_t>(T) * N > INT32_MAX) throw std::invalid_argument("T*N exceeds INT32_MAX (implementation cap)");
   ArrU8 mh;
   const uint8_t* mp = mask_or_null(mask, "mask", T, N, mh);
-  fcb_workspace* ws = ws_ptr(workspace);
+  fcb_workspace* ws = ws_ptr<CsRankWorkspace>(workspace, "CsRankWorkspace");
   py::array_t<float> out({T, N});
   float* op = out.mutable_data();
   const float* xp = xa.data();
@@ -144,7 +151,7 @@ py::object rolling_ic_f64(py::object F, py::object R, py::object fmask, py::obje
   ArrU8 fh, rh;
   const uint8_t* fmp = mask_or_null(fmask, "fmask", T, N, fh);
   const uint8_t* rmp = mask_or_null(rmask, "rmask", T, N, rh);
-  fcb_workspace* ws = ws_ptr(workspace);
+  fcb_workspace* ws = ws_ptr<RollingIcWorkspace>(workspace, "RollingIcWorkspace");
   py::array_t<double> ic({T});
   py::array_t<double> rf, rr;
   double *rfp = nullptr, *rrp = nullptr;
@@ -230,7 +237,7 @@ py::dict parameter_scan_f32(py::object X, py::object mask, bool return_timing, p
   }
   if (static_cast<size_t>(nact) * static_cast<size_t>(total) * sizeof(float) > (4ull << 30))
     throw std::invalid_argument("active*T*N*4 bytes exceeds the host output budget");
-  fcb_workspace* ws = ws_ptr(workspace);
+  fcb_workspace* ws = ws_ptr<CsRankWorkspace>(workspace, "CsRankWorkspace");
   py::array_t<float> outs[4];
   float* op[4] = {nullptr, nullptr, nullptr, nullptr};
   for (int g = 0; g < 4; ++g)

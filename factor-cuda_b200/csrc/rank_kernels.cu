@@ -341,15 +341,6 @@ struct RankIcLayout {
   }
 };
 
-// IC from the exact integer sums (see k_rank_ic header comment).
-FCB_DEV double spearman_from_sum(long long m, long long sum_rr) {
-  const long long s4 = 4 * sum_rr - m * (m + 1) * (m + 1);  // 4*sxy
-  const long long q4 = m * (m * m - 1) / 3;                // 4*sxx == 4*syy
-  const double sxy = static_cast<double>(s4) * 0.25;
-  const double sxx = static_cast<double>(q4) * 0.25;
-  return (sxy / sqrt(sxx)) / sqrt(sxx);
-}
-
 // The staging barriers (five) sit at the start of every rank+IC layout.
 FCB_DEV void rank_ic_cta_init(uint8_t* sm) {
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm);
@@ -577,145 +568,6 @@ FCB_DEV bool rank_ic_date(const RankIcArgs<TF, TR>& a, const int t, uint8_t* sm,
   return true;
 }
 
-// Returns prepared once per date for the per-(date, factor) kernel: row t of
-// each array starts on a 16-byte boundary (one bulk copy per row).
-//   ir[t*ld_ir ...]    column ids of the valid returns in ascending key order
-//   tie[t*ld_tie ...]  bit p set when sorted position p starts a new key
-//   flags[t*ld_fl ...] bit 0 returns valid, bit 1 factor mask
-//   mr[t]              number of valid returns
-template <int NT, int MAXIPT, typename TR>
-__global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT))
-    k_ric_returns(const TR* __restrict__ R, const uint8_t* __restrict__ rmask, const uint8_t* __restrict__ fmask, int N,
-                  RicPrep rp, int* status) {
-  using KR = typename KeyOf<TR>::type;
-  extern __shared__ __align__(16) uint8_t sm[];
-  const RankIcLayout L(N, int(sizeof(KR)), SortScratch<NT>::bytes);
-  rank_ic_cta_init(sm);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L.bars);
-  uint32_t* scan = reinterpret_cast<uint32_t*>(sm + L.scratch + SortScratch<NT>::hist_bytes +
-                                               SortScratch<NT>::base_bytes);
-  const int t = blockIdx.x;
-  const size_t row = static_cast<size_t>(t) * N;
-  uint8_t* flags = sm + L.flags;
-  uint16_t* i0 = reinterpret_cast<uint16_t*>(sm + L.i0);
-  uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
-  uint32_t ph[3] = {0, 0, 0};
-  bool arm[3] = {false, false, false};
-  const TR* r = stage_issue(sm + L.k1, R + row, N, &bars[0], arm[0]);
-  const uint8_t* rm = nullptr;
-  const uint8_t* fm = nullptr;
-  if (rmask != nullptr) rm = stage_issue(sm + L.i1, rmask + row, N, &bars[1], arm[1]);
-  if (fmask != nullptr) fm = stage_issue(sm + L.i0, fmask + row, N, &bars[2], arm[2]);
-  bool ok = stage_wait(&bars[0], ph[0], arm[0]);
-  ok = stage_wait(&bars[1], ph[1], arm[1]) && ok;
-  ok = stage_wait(&bars[2], ph[2], arm[2]) && ok;
-  if (__syncthreads_or(!ok)) {
-    if (threadIdx.x == 0) atomicExch(status, 1);
-    return;
-  }
-  uint8_t* gflags = rp.flags + static_cast<size_t>(t) * rp.ld_fl;
-  for (int i = threadIdx.x; i < N; i += NT) {
-    const bool rv = KeyOf<TR>::finite(r[i]) && (rm == nullptr || rm[i] != 0);
-    const bool fv = (fm == nullptr) || fm[i] != 0;
-    const uint8_t v = static_cast<uint8_t>((rv ? 1u : 0u) | (fv ? 2u : 0u));
-    flags[i] = v;
-    gflags[i] = v;
-  }
-  __syncthreads();
-  KR* kr0 = reinterpret_cast<KR*>(sm + L.k0);
-  KR* kr1 = reinterpret_cast<KR*>(sm + L.k1);
-  const int mr = compact_keys<KR>(
-      N, [&](int i) { return (flags[i] & 1u) != 0; }, [&](int i) { return KeyOf<TR>::key(r[i]); }, kr0, i0,
-      scan);
-  KR* krs;
-  uint16_t* irs;
-  block_radix_sort<NT, MAXIPT, KR>(kr0, i0, kr1, i1, mr, sm + L.scratch, &krs, &irs);
-  uint16_t* gir = rp.ir + static_cast<size_t>(t) * rp.ld_ir;
-  for (int p = threadIdx.x; p < mr; p += NT) gir[p] = irs[p];
-  // tie-start bits, one word per warp step: lane k tests sorted position
-  // w * 32 + k (consecutive keys across the lanes, no bank conflicts)
-  uint32_t* gtie = rp.tie + static_cast<size_t>(t) * rp.ld_tie;
-  const int nw = (N + 31) / 32;
-  for (int w = static_cast<int>(threadIdx.x >> 5); w < nw; w += NT / 32) {  // uniform per warp
-    const int p = w * 32 + static_cast<int>(threadIdx.x & 31);
-    const bool start = p < mr && (p == 0 || krs[p] != krs[p - 1]);
-    const uint32_t bitsw = __ballot_sync(kFull, start);
-    if ((threadIdx.x & 31) == 0) gtie[w] = bitsw;
-  }
-  if (threadIdx.x == 0) rp.mr[t] = mr;
-}
-
-// One (date, factor) per CTA: blockIdx.x = t * F + f (the factors of a date
-// run side by side and share its prepared returns in L2).
-template <int NT, int MAXIPT, typename TF, typename TR, bool LEARNED>
-__global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT))
-    k_rank_ic_item(RankIcArgs<TF, TR> a, RicPrep rp, int resident, int* status) {
-  using KF = typename KeyOf<TF>::type;
-  using KR = typename KeyOf<TR>::type;
-  constexpr int KSZ = (sizeof(KF) > sizeof(KR)) ? int(sizeof(KF)) : int(sizeof(KR));
-  extern __shared__ __align__(16) uint8_t sm[];
-  const int N = a.N;
-  const RankIcLayout L(N, KSZ, SortScratch<NT>::bytes);
-  rank_ic_cta_init(sm);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L.bars);
-  const int t = blockIdx.x / a.F, f = blockIdx.x % a.F;
-  const int mr = rp.mr[t];
-  const int nw = (N + 31) / 32;
-  uint32_t ph[5] = {0, 0, 0, 0, 0};
-  bool arm[5] = {false, false, false, false, false};
-  // every input of this item in flight at once: prepared returns, the factor
-  // row, and (learned) the factor's CDF table into the idle histogram region
-  uint8_t* flags = stage_issue(sm + L.flags, rp.flags + static_cast<size_t>(t) * rp.ld_fl, N, &bars[0], arm[0]);
-  const uint16_t* IR = stage_issue(sm + L.ir, rp.ir + static_cast<size_t>(t) * rp.ld_ir, mr, &bars[1], arm[1]);
-  const uint32_t* tie = stage_issue(sm + L.gr, rp.tie + static_cast<size_t>(t) * rp.ld_tie, nw, &bars[2], arm[2]);
-  const size_t frow = (static_cast<size_t>(f) * a.T + t) * N;
-  const TF* x = stage_issue(sm + L.k1, a.X + frow, N, &bars[3], arm[3]);
-  const bool with_table = LEARNED && a.cdf_table != nullptr;
-  if (with_table) {
-    // table rows are 4 KB apart from an aligned base: the row lands at sm + L.scratch exactly
-    (void)stage_issue(sm + L.scratch, a.cdf_table + static_cast<size_t>(f) * kCdfKnots, kCdfKnots, &bars[4],
-                      arm[4]);
-  }
-  // items are dispatched in order: the CTA that starts when this one ends
-  // will take item blockIdx.x + resident -- bring its rows into L2 now
-  if (threadIdx.x == 0 && resident > 0) {
-    const unsigned nx = blockIdx.x + static_cast<unsigned>(resident);
-    if (nx < gridDim.x) {
-      const int tn = static_cast<int>(nx) / a.F, fn = static_cast<int>(nx) % a.F;
-      bulk_prefetch_l2(a.X + (static_cast<size_t>(fn) * a.T + tn) * N, static_cast<size_t>(N) * sizeof(TF));
-      if (fn == 0 || nx == blockIdx.x + static_cast<unsigned>(resident)) {
-        bulk_prefetch_l2(rp.flags + static_cast<size_t>(tn) * rp.ld_fl, static_cast<size_t>(N));
-        bulk_prefetch_l2(rp.ir + static_cast<size_t>(tn) * rp.ld_ir, static_cast<size_t>(N) * 2);
-      }
-    }
-  }
-  bool ok = stage_wait(&bars[0], ph[0], arm[0]);
-  ok = stage_wait(&bars[1], ph[1], arm[1]) && ok;
-  ok = stage_wait(&bars[2], ph[2], arm[2]) && ok;
-  ok = stage_wait(&bars[3], ph[3], arm[3]) && ok;
-  if (with_table) ok = stage_wait(&bars[4], ph[4], arm[4]) && ok;
-  if (__syncthreads_or(!ok)) {
-    if (threadIdx.x == 0) atomicExch(status, 1);
-    return;
-  }
-  // sorted returns positions p < q hold equal keys iff no key starts in (p, q]
-  auto same_group = [&](int p, int q) {
-    bool brk = false;
-    if (q > p) {
-      const int w0 = (p + 1) >> 5, w1 = q >> 5;
-      for (int w = w0 + static_cast<int>(threadIdx.x); w <= w1; w += NT) {
-        uint32_t m = tie[w];
-        if (w == w0) m &= 0xFFFFFFFFu << ((p + 1) & 31);
-        if (w == w1) m &= 0xFFFFFFFFu >> (31 - (q & 31));
-        brk = brk || (m != 0u);
-      }
-    }
-    return !__syncthreads_or(brk);
-  };
-  (void)rank_ic_factor<NT, MAXIPT, TF, TR, LEARNED>(a, t, f, sm, L, ph, status, flags, IR, mr, same_group, x,
-                                                   with_table);
-}
-
 template <int NT, int MAXIPT, typename TF, typename TR, bool LEARNED>
 __global__ void __launch_bounds__(NT, (NT >= 1024 ? 1 : 1024 / NT)) k_rank_ic(RankIcArgs<TF, TR> a, int* status) {
   extern __shared__ __align__(16) uint8_t sm[];
@@ -899,83 +751,5 @@ template cudaError_t launch_rank_ic_batch<float, float>(int, bool, const RankIcA
                                                          int*, int, size_t, int*, cudaStream_t, int*);
 template cudaError_t launch_rank_ic_batch<double, double>(int, bool, const RankIcArgs<double, double>*, const int2*,
                                                            int, int*, int, size_t, int*, cudaStream_t, int*);
-
-// ---------------------------------------------------------------------------
-// per-(date, factor) rank + IC: returns prepared once per date
-// ---------------------------------------------------------------------------
-size_t ric_prep_bytes(int T, int N) {
-  const size_t ld_ir = (static_cast<size_t>(N) + 7) / 8 * 8, ld_tie = ((static_cast<size_t>(N) + 31) / 32 + 3) / 4 * 4,
-               ld_fl = (static_cast<size_t>(N) + 15) / 16 * 16;
-  return static_cast<size_t>(T) * (ld_ir * 2 + ld_tie * 4 + ld_fl + 4) + 4 * 256;
-}
-
-RicPrep ric_prep_carve(void* base, int T, int N) {
-  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-  RicPrep rp{};
-  rp.ld_ir = (N + 7) / 8 * 8;
-  rp.ld_tie = ((N + 31) / 32 + 3) / 4 * 4;
-  rp.ld_fl = (N + 15) / 16 * 16;
-  uint8_t* p = static_cast<uint8_t*>(base);
-  rp.ir = reinterpret_cast<uint16_t*>(p);
-  p += al(static_cast<size_t>(T) * rp.ld_ir * 2);
-  rp.tie = reinterpret_cast<uint32_t*>(p);
-  p += al(static_cast<size_t>(T) * rp.ld_tie * 4);
-  rp.flags = p;
-  p += al(static_cast<size_t>(T) * rp.ld_fl);
-  rp.mr = reinterpret_cast<int*>(p);
-  return rp;
-}
-
-template <int NT, typename TF, typename TR, bool LEARNED>
-static cudaError_t items_nt(const RankIcArgs<TF, TR>& a, RicPrep rp, int* status, cudaStream_t st) {
-  constexpr int KSZ = (sizeof(TF) > sizeof(TR)) ? int(sizeof(TF)) : int(sizeof(TR));
-  const size_t smem_r = RankIcLayout(a.N, int(sizeof(typename KeyOf<TR>::type)), SortScratch<NT>::bytes).total;
-  const size_t smem = RankIcLayout(a.N, KSZ, SortScratch<NT>::bytes).total;
-  if (smem > kMaxSmemPerBlock) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(k_ric_returns<NT, 16, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem_r));
-  if (e != cudaSuccess) return e;
-  k_ric_returns<NT, 16, TR><<<a.T, NT, smem_r, st>>>(a.R, a.rmask, a.fmask, a.N, rp, status);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_rank_ic_item<NT, 16, TF, TR, LEARNED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem));
-  if (e != cudaSuccess) return e;
-  const long long grid = static_cast<long long>(a.T) * a.F;
-  if (grid > 2147483647LL) return cudaErrorInvalidValue;
-  // resident CTAs (the prefetch distance)
-  int occ = 0, dev = 0, sms = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rank_ic_item<NT, 16, TF, TR, LEARNED>, NT, smem) !=
-          cudaSuccess ||
-      cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-    occ = sms = 0;
-  k_rank_ic_item<NT, 16, TF, TR, LEARNED><<<static_cast<unsigned>(grid), NT, smem, st>>>(a, rp, occ * sms, status);
-  return cudaGetLastError();
-}
-
-template <typename TF, typename TR>
-cudaError_t launch_rank_ic_items(const RankIcArgs<TF, TR>& a, RicPrep rp, bool learned, int* status,
-                                 cudaStream_t st) {
-  if (!rank_ic_fits_smem<TF, TR>(a.N)) return cudaErrorInvalidValue;
-  if (learned) {
-    if constexpr (std::is_same<TF, float>::value && std::is_same<TR, float>::value) {
-      if (a.cdf_table == nullptr || a.cdf_zrange == nullptr) return cudaErrorInvalidValue;
-      switch (pick_nt(a.N)) {
-        case 256: return items_nt<256, TF, TR, true>(a, rp, status, st);
-        case 512: return items_nt<512, TF, TR, true>(a, rp, status, st);
-        default: return items_nt<1024, TF, TR, true>(a, rp, status, st);
-      }
-    } else {
-      return cudaErrorInvalidValue;
-    }
-  }
-  switch (pick_nt(a.N)) {
-    case 256: return items_nt<256, TF, TR, false>(a, rp, status, st);
-    case 512: return items_nt<512, TF, TR, false>(a, rp, status, st);
-    default: return items_nt<1024, TF, TR, false>(a, rp, status, st);
-  }
-}
-template cudaError_t launch_rank_ic_items<float, float>(const RankIcArgs<float, float>&, RicPrep, bool, int*,
-                                                         cudaStream_t);
 
 }  // namespace fcb

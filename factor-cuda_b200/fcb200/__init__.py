@@ -679,6 +679,22 @@ class CdfModel:
                                          int(tcount), int(steps), float(lr), stream)
         nat.check(rc, "fcb_cdf_model_fit")
 
+    def sample(self, d_x, d_ranks, T, N, t0, tcount, stream=None):
+        """Draw training samples from dates [t0, t0+tcount) (first half of a fit)."""
+        rc = nat.lib().fcb_cdf_model_sample(self._h, nat.ptr(d_x), nat.ptr(d_ranks), int(T), int(N), int(t0),
+                                            int(tcount), stream)
+        nat.check(rc, "fcb_cdf_model_sample")
+
+    def train(self, steps, lr, into_idle=True, stream=None):
+        """Adam steps on the drawn samples, tabulated into the idle table slot
+        (rank calls keep reading the current one) or the current slot."""
+        nat.check(nat.lib().fcb_cdf_model_train(self._h, int(steps), float(lr), 1 if into_idle else 0, stream),
+                  "fcb_cdf_model_train")
+
+    def swap(self):
+        """Make the slot the last train(into_idle=True) wrote the current one."""
+        nat.check(nat.lib().fcb_cdf_model_swap(self._h), "fcb_cdf_model_swap")
+
     def state(self):
         P, K = 1153, 1024
         params = np.empty((self.F, P), np.float32)

@@ -79,10 +79,15 @@ PROTOTYPES = {
     "fcb_dev_factor_corr_noalloc": (_i, [_p, _i, _p, _i, _i, _i, _p, _p]),
     "fcb_stock_corr_prec": (_i, [_p, _p, _i, _i, _i, _p, _p]),
     "fcb_dev_stock_corr_prec": (_i, [_p, _p, _i, _i, _i, _p, _p, _p]),
+    "fcb_factor_corr_bf16x3": (_i, [_p, _p, _i, _i, _i, _p, _p]),
+    "fcb_dev_factor_corr_bf16x3": (_i, [_p, _p, _i, _i, _i, _i, _p, _p, _p]),
     "fcb_cdf_model_create": (_p, [_i, C.c_uint64]),
     "fcb_cdf_model_destroy": (None, [_p]),
     "fcb_cdf_model_set_linear": (_i, [_p, _i]),
     "fcb_cdf_model_fit": (_i, [_p, _p, _p, _i, _i, _i, _i, _i, C.c_float, _p]),
+    "fcb_cdf_model_sample": (_i, [_p, _p, _p, _i, _i, _i, _i, _p]),
+    "fcb_cdf_model_train": (_i, [_p, _i, C.c_float, _i, _p]),
+    "fcb_cdf_model_swap": (_i, [_p]),
     "fcb_cdf_model_state": (_i, [_p, _p, _p, _p, _p]),
     "fcb_cdf_model_load": (_i, [_p, _p, _p, _p]),
     "fcb_cdf_grad": (_i, [_p, _p, _p, _i, _p, _p]),

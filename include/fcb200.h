@@ -241,6 +241,20 @@ int fcb_cdf_model_set_linear(fcb_cdf_model* m, int linear);
  * continuing from the model's previous state, then tabulation.  Async. */
 int fcb_cdf_model_fit(fcb_cdf_model* m, const float* d_x, const float* d_ranks, int T, int N, int t0, int tcount,
                       int steps, float lr, void* stream);
+/* The two halves of a fit, for refits that overlap ranking (no reference
+ * counterpart).  fcb_cdf_model_sample draws the training samples from dates
+ * [t0, t0+tcount) of d_x and its exact ranks d_ranks on `stream` (order it
+ * after the kernel that wrote the ranks; the ranks buffer may be reused once
+ * it has run).  fcb_cdf_model_train runs `steps` Adam steps on the drawn
+ * samples and tabulates into the current table slot (into_idle = 0) or into
+ * the idle one (into_idle = 1), which rank calls do not read.
+ * fcb_cdf_model_swap makes the idle slot current for later rank calls: call
+ * it after the training stream has passed the refit (or order the next rank
+ * call's stream after it).  Only one refit may be in flight per model. */
+int fcb_cdf_model_sample(fcb_cdf_model* m, const float* d_x, const float* d_ranks, int T, int N, int t0,
+                         int tcount, void* stream);
+int fcb_cdf_model_train(fcb_cdf_model* m, int steps, float lr, int into_idle, void* stream);
+int fcb_cdf_model_swap(fcb_cdf_model* m);
 /* Save / restore (host buffers): params (F*FCB_CDF_PARAMS), zrange (F*2),
  * table (F*FCB_CDF_KNOTS), last minibatch loss (F); NULL skips a field. */
 int fcb_cdf_model_state(const fcb_cdf_model* m, float* params, float* zrange, float* table, float* loss);
@@ -280,6 +294,26 @@ int fcb_stock_corr_prec(const float* x, const uint8_t* mask, int T, int N, int m
                         fcb_workspace* ws);
 int fcb_dev_stock_corr_prec(const float* d_x, const uint8_t* d_mask, int T, int N, int mode, double* d_out,
                             fcb_workspace* ws, void* stream);
+
+/* BF16x3 precision form of factor_corr (no reference counterpart; the
+ * tensor-core form of factor_corr_gpu, src/factor_corr.cuh:46-49).  The pooled
+ * moment products n, sum x', sum x'^2, sum x'x' over the T*N (t,i) rows of an
+ * f32 panel (x' = x minus a per-factor shift near its mean) are tcgen05 GEMMs
+ * on three bf16 limbs of x' and of x'^2 with fp32 accumulation, split over the
+ * SMs and merged in f64; r = (cov/sqrt(vx))/sqrt(vy) in f64, NaN for n < 2 or
+ * a non-positive variance, diagonal 1.0 iff finite, lower triangle mirrored.
+ * No cancellation fallback: tolerance (|err| <= 1e-6 per output against the
+ * f64 path, stated in the tests), not bit parity.  F <= 16 (larger F returns
+ * FCB_ERR_UNSUPPORTED; the f64 entry points take F <= 128).
+ * fcb_factor_corr_bf16x3: host (T,N,F) panel, synchronous, ws may be NULL.
+ * fcb_dev_factor_corr_bf16x3: device buffers, planes = 0 (T,N,F) or 1 (F,T,N)
+ * factor planes, asynchronous on `stream`, scratch from `ws` (required);
+ * bounded waits report through fcb_dev_status.
+ * Returns -1 null/dim, -2 T*N > INT32_MAX, -3 F > 128. */
+int fcb_factor_corr_bf16x3(const float* x, const uint8_t* mask, int T, int N, int F, double* out,
+                           fcb_workspace* ws);
+int fcb_dev_factor_corr_bf16x3(const float* d_x, const uint8_t* d_mask, int T, int N, int F, int planes,
+                               double* d_out, fcb_workspace* ws, void* stream);
 
 /* ------------------------------------------------ no-allocation variant ---
  * No counterpart in the reference.  factor_corr for callers that cannot let a

@@ -1,10 +1,10 @@
 """Generate the golden vectors that pin the oracle and the CUDA path.
 
-Run in a container where the reference is mounted (it is read-only; nothing is
-copied from it except the outputs its own CPU path computes here and the
+Run where a checkout of the reference is available (it is only read; nothing
+is copied from it except the outputs its own CPU path computes here and the
 frozen anchor arrays/expected values of its fixtures):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path to the reference checkout>
 
 Writes ``tests/golden/golden_v1.npz`` (arrays) and ``tests/golden/golden_v1.json``
 (case list).  Sources of truth, all from the reference:
@@ -239,4 +239,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the reference checkout>")
+    main(sys.argv[1])

@@ -58,6 +58,13 @@ def test_contract_errors_without_device(native):
     assert lib.fcb_factor_corr(P(x), 0, None, 1, 1, 129, P(o), None) == -3
     assert lib.fcb_factor_corr(P(x), 0, None, 1 << 16, 1 << 16, 2, P(o), None) == -2
     assert lib.fcb_dev_factor_corr(P(x), 0, None, 1, 1, 129, 0, P(o), None, None) == -3
+    # the BF16x3 precision form: same caps, F <= 16 on the tensor-core path
+    assert lib.fcb_factor_corr_bf16x3(None, None, 2, 2, 2, P(o), None) == -1
+    assert lib.fcb_factor_corr_bf16x3(P(x), None, 1, 1, 129, P(o), None) == -3
+    assert lib.fcb_factor_corr_bf16x3(P(x), None, 1 << 16, 1 << 16, 2, P(o), None) == -2
+    assert lib.fcb_factor_corr_bf16x3(P(x), None, 1, 1, 17, P(o), None) == -5   # F > 16: unsupported
+    assert lib.fcb_dev_factor_corr_bf16x3(P(x), None, 1, 1, 2, 2, P(o), None, None) == -1   # planes 0/1
+    assert lib.fcb_dev_factor_corr_bf16x3(P(x), None, 1, 1, 2, 1, P(o), None, None) == -1   # workspace required
     assert lib.fcb_dev_factor_corr(P(x), 0, None, 2, 2, 2, 0, P(o), None, None) == -1   # workspace required
     assert lib.fcb_dev_factor_corr(P(x), 0, None, 2, 2, 2, 2, P(o), None, None) == -1   # layout flag
     assert lib.fcb_stock_corr(P(x), 0, None, 1, 46341, P(o), None, None) == -3
@@ -178,6 +185,16 @@ def test_dropin_modules_import_and_gate_dtypes(native):
     ws.clear()
     ws.clear()
     fcb.RollingIcWorkspace().clear()
+    # each function takes only the workspace class it is bound to
+    # (src/factor_cuda_pybind.cpp:135,179,293 bind the typed handles)
+    with pytest.raises(TypeError):
+        fcb.cs_rank_f32(x32, None, False, fcb.RollingIcWorkspace())
+    with pytest.raises(TypeError):
+        fcb.parameter_scan_f32(x32, np.ones((2, 3), bool), workspace=fcb.RollingIcWorkspace())
+    with pytest.raises(TypeError):
+        fcb.rolling_ic_f64(x32, x32, None, None, 30, workspace=ws)
+    with pytest.raises(TypeError):
+        fcb.cs_rank_f32(x32, None, False, object())
 
 
 def test_package_layout():
