@@ -20,6 +20,7 @@ workload on its own GPU ("replicas only": the path has no exchange step).
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import pathlib
@@ -269,19 +270,17 @@ def run_b200(args, rank, world):
         e1.record(stream)
         torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1) / args.steps
-    # parity spot check of the timed outputs against the oracle (a few dates)
-    spot = check_spot(X, R, fm, rm, dranks, dic)
+    timed_ranks = dranks.cpu().numpy()
+    timed_ic = dic.cpu().numpy()
     learned_info = None
     if learn is not None:
         st = learn["stats"].cpu().numpy()
         codes = st[..., 0]
         # bit-exactness of the whole learned output against the radix path
-        lr_ranks = dranks.clone()
-        lr_ic = dic.clone()
         radix_step()
         torch.cuda.synchronize(dev)
-        exact = bool(torch.equal(lr_ranks.view(torch.int32), dranks.view(torch.int32))) and \
-            bool(torch.equal(torch.nan_to_num(lr_ic, nan=7.0), torch.nan_to_num(dic, nan=7.0)))
+        exact = bool(np.array_equal(timed_ranks.view(np.uint32), dranks.cpu().numpy().view(np.uint32))) and \
+            ic_bitwise(timed_ic, dic.cpu().numpy())
         # learned vs radix under the same conditions: alternating windows of
         # max(K, 20) steps each, three rounds, medians (the headline `value`
         # above is the contract's K-step measurement)
@@ -301,7 +300,11 @@ def run_b200(args, rank, world):
         rounds = [(window(step), window(radix_step)) for _ in range(3)]
         learned_ms_cmp = sorted(r[0] for r in rounds)[1]
         radix_ms = sorted(r[1] for r in rounds)[1]
+        saved = radix_ms - learned_ms_cmp
         learned_info = {"fit_ms": learn["fit_ms"], "train_dates": learn["train_dates"],
+                        "fit": "1500 Adam steps on 64 samples per (factor, date) of dates [0, 250), once, "
+                               "before the timed steps (not in ms_per_step)",
+                        "break_even_steps": (learn["fit_ms"] / saved) if saved > 0 else None,
                         "learned_fraction": float((codes == 1).mean()),
                         "fallback_overflow": float((codes == 2).mean()),
                         "fallback_judge": float((codes == 3).mean()),
@@ -313,55 +316,90 @@ def run_b200(args, rank, world):
                         "speedup_vs_radix": radix_ms / learned_ms_cmp}
 
     # e2e: host entry point, pinned buffers, copies in the timed region
-    if args.no_e2e:
-        res = finish(args, world, X, R, fm, rm, ms, None, None, clk, spot, dev, learned_info)
-        res["factor_corr"] = bench_factor_corr(dX, dfm, X, fm, dev, steps=max(3, args.steps // 2))
-        res["c2_stages"] = bench_c2_stages(dX, X, fm, dev, ms, res["factor_corr"]["ms"])
-        return res
-    hX = torch.from_numpy(X).pin_memory()
-    hR = torch.from_numpy(R).pin_memory()
-    hfm = torch.from_numpy(fm).pin_memory()
-    hrm = torch.from_numpy(rm).pin_memory()
-    hranks = torch.empty((F, T, N), dtype=torch.float32).pin_memory()
-    hic = torch.empty((F, T), dtype=torch.float64).pin_memory()
-    ws = lib.fcb_workspace_create()
+    e2e_s = e2e_ok = None
+    if not args.no_e2e:
+        hX = torch.from_numpy(X).pin_memory()
+        hR = torch.from_numpy(R).pin_memory()
+        hfm = torch.from_numpy(fm).pin_memory()
+        hrm = torch.from_numpy(rm).pin_memory()
+        hranks = torch.empty((F, T, N), dtype=torch.float32).pin_memory()
+        hic = torch.empty((F, T), dtype=torch.float64).pin_memory()
+        ws = lib.fcb_workspace_create()
 
-    def host_step():
-        rc = lib.fcb_rank_ic_panel(hX.data_ptr(), hR.data_ptr(), hfm.data_ptr(), hrm.data_ptr(), F, T, N,
-                                   MIN_VALID, hranks.data_ptr(), hic.data_ptr(), method, ws)
-        nat.check(rc, "fcb_rank_ic_panel")
+        def host_step():
+            rc = lib.fcb_rank_ic_panel(hX.data_ptr(), hR.data_ptr(), hfm.data_ptr(), hrm.data_ptr(), F, T, N,
+                                       MIN_VALID, hranks.data_ptr(), hic.data_ptr(), method, ws)
+            nat.check(rc, "fcb_rank_ic_panel")
 
-    for _ in range(max(1, args.warmup)):
-        host_step()
-    if method == 1:
-        # let the workspace's background fit land before timing (bounded)
-        import ctypes as C
-        rdy, fits, lch = C.c_int(), C.c_int(), C.c_int()
-        for _ in range(5):
-            lib.fcb_workspace_learned_state(ws, C.byref(rdy), C.byref(fits), C.byref(lch))
-            if rdy.value:
-                break
+        for _ in range(max(1, args.warmup)):
             host_step()
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        host_step()
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    lib.fcb_workspace_destroy(ws)
-    e2e_ok = bool(np.array_equal(hranks.numpy().view(np.uint32), dranks.cpu().numpy().view(np.uint32)))
-    res = finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info)
-    res["factor_corr"] = bench_factor_corr(dX, dfm, X, fm, dev, steps=max(3, args.steps // 2))
-    res["c2_stages"] = bench_c2_stages(dX, X, fm, dev, ms, res["factor_corr"]["ms"])
+        if method == 1:
+            # let the workspace's background fit land before timing (bounded)
+            import ctypes as C
+            rdy, fits, lch = C.c_int(), C.c_int(), C.c_int()
+            for _ in range(5):
+                lib.fcb_workspace_learned_state(ws, C.byref(rdy), C.byref(fits), C.byref(lch))
+                if rdy.value:
+                    break
+                host_step()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            host_step()
+        e2e_s = (time.perf_counter() - t0) / args.steps
+        lib.fcb_workspace_destroy(ws)
+        e2e_ok = bool(np.array_equal(hranks.numpy().view(np.uint32), timed_ranks.view(np.uint32)))
+    res = finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, dev, learned_info)
+    fcl = bench_factor_corr(dX, dfm, X, fm, dev, steps=max(3, args.steps // 2))
+    res["factor_corr"] = fcl
+    res["c2_stages"] = bench_c2_stages(dX, X, fm, dev, ms, fcl["f64"]["ms"])
+    # parity of the timed outputs (and of the stage legs) against the oracle on
+    # the whole panel
+    if not args.no_parity and rank == 0:
+        orc = oracle_c2(X, R, fm, rm)
+        rank_ok = all(_sha(timed_ranks[f]) == orc["rank_sha"][f] for f in range(F))
+        ic_ok = ic_bitwise(timed_ic, orc["ic"])
+        fmb = fm.astype(bool)
+        scan_ok = True
+        for f, shas in orc["scan_sha"].items():
+            r = nat.fcb().parameter_scan_f32(np.ascontiguousarray(X[f]), fmb, return_timing=False)
+            scan_ok &= [_sha(g) for g in r["groups"]] == shas
+        ex = orc["factor_corr"]
+        f64 = np.asarray(fcl.pop("_f64_out"))
+        bf = np.asarray(fcl.pop("_bf16x3_out"))
+        same_nan = bool(np.array_equal(np.isnan(f64), np.isnan(ex)))
+        e64 = float(np.nanmax(np.abs(f64 - ex)))
+        ebf = np.abs(bf - ex)
+        res["parity"] = {
+            "oracle": "numpy restatement of the reference CPU path (fc/_cpu_core.py), pinned to its outputs",
+            "rank_ic": {"compared": f"cs ranks of all {F}x{T}x{N} cells (bit patterns) and the IC of all "
+                                    f"{F}x{T} (factor, date) sections of the timed step",
+                        "bit_exact": bool(rank_ok and ic_ok)},
+            "parameter_scan": {"compared": f"all four groups of planes {sorted(orc['scan_sha'])} "
+                                           f"({T}x{N}), drop-in binding parameter_scan_f32",
+                               "bit_exact": bool(scan_ok)},
+            "factor_corr_f64": {"compared": f"{F}x{F} over {T * N} rows, fcb_dev_factor_corr on factor planes",
+                                "max_abs_err": e64, "tol": 1e-12, "ok": bool(same_nan and e64 <= 1e-12)},
+            "factor_corr_bf16x3": {"max_abs_err": float(np.nanmax(ebf)), "mean_abs_err": float(np.nanmean(ebf)),
+                                   "tol": 1e-6, "nan_pattern_matches": bool(np.array_equal(np.isnan(bf),
+                                                                                           np.isnan(ex)))},
+            "oracle_seconds": orc["seconds"]}
+        fcl["f64"]["max_abs_err_vs_oracle"] = e64
+        fcl["bf16x3"]["max_abs_err_vs_oracle"] = float(np.nanmax(ebf))
+        fcl["bf16x3"]["mean_abs_err_vs_oracle"] = float(np.nanmean(ebf))
+    else:
+        fcl.pop("_f64_out", None)
+        fcl.pop("_bf16x3_out", None)
     return res
 
 
-# DRAM bytes of one rank + IC step per date at N=5000, F=12 (k_ric_returns +
-# k_rank_ic_item), from one ncu capture each at T=600
-# (profiles/k_rank_ic_item_T600_N5000_F12.md): dram__bytes_read.sum +
-# dram__bytes_write.sum.  Traffic grows with the number of dates at fixed N
-# and F, so the bench's step is that times T.
+# DRAM bytes of one rank + IC step per date at N=5000, F=12 (the returns
+# preparation plus the per-(date, factor) rank kernel), from one ncu capture
+# of each kernel at T=600: dram__bytes_read.sum + dram__bytes_write.sum.
+# Traffic grows with the number of dates at fixed N and F, so the bench's step
+# is that times T.
 TRAFFIC_PER_DATE = {"learned": (153.391360e6 + 103.361792e6 + 18.050048e6) / 600,
                     "radix": (153.914368e6 + 102.658048e6 + 18.050048e6) / 600}
 
@@ -382,7 +420,7 @@ def job_throughput(world, cells_per_rank, ms_max):
     return world * cells_per_rank / (ms_max / 1e3) / 1e9
 
 
-def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned_info=None):
+def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, dev, learned_info=None):
     F, T, N = X.shape
     ms_all, e2e_all = ms, (e2e_s if e2e_s is not None else 0.0)
     if world > 1:
@@ -409,10 +447,11 @@ def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "traffic_source": "ncu dram bytes at T=600 scaled by T/600" if traffic else None,
-                     "kernel": "k_ric_returns + k_rank_ic_item", "algorithmic_bytes_per_launch": bytes_launch},
-        "gpu_launches": args.steps,
+                     "kernel": "k_ric_prep + k_ric_learned" if args.method == "learned" else
+                               "k_ric_prep + k_ric_radix",
+                     "algorithmic_bytes_per_launch": bytes_launch},
+        "gpu_launches": args.steps * (3 if args.method == "learned" else 2),
         "clocks": clk.summary(),
-        "parity_spot_check": spot,
     }
     if learned_info is not None:
         res["learned"] = learned_info
@@ -421,9 +460,10 @@ def finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, spot, dev, learned
 
 def bench_factor_corr(dX, dfm, X, fm, dev, steps=5, warmup=2):
     """factor_corr of the C2 panel (F factors pooled over the T*N (t, i) rows,
-    factor mask broadcast per column), device-resident factor planes, through
-    fcb_dev_factor_corr; spot-checked against the host entry point on the
-    reference's (T,N,F) layout."""
+    factor mask broadcast per column) on the device-resident factor planes:
+    the FP64 drop-in (fcb_dev_factor_corr) and the BF16x3 tensor-core form
+    (fcb_dev_factor_corr_bf16x3).  Both outputs are handed back for the
+    oracle comparison."""
     import torch
     from fcb200 import _native as nat
     lib = nat.lib()
@@ -431,41 +471,44 @@ def bench_factor_corr(dX, dfm, X, fm, dev, steps=5, warmup=2):
     ws = lib.fcb_workspace_create()
     out = torch.empty((F, F), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
-
-    def run():
-        nat.check(lib.fcb_dev_factor_corr(dX.data_ptr(), 0, dfm.data_ptr(), T, N, F, 1, out.data_ptr(), ws,
-                                          stream.cuda_stream), "fcb_dev_factor_corr")
-
-    for _ in range(warmup):
-        run()
-    torch.cuda.synchronize(dev)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
-        run()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1) / steps
-    got = out.cpu().numpy()
-    ref = np.empty((F, F))
-    x3 = np.ascontiguousarray(np.moveaxis(X, 0, -1))
-    nat.check(lib.fcb_factor_corr(nat.ptr(x3), 0, nat.ptr(fm), T, N, F, nat.ptr(ref), None), "fcb_factor_corr")
-    lib.fcb_workspace_destroy(ws)
     rows = T * N
-    alg_bytes = rows * (4 * F + 1)
     peak, _ = measured_peaks()
-    same = bool(np.array_equal(np.isnan(got), np.isnan(ref)) and
-                np.nanmax(np.abs(np.nan_to_num(got) - np.nan_to_num(ref))) <= 1e-12)
-    return {"workload": f"factor_corr {F}x{F} over {rows} (t,i) rows, f32 factor planes, factor mask",
-            "ms": ms, "rows_per_s": rows / (ms / 1e3), "algorithmic_gb_s": alg_bytes / (ms / 1e3) / 1e9,
-            "hbm_frac": alg_bytes / (ms / 1e3) / 1e9 / peak, "matches_host_entry_point": same}
+    res = {"workload": f"factor_corr {F}x{F} over {rows} (t,i) rows, f32 factor planes, factor mask"}
+    for name, fn in (("f64", lib.fcb_dev_factor_corr), ("bf16x3", lib.fcb_dev_factor_corr_bf16x3)):
+        def run():
+            if name == "f64":
+                nat.check(fn(dX.data_ptr(), 0, dfm.data_ptr(), T, N, F, 1, out.data_ptr(), ws, stream.cuda_stream),
+                          "fcb_dev_factor_corr")
+            else:
+                nat.check(fn(dX.data_ptr(), dfm.data_ptr(), T, N, F, 1, out.data_ptr(), ws, stream.cuda_stream),
+                          "fcb_dev_factor_corr_bf16x3")
+
+        for _ in range(warmup):
+            run()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / steps
+        nat.check(lib.fcb_dev_status(), "fcb_dev_status")
+        alg_bytes = rows * (4 * F + 1)
+        res[name] = {"ms": ms, "rows_per_s": rows / (ms / 1e3), "algorithmic_gb_s": alg_bytes / (ms / 1e3) / 1e9,
+                     "hbm_frac": alg_bytes / (ms / 1e3) / 1e9 / peak}
+        res["_" + name + "_out"] = out.cpu().numpy()
+    lib.fcb_workspace_destroy(ws)
+    res["bf16x3"]["algorithmic_tflops"] = 4 * 2.0 * F * F * rows / (res["bf16x3"]["ms"] / 1e3) / 1e12
+    res["bf16x3_speedup_vs_f64"] = res["f64"]["ms"] / res["bf16x3"]["ms"]
+    return res
 
 
 def bench_c2_stages(dX, X, fm, dev, rank_ic_ms, factor_corr_ms, steps=3):
     """The C2 pipeline stage by stage on the same panel: cs_rank of every factor
     plane (device entry point, CUDA events), parameter_scan (4 groups) of every
-    plane (its own device timing, host buffers), and the fused rank + IC and
+    plane (device entry point, CUDA events), and the fused rank + IC and
     factor_corr legs measured above -- the counterpart of the reference's
     parameter_scan -> rolling_ic -> factor_corr pipeline figure."""
     import ctypes as C
@@ -475,6 +518,9 @@ def bench_c2_stages(dX, X, fm, dev, rank_ic_ms, factor_corr_ms, steps=3):
     F, T, N = X.shape
     dfm = torch.from_numpy(fm).to(dev)
     out = torch.empty((T, N), dtype=torch.float32, device=dev)
+    souts = [torch.empty((T, N), dtype=torch.float32, device=dev) for _ in range(4)]
+    optr = (C.c_void_p * 4)(*[o.data_ptr() for o in souts])
+    st = (C.c_int * 4)()
     stream = torch.cuda.current_stream(dev)
 
     def cs_all():
@@ -482,38 +528,30 @@ def bench_c2_stages(dX, X, fm, dev, rank_ic_ms, factor_corr_ms, steps=3):
             nat.check(lib.fcb_dev_cs_rank_f32(dX[f].data_ptr(), dfm.data_ptr(), T, N, 0, out.data_ptr(),
                                               stream.cuda_stream), "fcb_dev_cs_rank_f32")
 
-    cs_all()
-    torch.cuda.synchronize(dev)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
-        cs_all()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    cs_ms = e0.elapsed_time(e1) / steps
-    # parameter_scan: device time of the fused four-group pass per plane
-    outs = [np.empty((T, N), np.float32) for _ in range(4)]
-    optr = (C.c_void_p * 4)(*[nat.ptr(o) for o in outs])
-    st = (C.c_int * 4)()
-    tg = (C.c_float * 4)()
-    ws = lib.fcb_workspace_create()
-    scan_ms = []
-    for _ in range(2):
-        tot = 0.0
+    def scan_all():
         for f in range(F):
-            xf = np.ascontiguousarray(X[f])
-            nat.check(lib.fcb_parameter_scan_f32(nat.ptr(xf), nat.ptr(fm), T, N, optr, st, None, tg, None, ws),
-                      "fcb_parameter_scan_f32")
-            tot += sum(float(v) for v in tg)
-        scan_ms.append(tot)
-    lib.fcb_workspace_destroy(ws)
-    scan = min(scan_ms)
+            nat.check(lib.fcb_dev_parameter_scan_f32(dX[f].data_ptr(), dfm.data_ptr(), T, N, optr, st, None,
+                                                     stream.cuda_stream), "fcb_dev_parameter_scan_f32")
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / steps
+
+    cs_ms = timed(cs_all)
+    scan = timed(scan_all)
     return {"workload": f"C2 stages on {F} factor planes of {T}x{N}",
             "cs_rank_ms_all_planes": cs_ms, "parameter_scan_ms_all_planes": scan,
             "rank_ic_ms_all_planes": rank_ic_ms, "factor_corr_ms": factor_corr_ms,
             "pipeline_ms": scan + rank_ic_ms + factor_corr_ms,
-            "pipeline": "parameter_scan (4 groups) + cs_rank/rolling_ic (fused, learned) + factor_corr, "
+            "pipeline": "parameter_scan (4 groups) + cs_rank/rolling_ic (fused, learned) + factor_corr (f64), "
                         "device-resident kernels"}
 
 
@@ -547,7 +585,7 @@ def make_batch_panels(dev, n=64, F=8, seed=20261205):
     return panels
 
 
-def bench_batch(dev, steps=5, warmup=2, tune_cache=None):
+def bench_batch(dev, steps=5, warmup=2, tune_cache=None, cpu_sample=True):
     """Batched uneven panels: one autotuned CUDA-graph replay of the
     persistent rank+IC kernels + per-panel factor_corr, against the same work
     issued one panel at a time.  Device-resident inputs (8.8 GB of factors,
@@ -606,6 +644,25 @@ def bench_batch(dev, steps=5, warmup=2, tune_cache=None):
            "bit_exact_graph_vs_per_panel": bool(same),
            "autotune": {"config": cfg, "tuned_ms": tuned_ms, "tuning_s": tune_s, "from_cache": cached}}
     b.close()
+    if cpu_sample:
+        # CPU baseline: the oracle port of the reference CPU path on one whole
+        # panel (cs_rank + rolling_ic of every factor, factor_corr), scaled to
+        # the batch by cells
+        from oracle import fc_oracle as O
+        p0 = panels[0]
+        Xh, Rh = p0["X"].cpu().numpy(), p0["R"].cpu().numpy()
+        fmh, rmh = p0["fmask"].cpu().numpy().astype(bool), p0["rmask"].cpu().numpy().astype(bool)
+        t0 = time.perf_counter()
+        for f in range(Xh.shape[0]):
+            O.cs_rank(Xh[f], fmh, False)
+            O.rolling_ic(Xh[f], Rh, fmh, rmh, MIN_VALID)
+        O.factor_corr(np.ascontiguousarray(np.moveaxis(Xh, 0, -1)), fmh)
+        el = time.perf_counter() - t0
+        v = Xh.size / el / 1e9
+        res["cpu_baseline"] = {"value": v, "unit": "Gelem/s", "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"panel 0 ({Xh.shape[1]}x{Xh.shape[2]}x{Xh.shape[0]}, {el:.1f} s): "
+                                         "np_cs_rank + np_rolling_ic per factor + np_factor_corr; the 64-panel "
+                                         f"batch extrapolates to {cells / v / 1e9:.0f} s"}
     del panels
     torch.cuda.empty_cache()
     return res
@@ -644,13 +701,22 @@ def make_c5_block(dev, g, rng, state, F, Tb, N, start):
     return X.contiguous(), R.float().contiguous(), listed.to(torch.uint8), torch.isfinite(R).to(torch.uint8)
 
 
-def bench_c5(dev, T=5000, N=8000, F=128, Tb=250, seed=20261206):
+def bench_c5(dev, T=5000, N=8000, F=128, Tb=250, seed=20261206, cpu_sample=True):
     """Learned splitters on the streaming configuration (T=5000, N=8000,
     F=128: 5.12 G cells, 20.5 GB of f32 factors, device-resident in blocks of
-    250 dates).  The CDF networks are fitted on the exact ranks of dates
-    [0, 500) and refitted on every later block's ranks before the next block;
-    every block is ranked by the learned path and by the plain radix path, and
-    the two outputs are compared bit for bit."""
+    250 dates), two end-to-end runs timed by CUDA events around the whole
+    block loop:
+      radix    every block ranked by the plain radix path;
+      learned  blocks 0 and 1 ranked by radix and the networks fitted on their
+               exact ranks (1500 + 300 Adam steps, in line: nothing else is
+               ready to run); every later block ranked by the learned path;
+               after each block the training samples are drawn from its
+               (exact) ranks on the ranking stream and a 100-step refit runs
+               on a second stream into the idle table slot, overlapping the
+               next blocks; the slot becomes current at the first block that
+               starts after the refit has finished.
+    The learned figures include the fitting.  An untimed pass then compares
+    the learned output of every block with the radix output bit for bit."""
     import torch
     import fcb200
     from fcb200 import _native as nat
@@ -661,84 +727,153 @@ def bench_c5(dev, T=5000, N=8000, F=128, Tb=250, seed=20261206):
     state = [torch.zeros(F, device=dev), torch.zeros(F, device=dev),
              torch.from_numpy(rng.integers(0, int(0.2 * T), N)).to(dev)]
     blocks = [make_c5_block(dev, g, rng, state, F, Tb, N, b * Tb) for b in range(T // Tb)]
+    nb = len(blocks)
     torch.cuda.synchronize(dev)
     stream = torch.cuda.current_stream(dev)
+    side = torch.cuda.Stream(dev)
     s = stream.cuda_stream
-    ranks_r = torch.empty((F, Tb, N), dtype=torch.float32, device=dev)
-    ranks_l = torch.empty_like(ranks_r)
-    ic_r = torch.empty((F, Tb), dtype=torch.float64, device=dev)
-    ic_l = torch.empty_like(ic_r)
-    stats = torch.zeros((F, Tb, 4), dtype=torch.int32, device=dev)
-    model = fcb200.CdfModel(F, seed=seed)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    t_radix = t_radix_lb = t_learn = t_fit = 0.0
-    exact = True
-    codes = []
-    learned_cells = 0
-    for b, (X, R, fm, rm) in enumerate(blocks):
-        ev[0].record(stream)
+    ranks = torch.empty((F, Tb, N), dtype=torch.float32, device=dev)
+    ranks2 = torch.empty_like(ranks)
+    ic = torch.empty((F, Tb), dtype=torch.float64, device=dev)
+    stats = torch.zeros((nb, F, Tb, 4), dtype=torch.int32, device=dev)
+
+    def radix(X, R, fm, rm, out):
         nat.check(lib.fcb_dev_rank_ic_panel(X.data_ptr(), R.data_ptr(), fm.data_ptr(), rm.data_ptr(), F, Tb, N,
-                                            MIN_VALID, ranks_r.data_ptr(), ic_r.data_ptr(), 0, s), "radix")
-        ev[1].record(stream)
-        if b >= 2:
-            nat.check(lib.fcb_dev_rank_ic_panel_learned(X.data_ptr(), R.data_ptr(), fm.data_ptr(), rm.data_ptr(), F,
-                                                        Tb, N, MIN_VALID, ranks_l.data_ptr(), ic_l.data_ptr(),
-                                                        model.handle, 64, stats.data_ptr(), s), "learned")
-        ev[2].record(stream)
-        # fit on the exact ranks of this block: dates [0, 500) first, then a refit per block
-        if b == 0:
-            model.fit(X, ranks_r, Tb, N, 0, Tb, steps=1500, lr=3e-3, stream=s)
-        else:
-            model.fit(X, ranks_r, Tb, N, 0, Tb, steps=300 if b == 1 else 100, lr=1e-3, stream=s)
-        ev[3].record(stream)
-        torch.cuda.synchronize(dev)
-        t_radix += ev[0].elapsed_time(ev[1])
-        t_fit += ev[2].elapsed_time(ev[3])
-        if b >= 2:
-            t_learn += ev[1].elapsed_time(ev[2])
-            t_radix_lb += ev[0].elapsed_time(ev[1])
-            learned_cells += F * Tb * N
-            exact = exact and bool(torch.equal(ranks_l.view(torch.int32), ranks_r.view(torch.int32))) and \
-                bool(torch.equal(torch.nan_to_num(ic_l, nan=7.0), torch.nan_to_num(ic_r, nan=7.0)))
-            codes.append(stats[..., 0].flatten().cpu().numpy())
-    codes = np.concatenate(codes)
+                                            MIN_VALID, out.data_ptr(), ic.data_ptr(), 0, s), "radix")
+
+    def learned(model, b, X, R, fm, rm, out):
+        nat.check(lib.fcb_dev_rank_ic_panel_learned(X.data_ptr(), R.data_ptr(), fm.data_ptr(), rm.data_ptr(), F,
+                                                    Tb, N, MIN_VALID, out.data_ptr(), ic.data_ptr(), model.handle,
+                                                    64, stats[b].data_ptr(), s), "learned")
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    # ---- radix run (per-block events for the same-blocks comparison)
+    bev = [torch.cuda.Event(enable_timing=True) for _ in range(nb + 1)]
+    bev[0].record(stream)
+    for b, (X, R, fm, rm) in enumerate(blocks):
+        radix(X, R, fm, rm, ranks)
+        bev[b + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    t_radix = bev[0].elapsed_time(bev[nb])
+    t_radix_lb = bev[2].elapsed_time(bev[nb])
+    # ---- learned run, fitting included
+    model = fcb200.CdfModel(F, seed=seed)
+    fit_done = torch.cuda.Event()
+    inflight = False
+    refits = swaps = 0
+    ev[0].record(stream)
+    for b, (X, R, fm, rm) in enumerate(blocks):
+        if b < 2:
+            radix(X, R, fm, rm, ranks)
+            model.fit(X, ranks, Tb, N, 0, Tb, steps=1500 if b == 0 else 300, lr=3e-3 if b == 0 else 1e-3, stream=s)
+            if b == 1:
+                ev[1].record(stream)
+            continue
+        if inflight and fit_done.query():
+            model.swap()
+            swaps += 1
+            inflight = False
+        learned(model, b, X, R, fm, rm, ranks)
+        if not inflight:
+            model.sample(X, ranks, Tb, N, 0, Tb, stream=s)
+            side.wait_stream(stream)
+            model.train(100, 1e-3, into_idle=True, stream=side.cuda_stream)
+            fit_done.record(side)
+            inflight = True
+            refits += 1
+    stream.wait_stream(side)
+    ev[2].record(stream)
+    torch.cuda.synchronize(dev)
+    if inflight:
+        model.swap()
+    t_learn_all = ev[0].elapsed_time(ev[2])
+    t_learn_lb = ev[1].elapsed_time(ev[2])
+    t_fit0 = ev[0].elapsed_time(ev[1])
+    codes = stats[2:, ..., 0].flatten().cpu().numpy()
+    # ---- untimed exactness pass: learned (final model) vs radix, every block
+    exact = True
+    for b, (X, R, fm, rm) in enumerate(blocks):
+        if b < 2:
+            continue
+        radix(X, R, fm, rm, ranks)
+        ic_r = ic.clone()
+        learned(model, b, X, R, fm, rm, ranks2)
+        exact = exact and bool(torch.equal(ranks.view(torch.int32), ranks2.view(torch.int32))) and \
+            bool(torch.equal(torch.nan_to_num(ic_r, nan=7.0), torch.nan_to_num(ic, nan=7.0)))
+    torch.cuda.synchronize(dev)
+    lb_cells = F * (T - 2 * Tb) * N
     res = {"workload": f"learned splitters, streaming: T={T}, N={N}, F={F} ({F * T * N / 1e9:.2f} G cells, "
                        f"{F * T * N * 4 / 1e9:.1f} GB f32), blocks of {Tb} dates; fit on dates [0, {2 * Tb}), "
-                       f"refit after every block",
-           "learned_gelem_s": learned_cells / (t_learn / 1e3) / 1e9,
+                       f"refit after every block, overlapped",
            "radix_gelem_s": F * T * N / (t_radix / 1e3) / 1e9,
-           "speedup_vs_radix": (t_radix_lb / t_learn) if t_learn > 0 else None,
+           "learned_incl_fit_gelem_s": F * T * N / (t_learn_all / 1e3) / 1e9,
+           "learned_blocks_gelem_s": lb_cells / (t_learn_lb / 1e3) / 1e9,
+           "radix_same_blocks_gelem_s": lb_cells / (t_radix_lb / 1e3) / 1e9,
+           "speedup_vs_radix_same_blocks_incl_refits": t_radix_lb / t_learn_lb,
+           "speedup_vs_radix_whole_run_incl_all_fits": t_radix / t_learn_all,
+           "initial_fit_and_radix_blocks_ms": t_fit0, "refits_overlapped": refits, "table_swaps": swaps,
            "learned_fraction": float((codes == 1).mean()),
            "fallback_overflow": float((codes == 2).mean()), "fallback_judge": float((codes == 3).mean()),
            "fallback_scale": float((codes == 4).mean()),
-           "bit_exact_vs_radix": exact, "fit_ms_total": t_fit,
-           "cells_ranked_learned": learned_cells}
+           "bit_exact_vs_radix": exact}
+    if cpu_sample:
+        from oracle import fc_oracle as O
+        X, R, fm, rm = blocks[2]
+        nd = 16
+        Xh, Rh = X[:, :nd].cpu().numpy(), R[:nd].cpu().numpy()
+        fmh, rmh = fm[:nd].cpu().numpy().astype(bool), rm[:nd].cpu().numpy().astype(bool)
+        t0 = time.perf_counter()
+        for f in range(F):
+            O.cs_rank(Xh[f], fmh, False)
+            O.rolling_ic(Xh[f], Rh, fmh, rmh, MIN_VALID)
+        el = time.perf_counter() - t0
+        v = Xh.size / el / 1e9
+        res["cpu_baseline"] = {"value": v, "unit": "Gelem/s", "cores": 1, "kind": "port",
+                               "sample": f"{nd} dates x {F} factors x {N} stocks of block 2 ({el:.1f} s, "
+                                         "np_cs_rank + np_rolling_ic); the whole panel extrapolates to "
+                                         f"{F * T * N / v / 1e9 / 60:.0f} min"}
     del blocks
     torch.cuda.empty_cache()
     return res
 
 
-def bench_stock_corr(dev, N, T=1218, steps=5, warmup=2):
+def bench_stock_corr(dev, N, T=1218, steps=5, warmup=2, oracle=True):
     """stock_corr precision forms on one (T,N) panel, device-resident:
-    BF16x3 tensor-core path vs plain FP32, error against the f64 path."""
+    BF16x3 tensor-core path vs plain FP32, each against the oracle's
+    np_stock_corr restatement (FP64), which is also timed on the host as the
+    CPU baseline; the FP64 drop-in's distance to the oracle is reported too."""
     import torch
     from fcb200 import _native as nat
     lib = nat.lib()
     X, mask = make_stock_panel(T=T, N=N)
     m8 = mask.astype(np.uint8)
-    ref = np.empty((N, N))
-    nat.check(lib.fcb_stock_corr(nat.ptr(X), 0, nat.ptr(m8), T, N, nat.ptr(ref), None, None), "fcb_stock_corr")
+    f64 = np.empty((N, N))
+    nat.check(lib.fcb_stock_corr(nat.ptr(X), 0, nat.ptr(m8), T, N, nat.ptr(f64), None, None), "fcb_stock_corr")
+    alg_flops = 4 * 2.0 * N * N * T           # X.X^T, X.M^T, X^2.M^T, M.M^T (dense-equivalent)
+    res = {"N": N, "T": T, "algorithmic_gflop": alg_flops / 1e9}
+    if oracle:
+        from oracle import fc_oracle as O
+        t0 = time.perf_counter()
+        ref = O.stock_corr(X, mask)
+        cpu_s = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": alg_flops / cpu_s / 1e12, "unit": "TFLOP/s", "ms": cpu_s * 1e3,
+                               "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"the whole (T={T}, N={N}) panel, oracle np_stock_corr (numpy, "
+                                         "OpenBLAS GEMMs on every core)"}
+        res["error_reference"] = "oracle (numpy FP64 restatement of np_stock_corr)"
+        res["f64_dropin_max_abs_err_vs_oracle"] = float(np.nanmax(np.abs(f64 - ref)))
+    else:
+        ref = f64
+        res["error_reference"] = "FP64 drop-in path (fcb_stock_corr)"
     dX = torch.from_numpy(X).to(dev)
     dM = torch.from_numpy(m8).to(dev)
     dO = torch.empty((N, N), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
     ws = lib.fcb_workspace_create()
-    alg_flops = 4 * 2.0 * N * N * T           # X.X^T, X.M^T, X^2.M^T, M.M^T (dense-equivalent)
     Tp = (T + 31) // 32 * 32
     n_i = (N + 127) // 128
     tiles = sum(1 for ti in range(n_i) for tj in range((N + 31) // 32) if tj * 32 + 31 >= ti * 128)
     exec_flops = tiles * (Tp // 16) * 2.0 * 128 * 704 * 16   # issued MMA work (N-total 704 per 16 dates)
-    res = {"N": N, "T": T, "algorithmic_gflop": alg_flops / 1e9}
     out = {}
     for name, mode in (("bf16x3", 0), ("fp32", 1)):
         def call():
@@ -759,7 +894,7 @@ def bench_stock_corr(dev, N, T=1218, steps=5, warmup=2):
         err = np.abs(got - ref)
         same_nan = bool(np.array_equal(np.isnan(got), np.isnan(ref)))
         d = {"ms": ms, "tflops_algorithmic": alg_flops / (ms / 1e3) / 1e12,
-             "max_abs_err_vs_f64": float(np.nanmax(err)), "mean_abs_err_vs_f64": float(np.nanmean(err)),
+             "max_abs_err": float(np.nanmax(err)), "mean_abs_err": float(np.nanmean(err)),
              "nan_pattern_matches": same_nan}
         if mode == 0:
             d["tflops_mma_issued"] = exec_flops / (ms / 1e3) / 1e12
@@ -770,20 +905,46 @@ def bench_stock_corr(dev, N, T=1218, steps=5, warmup=2):
     return res
 
 
-def check_spot(X, R, fm, rm, dranks, dic):
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).view(np.uint8)).hexdigest()
+
+
+def oracle_c2(X, R, fm, rm, scan_planes=(0, 6), threads=None):
+    """The oracle's results on the whole panel: cs ranks (as digests of their
+    bit patterns) and IC of every factor, all four parameter_scan groups of
+    `scan_planes`, and factor_corr.  Computed in a thread pool (numpy releases
+    the GIL inside its sorts and GEMMs)."""
+    from concurrent.futures import ThreadPoolExecutor
     from oracle import fc_oracle as O
-    F, T, N = X.shape
-    ts = [0, T // 2, T - 1]
-    ok = True
-    for f in (0, F - 1):
-        sl = slice(ts[1], ts[1] + 2)
-        exp_r = O.cs_rank(X[f, sl], fm[sl].astype(bool), False)
-        got_r = dranks[f, sl].cpu().numpy()
-        ok &= bool(np.array_equal(exp_r.view(np.uint32), got_r.view(np.uint32)))
-        exp_ic = O.rolling_ic(X[f, sl], R[sl], fm[sl].astype(bool), rm[sl].astype(bool), MIN_VALID)
-        got_ic = dic[f, sl].cpu().numpy()
-        ok &= bool(np.array_equal(np.nan_to_num(exp_ic, nan=7.0), np.nan_to_num(got_ic, nan=7.0)))
-    return "bit-exact" if ok else "MISMATCH"
+    F = X.shape[0]
+    fmb, rmb = fm.astype(bool), rm.astype(bool)
+    threads = threads or max(1, min(16, os.cpu_count() or 1))
+
+    def rank_ic(f):
+        return _sha(O.cs_rank(X[f], fmb, False)), O.rolling_ic(X[f], R, fmb, rmb, MIN_VALID)
+
+    def scan(f):
+        return [_sha(g) for g in O.parameter_scan(X[f], fmb)]
+
+    def fcorr():
+        return O.factor_corr(np.ascontiguousarray(np.moveaxis(X, 0, -1)), fmb)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        fc_fut = ex.submit(fcorr)
+        sc_fut = {f: ex.submit(scan, f) for f in scan_planes}
+        ri = list(ex.map(rank_ic, range(F)))
+        res = {"rank_sha": [a for a, _ in ri], "ic": np.stack([b for _, b in ri]),
+               "scan_sha": {f: v.result() for f, v in sc_fut.items()}, "factor_corr": fc_fut.result()}
+    res["seconds"] = time.perf_counter() - t0
+    return res
+
+
+def ic_bitwise(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return a.shape == b.shape and bool(np.array_equal(np.isnan(a), np.isnan(b))) and \
+        bool(np.array_equal(a[~np.isnan(a)].view(np.uint64), b[~np.isnan(b)].view(np.uint64)))
 
 
 def run_reference(args):
@@ -824,6 +985,7 @@ def main():
     ap.add_argument("--no-stock-corr", action="store_true", help="skip the stock_corr precision-form leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--no-parity", action="store_true", help="skip the whole-panel oracle comparison")
     ap.add_argument("--only-stock-corr", type=int, default=0, metavar="N",
                     help="run only the stock_corr precision leg at this N (profiling)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-panel leg")
@@ -843,11 +1005,11 @@ def main():
     if args.only_stock_corr:
         import torch
         print(json.dumps(bench_stock_corr(torch.device("cuda", 0), args.only_stock_corr, steps=args.steps,
-                                          warmup=args.warmup)))
+                                          warmup=args.warmup, oracle=not args.no_cpu_baseline)))
         return
     if args.only_c5:
         import torch
-        print(json.dumps(bench_c5(torch.device("cuda", 0))))
+        print(json.dumps(bench_c5(torch.device("cuda", 0), cpu_sample=not args.no_cpu_baseline)))
         return
     if args.only_batch:
         import torch
@@ -873,7 +1035,7 @@ def main():
         p = ROOT / "MEASURED_PEAKS.json"
         if p.exists():
             peak_bf16 = float(json.loads(p.read_text())["bf16_tflops"])
-        sc = [bench_stock_corr(dev, N) for N in (2000, 5000)]
+        sc = [bench_stock_corr(dev, N, oracle=not args.no_cpu_baseline) for N in (2000, 5000)]
         for r in sc:
             if peak_bf16:
                 r["bf16x3"]["tensor_frac_of_measured_bf16_peak"] = r["bf16x3"]["tflops_mma_issued"] / peak_bf16
@@ -882,10 +1044,12 @@ def main():
                              "bf16_peak_tflops_measured": peak_bf16, "results": sc}
     if not args.no_batch:
         import torch
-        res["batch"] = bench_batch(torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+        res["batch"] = bench_batch(torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))),
+                                   cpu_sample=not args.no_cpu_baseline)
     if not args.no_c5:
         import torch
-        res["c5_learned_streaming"] = bench_c5(torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+        res["c5_learned_streaming"] = bench_c5(torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))),
+                                               cpu_sample=not args.no_cpu_baseline)
     if rank == 0:
         if not args.no_cpu_baseline:
             X, R, fm, rm = make_panel()

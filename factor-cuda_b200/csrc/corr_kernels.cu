@@ -1009,7 +1009,7 @@ __global__ void k_fc_fallback(const TIN* __restrict__ X, const uint8_t* __restri
 // form to rounding (the reference's multi-block kahan_reduce kernels,
 // src/factor_corr.cu:188-322, split the rows the same way).
 constexpr int kFbThreads = 256;
-constexpr int kFbP1 = 9;  // n, sx.s, sx.c, sy.s, sy.c, min x, max x, min y, max y
+constexpr int kFbP1 = kFcFbPartDoubles;  // n, sx.s, sx.c, sy.s, sy.c, min x, max x, min y, max y
 constexpr int kFbP2 = 6;  // sxx.s, sxx.c, syy.s, syy.c, sxy.s, sxy.c
 
 FCB_DEV void fb_tree_kahan(double (*sh)[kFbThreads], int q0, int nq) {
@@ -1285,7 +1285,7 @@ size_t fc_fb_part_doubles(long long R, int F) {
 int fc_fb_nblk(long long R, int F) {
   const int maxpairs = F * (F - 1) / 2 > 0 ? F * (F - 1) / 2 : 1;
   long long nb = R / 32768;
-  nb = std::min<long long>(nb, 64);
+  nb = std::min<long long>(nb, kFcFbMaxNblk);
   nb = std::min<long long>(nb, 65536 / maxpairs);
   return static_cast<int>(std::max<long long>(nb, 1));
 }

@@ -70,8 +70,11 @@ inline int fc_gram_blocks(long long R, int F) {
   if (nb < 1) nb = 1;
   return static_cast<int>(nb < cap ? nb : cap);
 }
-// Row blocks per flagged pair of the multi-block fallback, and the partials
-// buffer it needs (doubles).
+// Row blocks per flagged pair of the multi-block fallback (at most
+// kFcFbMaxNblk), and the partials buffer it needs (doubles): kFcFbPartDoubles
+// per pair and block plus 4 per pair.
+constexpr int kFcFbMaxNblk = 64;
+constexpr int kFcFbPartDoubles = 9;
 int fc_fb_nblk(long long R, int F);
 size_t fc_fb_part_doubles(long long R, int F);
 

@@ -54,58 +54,69 @@ def _dtype_ok(dt, dtypes):
     return dt in allowed
 
 
+def _dtype_error(name, dt):
+    return ValueError(f"{name}: dtype {dt} is not accepted (float32 or float64 only)")
+
+
 def _to_numpy(x, *, name, ndim, dtypes="f32f64", downcast_to=None):
+    """Host copy of a numpy array, torch tensor or DLPack capsule, with the
+    container kind and device it came from.  The input rules are the fc
+    adapter's (fc/_util.py:79-136): float32/float64 only (ValueError), a
+    DLPack capsule is single-use (ValueError on re-use), anything else is a
+    TypeError; f64 is rounded to f32 (nearest-even) when downcast_to asks."""
     kind, device = "numpy", "cpu"
     if isinstance(x, np.ndarray):
         if not _dtype_ok(x.dtype, dtypes):
-            raise ValueError(f"{name} dtype {x.dtype} not in whitelist {{float32,float64}}")
+            raise _dtype_error(name, x.dtype)
         arr = np.ascontiguousarray(x)
     elif _torch is not None and isinstance(x, _torch.Tensor):
         kind = "torch"
         device = "cpu" if not x.is_cuda else f"cuda:{x.device.index}"
         x = x.detach()
         if not _dtype_ok(x.dtype, dtypes):
-            raise ValueError(f"{name} dtype {x.dtype} not in whitelist {{float32,float64}}")
+            raise _dtype_error(name, x.dtype)
         arr = x.contiguous().cpu().numpy()
     else:
         if _torch is None:
-            raise TypeError(f"{name} must be a numpy array or torch.Tensor")
+            raise TypeError(f"{name}: pass a numpy array or a torch tensor")
         try:
             t = _torch.utils.dlpack.from_dlpack(x)
         except (RuntimeError, TypeError, AttributeError):
             if type(x).__name__ == "PyCapsule":
-                raise ValueError(f"{name}: DLPack capsule already consumed") from None
-            raise TypeError(f"{name} must be a numpy array, torch.Tensor, or DLPack capsule") from None
+                raise ValueError(f"{name}: this DLPack capsule was consumed by an earlier call") from None
+            raise TypeError(f"{name}: pass a numpy array, a torch tensor or a DLPack capsule") from None
         kind = "dlpack"
         device = "cpu" if not t.is_cuda else f"cuda:{t.device.index}"
         if not _dtype_ok(t.dtype, dtypes):
-            raise ValueError(f"{name} dtype {t.dtype} not in whitelist {{float32,float64}}")
+            raise _dtype_error(name, t.dtype)
         arr = t.detach().contiguous().cpu().numpy()
     ok = arr.ndim == ndim if isinstance(ndim, int) else arr.ndim in ndim
     if not ok:
-        raise ValueError(f"{name} must be {ndim}-D, got ndim={arr.ndim}")
+        raise ValueError(f"{name}: expected a {ndim}-D array, got {arr.ndim}-D")
     if downcast_to == "float32" and arr.dtype == np.float64:
         arr = arr.astype(np.float32)  # IEEE round-to-nearest-even
     return kind, device, np.ascontiguousarray(arr)
 
 
 def _check_mask(mask, *, name, T, N, allow_none=True):
+    """A (T,N) boolean mask as a host array (None passes through when
+    allowed).  Masks are strictly bool (the mask alone decides validity)."""
     if mask is None:
         if allow_none:
             return None
-        raise ValueError(f"{name} is required")
+        raise ValueError(f"{name}: a mask is needed here")
     if isinstance(mask, np.ndarray):
         if mask.dtype != np.bool_:
-            raise ValueError(f"{name} must be bool, got {mask.dtype}")
+            raise ValueError(f"{name}: masks are bool arrays, this one is {mask.dtype}")
         arr = np.ascontiguousarray(mask)
     elif _torch is not None and isinstance(mask, _torch.Tensor):
         if mask.dtype != _torch.bool:
-            raise ValueError(f"{name} must be bool, got {mask.dtype}")
+            raise ValueError(f"{name}: masks are bool tensors, this one is {mask.dtype}")
         arr = mask.detach().cpu().numpy()
     else:
-        raise TypeError(f"{name} must be a bool numpy array or torch.Tensor")
+        raise TypeError(f"{name}: pass a bool numpy array or torch tensor")
     if arr.shape != (T, N):
-        raise ValueError(f"{name} shape must be (T,N) matching input, got {arr.shape}")
+        raise ValueError(f"{name}: shape {arr.shape} does not match the input's (T,N) = {(T, N)}")
     return arr
 
 
@@ -315,35 +326,40 @@ def factor_plane(factors, f):
     return _make_output(plane, kind, device)
 
 
-_AXES = ("direction", "mask_mode")
-_DIR = ("ascending", "descending")
-_MM = ("masked", "unmasked")
-_BINDING_INDEX = {"ascending": {"masked": 0, "unmasked": 1},
-                  "descending": {"masked": 2, "unmasked": 3}}
+# parameter_scan axes: the values each accepts and the one used when the
+# caller leaves the axis out, in the canonical order of the effective spec
+# (the rules of fc/parameter_scan.py:26-58).
+_SCAN_AXES = {"direction": (("ascending", "descending"), "ascending"),
+              "mask_mode": (("masked", "unmasked"), "masked")}
+# position of each (direction, mask_mode) group in the binding's four outputs
+_BINDING_INDEX = {("ascending", "masked"): 0, ("ascending", "unmasked"): 1,
+                  ("descending", "masked"): 2, ("descending", "unmasked"): 3}
 
 
 def _normalize_axes(axes):
-    if not isinstance(axes, (list, tuple)) or not all(
-            isinstance(a, (list, tuple)) and len(a) == 2 for a in axes):
-        raise ValueError("axes must be a list of (axis_name, values_list) tuples")
-    user, seen = {}, set()
-    for name, vals in axes:
-        if name not in _AXES:
-            raise ValueError(f"unknown scan axis {name!r}; allowed: direction, mask_mode")
-        if name in seen:
-            raise ValueError(f"duplicate axis {name!r}")
-        seen.add(name)
+    """Validate a parameter_scan axis list and expand it into the effective
+    spec (every axis, canonical order, defaults filled in) and the groups
+    (direction-major product of the values).  Any malformed, unknown,
+    repeated or empty axis, or an unknown or repeated value, is a ValueError."""
+    pairs = list(axes) if isinstance(axes, (list, tuple)) else None
+    if pairs is None or any(not isinstance(p, (list, tuple)) or len(p) != 2 for p in pairs):
+        raise ValueError("parameter_scan: axes must be a sequence of (name, values) pairs")
+    given = {}
+    for name, vals in pairs:
+        if name not in _SCAN_AXES:
+            raise ValueError(f"parameter_scan: {name!r} is not a scan axis (known: {', '.join(_SCAN_AXES)})")
+        if name in given:
+            raise ValueError(f"parameter_scan: axis {name!r} is given more than once")
         if not isinstance(vals, (list, tuple)) or len(vals) == 0:
-            raise ValueError(f"axis {name!r} values must be non-empty")
-        if len(set(vals)) != len(vals):
-            raise ValueError(f"axis {name!r} contains duplicate values")
-        if name == "direction" and not set(vals) <= set(_DIR):
-            raise ValueError(f"direction values must be in {_DIR}")
-        if name == "mask_mode" and not set(vals) <= set(_MM):
-            raise ValueError(f"mask_mode values must be in {_MM}")
-        user[name] = list(vals)
-    eff = {"direction": user.get("direction", ["ascending"]),
-           "mask_mode": user.get("mask_mode", ["masked"])}
+            raise ValueError(f"parameter_scan: axis {name!r} needs at least one value")
+        if len(set(vals)) < len(vals):
+            raise ValueError(f"parameter_scan: axis {name!r} repeats a value in {list(vals)}")
+        allowed = _SCAN_AXES[name][0]
+        unknown = [v for v in vals if v not in allowed]
+        if unknown:
+            raise ValueError(f"parameter_scan: {unknown} not allowed for axis {name!r} (allowed: {allowed})")
+        given[name] = list(vals)
+    eff = {name: given.get(name, [default]) for name, (_, default) in _SCAN_AXES.items()}
     return eff, [(d, m) for d in eff["direction"] for m in eff["mask_mode"]]
 
 
@@ -362,8 +378,8 @@ def parameter_scan(axes, X, mask=None):
     m = (_check_mask(mask, name="mask", T=T, N=N, allow_none=False) if any_masked
          else np.ones((T, N), dtype=np.bool_))
     active = [0, 0, 0, 0]
-    for d, mm in combos:
-        active[_BINDING_INDEX[d][mm]] = 1
+    for combo in combos:
+        active[_BINDING_INDEX[combo]] = 1
     _sync_entry(device)
     t0 = time.perf_counter()
     with _SCAN_CACHE.use((T, N)) as ws:
@@ -383,8 +399,8 @@ def _parameter_scan_dev(effective, combos, X, mask):
     any_masked = any(mm == "masked" for _, mm in combos)
     m = _dev_mask(mask, name="mask", T=T, N=N, device=x.device, allow_none=False) if any_masked else None
     active = [0, 0, 0, 0]
-    for d, mm in combos:
-        active[_BINDING_INDEX[d][mm]] = 1
+    for combo in combos:
+        active[_BINDING_INDEX[combo]] = 1
     nact = sum(active)
     outs = [_torch.empty((T, N), dtype=_torch.float32, device=x.device) if a else None for a in active]
     optrs = (C.c_void_p * 4)(*[nat.ptr(o) for o in outs])
@@ -411,29 +427,31 @@ def _parameter_scan_dev(effective, combos, X, mask):
 
 
 def _scan_result(effective, combos, r, elapsed_ms):
+    """The parameter_scan record (schema of fc/parameter_scan.py:101-132) from
+    the binding's four group outputs: one entry per requested group, in
+    request order.  Status 0 is a finished group; 9 and 701 (launch
+    failures the contract confines to one group) mark that group failed with
+    zero time; any other status fails the whole scan with RuntimeError."""
     groups = []
     for gi, (d, mm) in enumerate(combos):
-        g = _BINDING_INDEX[d][mm]
+        g = _BINDING_INDEX[(d, mm)]
         st = r["group_status"][g]
+        entry = {"group_index": gi, "axis_values": {"direction": d, "mask_mode": mm}}
         if st == 0:
-            groups.append({"group_index": gi, "axis_values": {"direction": d, "mask_mode": mm},
-                           "result": r["groups"][g], "status": "ok", "error": None,
-                           "error_stage": None, "time_ms": r["time_ms"][g],
-                           "time_gpu_ms": r["time_gpu_ms"][g]})
+            entry.update(result=r["groups"][g], status="ok", error=None, error_stage=None,
+                         time_ms=r["time_ms"][g], time_gpu_ms=r["time_gpu_ms"][g])
         elif st in (9, 701):
-            groups.append({"group_index": gi, "axis_values": {"direction": d, "mask_mode": mm},
-                           "result": None, "status": "failed",
-                           "error": f"group-level CUDA error {st}", "error_stage": "launch",
-                           "time_ms": 0.0, "time_gpu_ms": 0.0})
+            entry.update(result=None, status="failed", error=f"launch of this group failed: CUDA status {st}",
+                         error_stage="launch", time_ms=0.0, time_gpu_ms=0.0)
         else:
-            raise RuntimeError(f"non-whitelist CUDA status {st} for group {g} "
-                               "(must be scan-level, not group-failed)")
-    ok = [g for g in groups if g["status"] == "ok"]
+            raise RuntimeError(f"parameter_scan: CUDA status {st} (group {g}) is not a per-group failure")
+        groups.append(entry)
+    done = [g for g in groups if g["status"] == "ok"]
     return {"spec": effective, "groups": groups,
             "summary": {"total_groups": len(combos),
-                        "n_failed": sum(1 for g in groups if g["status"] == "failed"),
-                        "total_time_ms": sum(g["time_ms"] for g in ok),
-                        "total_time_gpu_ms": sum(g["time_gpu_ms"] for g in ok),
+                        "n_failed": len(groups) - len(done),
+                        "total_time_ms": sum(g["time_ms"] for g in done),
+                        "total_time_gpu_ms": sum(g["time_gpu_ms"] for g in done),
                         "elapsed_ms": elapsed_ms}}
 
 

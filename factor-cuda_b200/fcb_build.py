@@ -80,8 +80,12 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         objs = list(ex.map(compile_one, CU_SOURCES))
     lib = lib_path()
     if force or _stale(lib, objs):
-        _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(lib), *map(str, objs),
+        # link to a temporary name and rename: a process that loads the
+        # library meanwhile sees the old file or the new one, never a partial one
+        tmp = lib.with_name(lib.name + ".tmp")
+        _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(tmp), *map(str, objs),
               "-cudart", "static"])
+        os.replace(tmp, lib)
         if verbose:
             print(f"  link {lib.name}")
 
@@ -91,9 +95,11 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         out = BUILD / (mod + ext_suffix())
         s = CSRC / src
         if force or _stale(out, [s, lib] + hdrs):
+            tmp = out.with_name(out.name + ".tmp")
             _run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
                   "-I", py_inc, "-I", pybind11.get_include(), "-I", str(INCLUDE),
-                  str(s), "-o", str(out), "-L", str(BUILD), "-lfcb200", "-Wl,-rpath,$ORIGIN"])
+                  str(s), "-o", str(tmp), "-L", str(BUILD), "-lfcb200", "-Wl,-rpath,$ORIGIN"])
+            os.replace(tmp, out)
             if verbose:
                 print(f"  g++ {out.name}")
     return lib

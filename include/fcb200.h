@@ -319,19 +319,23 @@ int fcb_dev_factor_corr_bf16x3(const float* d_x, const uint8_t* d_mask, int T, i
  * No counterpart in the reference.  factor_corr for callers that cannot let a
  * library allocate device memory: applications whose device memory belongs to
  * a framework pool or a hard budget, and latency-sensitive loops that cannot
- * take the device-wide synchronisation of cudaMalloc/cudaFree.  Same kernels
- * and results (within 1e-12) as fcb_factor_corr, on caller-owned DEVICE
- * buffers: d_x (T,N,F) f32/f64, d_mask (T,N) or NULL, d_out (F,F) f64;
- * asynchronous on `stream` (NULL = legacy stream).
- * All scratch lives in one fixed device array of about 2.6 MB inside the
- * library, which every GPU that loads the library holds until exit; no
- * cudaMalloc/cudaFree or allocating library routine is called.  F is limited
- * to FCB_NOALLOC_MAX_F (larger F returns FCB_ERR_NOALLOC_CAP).  The first
- * call on each device resolves the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  Every call shares the one array: calls that
- * overlap on the GPU (concurrent streams or threads) race and must be
- * serialised by the caller. */
+ * take the device-wide synchronisation of cudaMalloc/cudaFree.  The
+ * factor_corr kernels of fcb_dev_factor_corr on caller-owned DEVICE buffers:
+ * d_x (T,N,F) f32/f64, d_mask (T,N) or NULL, d_out (F,F) f64; asynchronous on
+ * `stream` (NULL = legacy stream).  Its row partition is fixed (148 column /
+ * 74 Gram blocks) where fcb_dev_factor_corr sizes it from the pool, so partial
+ * sums are added in another order: results agree with fcb_factor_corr within
+ * 1e-12 per output, not bit for bit.
+ * All scratch -- the multi-block fallback's partials included -- lives in one
+ * fixed device array of about 4.9 MB inside the library, which every GPU that
+ * loads the library holds until exit; no cudaMalloc/cudaFree or allocating
+ * library routine is called.  F is limited to FCB_NOALLOC_MAX_F (larger F
+ * returns FCB_ERR_NOALLOC_CAP).  Each call resolves the array's device
+ * address on the current device (cudaGetSymbolAddress); the first call on a
+ * device also loads the library's device image there, so make it before any
+ * stream capture.  Every call shares the one array: calls that overlap on the
+ * GPU (concurrent streams or threads) race and must be serialised by the
+ * caller. */
 #define FCB_NOALLOC_MAX_F 32
 int fcb_dev_factor_corr_noalloc(const void* d_x, int dtype, const uint8_t* d_mask, int T, int N, int F,
                                 double* d_out, void* stream);

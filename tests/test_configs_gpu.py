@@ -10,7 +10,8 @@ oracle (itself pinned to the reference CPU path by test_oracle_pins.py).
   dates [0, 250)) bitwise on every (factor, date); all four parameter_scan
   groups of three planes bitwise; factor_corr (12x12) within 1e-12 of the
   oracle's np_factor_corr restatement, on the reference's (T,N,F) layout and
-  on the device-resident factor planes.
+  on the device-resident factor planes, and its BF16x3 tensor-core form
+  within 1e-6 of the oracle per output.
 * C3 -- stock_corr at N=2000, T=1218: the FP64 drop-in within 1e-12 of the
   oracle's np_stock_corr restatement; the BF16x3 tensor-core form within
   1e-6 and the FP32 form within 5e-5 of the oracle (absolute, per output).
