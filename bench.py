@@ -627,17 +627,23 @@ def bench_batch(dev, steps=5, warmup=2, tune_cache=None, cpu_sample=True):
                torch.equal(torch.nan_to_num(c, nan=7.0), torch.nan_to_num(p["corr"], nan=7.0)) and
                torch.equal(r.view(torch.int32), p["ranks"][:, :3].view(torch.int32))
                for a, c, r, p in zip(ic_g, corr_g, rk_g, panels))
-    classes = sorted({0 if p["X"].shape[2] <= cfg["nt_small_max"] else (1 if p["X"].shape[2] <= cfg["nt_mid_max"]
-                                                                           else 2) for p in panels})
+    def variant(n):  # the f32 kernel variant a panel of width n runs in (fcb200.h, batched panels)
+        if n <= min(cfg["nt_small_max"], 2048):
+            return 0
+        if n <= min(cfg["nt_mid_max"], 5120):
+            return 1
+        return 2 if n <= 8192 else 3
+    variants = sorted({variant(p["X"].shape[2]) for p in panels})
     res = {"workload": "64 uneven panels (N ~ U[300,6000], T ~ U[250,2500], F=8, gaps ~ U[0,0.2]): "
                        "cs_rank + rolling_ic(30) + factor_corr per panel",
            "cells": cells, "unit": "Gelem/s",
-           # kernels: one persistent rank + IC kernel per size class; per panel, factor_corr's
-           # column pass + merge, Gram + finalize and the four fallback kernels (launched for
-           # every pool of 4096 rows or more; they exit at once when no pair is flagged); the
-           # per-panel arm ranks through the returns kernel + per-(date, factor) kernel (F >= 2)
+           # kernels: per kernel variant, the returns pass and the rank pass over all its
+           # panels; per panel, factor_corr's column pass + merge, Gram + finalize and the
+           # four fallback kernels (launched for every pool of 4096 rows or more; they exit at
+           # once when no pair is flagged); the per-panel arm runs the returns kernel and the
+           # per-(date, factor) kernel of each panel (F >= 2)
            "graph": {"ms": ms_graph, "value": cells / (ms_graph / 1e3) / 1e9,
-                     "kernels_per_replay": len(classes) + 8 * len(panels)},
+                     "kernels_per_replay": 2 * len(variants) + 8 * len(panels)},
            "per_panel": {"ms": ms_pp, "value": cells / (ms_pp / 1e3) / 1e9,
                          "kernels_per_step": sum((2 if p["X"].shape[0] >= 2 else 1) + 8 for p in panels)},
            "speedup_graph_vs_per_panel": ms_pp / ms_graph,

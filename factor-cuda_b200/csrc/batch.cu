@@ -1,6 +1,15 @@
 // batch.cu -- many panels of uneven T x N per launch.
 //
-// Rank + IC: every (panel, date) pair is one work item.  Items are grouped by
+// Rank + IC of f32 panels: the per-(date, factor) kernels of the single-panel
+// entry points in batched form.  Panels are grouped by the kernel variant
+// their width needs (N up to 2048 / 5120 / 8192 / 16384; the first two
+// boundaries are tunable), and each variant is one returns-preparation
+// launch over all its panels' dates, one rank launch over all their
+// (date, factor) sections and, with learned splitters, one launch that ranks
+// the sections handed back to the radix sort -- the same device bodies, so
+// results are those of the single-panel calls bit for bit.
+//
+// Rank + IC of f64 panels: every (panel, date) pair is one work item.  Items are grouped by
 // the block size their cross-section needs (256 / 512 / 1024 threads; the
 // thresholds are tunable), each group is a device queue, and one persistent
 // kernel per group (k_rank_ic_batch) runs as many CTAs as fit, each taking
@@ -74,6 +83,10 @@ struct fcb_batch {
   void* d_prep_mem = nullptr;
   std::vector<RicPrep> preps;
   int* d_status = nullptr;
+  // f32 panels: descriptors, item offsets and fallback lists of every variant
+  void* d_ric = nullptr;
+  size_t ric_cap = 0;
+  RicBatchVariant var[kRicVariants] = {};
   std::vector<FcWork> fcw;
   std::vector<void*> fc_mem;
   // current schedule
@@ -101,6 +114,9 @@ struct fcb_batch {
     cudaFree(d_ctr);
     cudaFree(d_prep_mem);
     cudaFree(d_status);
+    cudaFree(d_ric);
+    d_ric = nullptr;
+    ric_cap = 0;
     for (void* m : fc_mem) cudaFree(m);
     fc_mem.clear();
     for (int k = 0; k < kClasses; ++k) {
@@ -170,8 +186,107 @@ int occupancy(const fcb_batch& b, int k, int* occ) {
                                             nullptr, 0, nullptr, 0, b.cls_smem[k], nullptr, nullptr, occ));
 }
 
+// f32 panels: the kernel variant of a panel of width N under the current
+// configuration (a panel may be served by a wider variant than it needs).
+int variant_of(const fcb_batch& b, int N) {
+  if (N <= std::min(b.cfg.nt_small_max, ric_variant_cap(0))) return 0;
+  if (N <= std::min(b.cfg.nt_mid_max, ric_variant_cap(1))) return 1;
+  if (N <= ric_variant_cap(2)) return 2;
+  return 3;
+}
+
+// f32 panels: per variant, the panel descriptors (order 1: widest work
+// first), their date and section offsets and the fallback list, uploaded in
+// one buffer.
+int plan_items(fcb_batch& b) {
+  std::vector<int> idx[kRicVariants];
+  for (size_t i = 0; i < b.p.size(); ++i) idx[variant_of(b, b.p[i].N)].push_back(static_cast<int>(i));
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  size_t total = 0;
+  size_t o_pan[kRicVariants], o_od[kRicVariants], o_oi[kRicVariants], o_cnt[kRicVariants], o_items[kRicVariants];
+  long long ndates[kRicVariants] = {}, nitems[kRicVariants] = {};
+  for (int k = 0; k < kRicVariants; ++k) {
+    if (b.cfg.order == 1)
+      std::stable_sort(idx[k].begin(), idx[k].end(), [&](int x, int y) {
+        const fcb_panel &px = b.p[x], &py = b.p[y];
+        return static_cast<double>(px.T) * px.F * px.N > static_cast<double>(py.T) * py.F * py.N;
+      });
+    for (int i : idx[k]) {
+      ndates[k] += b.p[i].T;
+      nitems[k] += static_cast<long long>(b.p[i].T) * b.p[i].F;
+    }
+    if (nitems[k] > 2147483647LL) return FCB_ERR_CAP3;
+    const size_t np = idx[k].size();
+    o_pan[k] = total;
+    total += al(np * sizeof(RicPanel));
+    o_od[k] = total;
+    total += al(np * sizeof(int));
+    o_oi[k] = total;
+    total += al(np * sizeof(int));
+    o_cnt[k] = total;
+    total += 256;
+    o_items[k] = total;
+    total += al(static_cast<size_t>(nitems[k]) * sizeof(int));
+  }
+  if (b.ric_cap < total) {
+    cudaFree(b.d_ric);
+    b.d_ric = nullptr;
+    b.ric_cap = 0;
+    FCB_BTRY(cudaMalloc(&b.d_ric, total));
+    b.ric_cap = total;
+  }
+  std::vector<uint8_t> host(total, 0);
+  uint8_t* base = static_cast<uint8_t*>(b.d_ric);
+  for (int k = 0; k < kRicVariants; ++k) {
+    RicBatchVariant& v = b.var[k];
+    v = RicBatchVariant{};
+    v.np = static_cast<int>(idx[k].size());
+    if (v.np == 0) continue;
+    RicPanel* hp = reinterpret_cast<RicPanel*>(host.data() + o_pan[k]);
+    int* hd = reinterpret_cast<int*>(host.data() + o_od[k]);
+    int* hi = reinterpret_cast<int*>(host.data() + o_oi[k]);
+    int od = 0, oi = 0;
+    for (int j = 0; j < v.np; ++j) {
+      const int i = idx[k][j];
+      const fcb_panel& q = b.p[i];
+      RankIcArgs<float, float> a{};
+      a.X = static_cast<const float*>(q.X);
+      a.R = static_cast<const float*>(q.R);
+      a.fmask = q.fmask;
+      a.rmask = q.rmask;
+      a.F = q.F;
+      a.T = q.T;
+      a.N = q.N;
+      a.min_valid = b.min_valid;
+      a.ranks_out = q.ranks_out;
+      a.ic_out = q.ic_out;
+      if (q.model != nullptr) {
+        a.cdf_table = q.model->table[q.model->cur];
+        a.cdf_zrange = q.model->zrange[q.model->cur];
+        v.learned = true;
+      }
+      a.learn_cap = b.cfg.learn_cap > 0 ? b.cfg.learn_cap : 64;
+      hp[j] = RicPanel{a, b.preps[i]};
+      hd[j] = od;
+      hi[j] = oi;
+      od += q.T;
+      oi += q.T * q.F;
+      v.maxN = std::max(v.maxN, q.N);
+    }
+    v.dates = od;
+    v.items = oi;
+    v.panels = reinterpret_cast<const RicPanel*>(base + o_pan[k]);
+    v.off_dates = reinterpret_cast<const int*>(base + o_od[k]);
+    v.off_items = reinterpret_cast<const int*>(base + o_oi[k]);
+    v.fb = RicList{reinterpret_cast<int*>(base + o_cnt[k]), reinterpret_cast<int*>(base + o_items[k])};
+  }
+  FCB_BTRY(cudaMemcpy(b.d_ric, host.data(), total, cudaMemcpyHostToDevice));
+  return FCB_OK;
+}
+
 // Items, per-class shared memory and grids for the current configuration.
 int plan(fcb_batch& b) {
+  if (b.dtx == FCB_DTYPE_F32) return plan_items(b);
   std::vector<std::vector<int2>> items(kClasses);
   for (int k = 0; k < kClasses; ++k) {
     b.cls_maxN[k] = 0;
@@ -226,10 +341,15 @@ int plan(fcb_batch& b) {
 
 // Enqueue one whole batch on s0 (and the batch's side streams).
 int enqueue(fcb_batch& b, cudaStream_t s0) {
-  FCB_BTRY(cudaMemsetAsync(b.d_ctr, 0, kClasses * sizeof(int), s0));
+  if (b.dtx != FCB_DTYPE_F32) FCB_BTRY(cudaMemsetAsync(b.d_ctr, 0, kClasses * sizeof(int), s0));
   FCB_BTRY(cudaEventRecord(b.ev_fork, s0));
   for (int k = 1; k < kClasses; ++k) FCB_BTRY(cudaStreamWaitEvent(b.s[k], b.ev_fork, 0));
-  for (int k = 0; k < kClasses; ++k) {
+  for (int k = 0; k < kRicVariants && b.dtx == FCB_DTYPE_F32; ++k) {
+    if (b.var[k].np == 0) continue;
+    cudaStream_t st = (b.cfg.concurrent && k > 0) ? b.s[std::min(k, kClasses - 1)] : s0;
+    FCB_BTRY(launch_rank_ic_items_batch(k, b.var[k], st));
+  }
+  for (int k = 0; k < kClasses && b.dtx != FCB_DTYPE_F32; ++k) {
     if (b.cls_cnt[k] == 0) continue;
     cudaStream_t st = (b.cfg.concurrent && k > 0) ? b.s[k] : s0;
     const int2* items = b.d_items + b.cls_off[k];
@@ -269,9 +389,9 @@ int build_graph(fcb_batch& b) {
   b.drop_graph();
   int r = plan(b);
   if (r != FCB_OK) return r;
-  // the scheduling knob learn_cap lives in the panel arguments
-  r = (b.dtx == FCB_DTYPE_F32) ? upload_args<float, float>(b) : upload_args<double, double>(b);
-  if (r != FCB_OK) return r;
+  // the scheduling knob learn_cap lives in the panel arguments (f32: in the
+  // descriptors plan() uploaded)
+  if (b.dtx != FCB_DTYPE_F32 && (r = upload_args<double, double>(b)) != FCB_OK) return r;
   FCB_BTRY(cudaStreamBeginCapture(b.s[0], cudaStreamCaptureModeRelaxed));
   r = enqueue(b, b.s[0]);
   cudaGraph_t g = nullptr;
@@ -365,9 +485,9 @@ extern "C" int fcb_batch_create(const fcb_panel* panels, int npanels, int dtype_
     if (static_cast<long long>(q.T) * q.N > 2147483647LL) return FCB_ERR_CAP3;
     if (q.N > kSmemRankCap) return FCB_ERR_UNSUPPORTED;
     // the cross-section must fit one CTA's shared memory (largest block size)
-    const size_t need = (dtype_x == FCB_DTYPE_F32) ? rank_ic_batch_smem<float, float>(1024, q.N)
-                                                   : rank_ic_batch_smem<double, double>(1024, q.N);
-    if (need > kMaxSmemPerBlock) return FCB_ERR_UNSUPPORTED;
+    if (dtype_x == FCB_DTYPE_F32 ? !ric_items_fit(q.N)
+                                 : rank_ic_batch_smem<double, double>(1024, q.N) > kMaxSmemPerBlock)
+      return FCB_ERR_UNSUPPORTED;
     if (q.corr_out != nullptr && q.F > 128) return FCB_ERR_CAP3;
     if (q.model != nullptr) {
       if (dtype_x != FCB_DTYPE_F32 || q.model->F != q.F || q.model->table[q.model->cur] == nullptr)
@@ -440,8 +560,24 @@ extern "C" int fcb_batch_create(const fcb_panel* panels, int npanels, int dtype_
     c8 += 256;
     w.fb_part = reinterpret_cast<double*>(c8);
   }
-  const int r = (dtype_x == FCB_DTYPE_F32) ? upload_args<float, float>(*b) : upload_args<double, double>(*b);
-  if (r != FCB_OK) return fail(r);
+  if (dtype_x == FCB_DTYPE_F32) {
+    // prepared returns of every panel (ric_prep_bytes each, 256-byte aligned),
+    // used by the batched launches and by the per-panel arm
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    size_t total = 0;
+    for (const fcb_panel& q : b->p) total += al(ric_prep_bytes(q.T, q.N, q.F));
+    e = cudaMalloc(&b->d_prep_mem, total);
+    if (e != cudaSuccess) return fail(rcode(e));
+    b->preps.resize(b->p.size());
+    uint8_t* c8 = static_cast<uint8_t*>(b->d_prep_mem);
+    for (size_t i = 0; i < b->p.size(); ++i) {
+      b->preps[i] = ric_prep_carve(c8, b->p[i].T, b->p[i].N, b->p[i].F);
+      c8 += al(ric_prep_bytes(b->p[i].T, b->p[i].N, b->p[i].F));
+    }
+  } else {
+    const int r = upload_args<double, double>(*b);
+    if (r != FCB_OK) return fail(r);
+  }
   *out = b;
   return FCB_OK;
 }
@@ -477,20 +613,6 @@ extern "C" int fcb_batch_run_per_panel(fcb_batch* b, void* stream) {
   if (b == nullptr) return FCB_ERR_ARG;
   int r = bind_device(*b);
   if (r != FCB_OK) return r;
-  if (b->dtx == FCB_DTYPE_F32 && b->d_prep_mem == nullptr) {
-    // prepared returns for the per-(date, factor) path, allocated on the first
-    // per-panel run (ric_prep_bytes per panel, 256-byte aligned)
-    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    size_t total = 0;
-    for (const fcb_panel& q : b->p) total += al(ric_prep_bytes(q.T, q.N, q.F));
-    FCB_BTRY(cudaMalloc(&b->d_prep_mem, total));
-    b->preps.resize(b->p.size());
-    uint8_t* c8 = static_cast<uint8_t*>(b->d_prep_mem);
-    for (size_t i = 0; i < b->p.size(); ++i) {
-      b->preps[i] = ric_prep_carve(c8, b->p[i].T, b->p[i].N, b->p[i].F);
-      c8 += al(ric_prep_bytes(b->p[i].T, b->p[i].N, b->p[i].F));
-    }
-  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   for (size_t i = 0; i < b->p.size(); ++i) {
     const fcb_panel& q = b->p[i];
@@ -582,7 +704,7 @@ std::string signature(const fcb_batch& b) {
     work[k] += item_work(q) * q.T;
   }
   char buf[512];
-  int n = std::snprintf(buf, sizeof(buf), "fcb-batch-v2 n=%zu dt=%d/%d l=%d", b.p.size(), b.dtx, b.dtr,
+  int n = std::snprintf(buf, sizeof(buf), "fcb-batch-v3 n=%zu dt=%d/%d l=%d", b.p.size(), b.dtx, b.dtr,
                         b.learned ? 1 : 0);
   for (int k = 0; k < kClasses; ++k)
     n += std::snprintf(buf + n, sizeof(buf) - n, " c%d=%lld:%lld:%.3e", k, cnt[k], mx[k], work[k]);
@@ -666,6 +788,44 @@ extern "C" int fcb_batch_autotune(fcb_batch* b, int reps, const char* cache_path
     if (c.order == o) continue;
     c.order = o;
     if ((r = consider(c)) != FCB_OK) return r;
+  }
+  if (b->dtx == FCB_DTYPE_F32) {
+    // f32: which kernel variant serves which widths (a narrow panel may run in
+    // a wider variant), variants concurrent or in sequence, the bucket cap
+    for (int v : {512, 1024, 2048}) {
+      fcb_batch_config c = best;
+      if (c.nt_small_max == v) continue;
+      c.nt_small_max = v;
+      if ((r = consider(c)) != FCB_OK) return r;
+    }
+    for (int v : {2048, 3072, 4096, 5120, 8192}) {
+      fcb_batch_config c = best;
+      if (c.nt_mid_max == v) continue;
+      c.nt_mid_max = v;
+      if ((r = consider(c)) != FCB_OK) return r;
+    }
+    for (int v = 0; v <= 1; ++v) {
+      fcb_batch_config c = best;
+      if (c.concurrent == v) continue;
+      c.concurrent = v;
+      if ((r = consider(c)) != FCB_OK) return r;
+    }
+    if (b->learned) {
+      for (int v : cap_opts) {
+        fcb_batch_config c = best;
+        if (c.learn_cap == v) continue;
+        c.learn_cap = v;
+        if ((r = consider(c)) != FCB_OK) return r;
+      }
+    }
+    b->cfg = best;
+    b->drop_graph();
+    r = build_graph(*b);
+    if (r != FCB_OK) return r;
+    cache_store(cache_path, sig, best, best_ms);
+    if (best_out != nullptr) *best_out = best;
+    if (best_ms_out != nullptr) *best_ms_out = best_ms;
+    return FCB_OK;
   }
   // class boundaries: fixed steps plus the occupancy cliffs inside the
   // batch's range of section widths

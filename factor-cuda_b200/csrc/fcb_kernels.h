@@ -79,7 +79,6 @@ int fc_fb_nblk(long long R, int F);
 size_t fc_fb_part_doubles(long long R, int F);
 
 // rank_kernels.cu
-size_t cs_rank_smem(int N);
 cudaError_t launch_cs_rank(const float* X, const uint8_t* mask, int T, int N, int desc, float* out,
                            int* status, cudaStream_t st);
 cudaError_t launch_param_scan(const float* X, const uint8_t* mask, int T, int N, ScanOut outs, int* status,
@@ -152,10 +151,35 @@ struct RicPrep {
   int* fb_items;
   int ld;
 };
+// A device list of sections (item ids) handed from the learned kernel to the
+// radix kernel.
+struct RicList {
+  int* count;
+  int* items;
+};
 size_t ric_prep_bytes(int T, int N, int F);
 RicPrep ric_prep_carve(void* base, int T, int N, int F);
 // True when the per-(date, factor) kernels take N (f32 factors and returns).
 bool ric_items_fit(int N);
+// Batched form: the panels of one size variant (variant v serves N up to
+// ric_variant_cap(v): 2048, 5120, 8192, 16384) in one returns launch, one rank
+// launch and (learned) one fallback launch; items are a panel's dates (returns
+// pass) or its (date, factor) sections, in panel order.
+constexpr int kRicVariants = 4;
+int ric_variant_cap(int variant);
+struct RicPanel {
+  RankIcArgs<float, float> a;
+  RicPrep rp;
+};
+struct RicBatchVariant {
+  const RicPanel* panels;  // device, np entries
+  const int* off_dates;    // device, exclusive prefix of the panels' T (np entries)
+  const int* off_items;    // device, exclusive prefix of the panels' T*F (np entries)
+  int np, dates, items, maxN;
+  bool learned;            // some panel has a model (its sections take the learned body)
+  RicList fb;              // the variant's fallback list (items entries)
+};
+cudaError_t launch_rank_ic_items_batch(int variant, const RicBatchVariant& v, cudaStream_t st);
 // Rank + IC of F >= 1 f32 factor panels against one f32 returns panel: the
 // returns pass, then one CTA per (date, factor) -- learned splitters (with the
 // radix kernel taking the sections they hand back) or radix.  Requires

@@ -209,14 +209,16 @@ FCB_DEV void drop_prefix(uint32_t* dw32, int nwd) {
 
 // The shared epilogue.  P[c] = cs rank (bits 0-15, 0 = not ranked) | joint
 // factor rank (bits 16-31, 0 = not joint).  Writes the rank row, and the IC
-// unless `bad` (then the section is queued for the radix kernel).  With
+// unless `bad` (then the section, item_id, is queued on `fb` for the radix
+// kernel).  With
 // KEYS the factor-constant test takes the min / max of the joint cells' keys
 // (key[]); otherwise fkmin / fkmax are the keys at the first and last joint
 // positions of the sorted order, provided by the caller.
 template <int NT, int V, bool KEYS>
 FCB_DEV void ric_epilogue(const RankIcArgs<float, float>& a, const RicPrep& rp, int t, int f, const uint32_t (&P)[4 * V],
                           const uint32_t (&key)[4 * V], uint32_t fkmin, uint32_t fkmax, uint32_t mj,
-                          const unsigned long long* dw, uint32_t* red, int bad, int* stats) {
+                          const unsigned long long* dw, uint32_t* red, int bad, int* stats, int item_id,
+                          RicList fb) {
   constexpr int C = 4 * V;
   const int N = a.N;
   const size_t frow = (static_cast<size_t>(f) * a.T + t) * N;
@@ -292,7 +294,7 @@ FCB_DEV void ric_epilogue(const RankIcArgs<float, float>& a, const RicPrep& rp, 
     if (b) {
       // the learned order failed its judge: the radix kernel redoes the section
       if (stats != nullptr) stats[0] = kLearnJudge;
-      rp.fb_items[atomicAdd(rp.fb_count, 1)] = t * a.F + f;
+      fb.items[atomicAdd(fb.count, 1)] = item_id;
     } else {
       double ic = __longlong_as_double(0x7ff8000000000000ll);
       const long long m = static_cast<long long>(mj);
@@ -308,16 +310,14 @@ FCB_DEV void ric_epilogue(const RankIcArgs<float, float>& a, const RicPrep& rp, 
 // ---------------------------------------------------------------------------
 // per-date returns preparation
 // ---------------------------------------------------------------------------
+// Date t of returns R (T,N) and masks: the prepared words of row t into out.
 template <int NT, int V>
-__global__ void __launch_bounds__(NT) k_ric_prep(const float* __restrict__ R, const uint8_t* __restrict__ rmask,
-                                                 const uint8_t* __restrict__ fmask, int N, RicPrep rp) {
+FCB_DEV void ric_prep_body(const float* __restrict__ R, const uint8_t* __restrict__ rmask,
+                           const uint8_t* __restrict__ fmask, int N, int t, uint32_t* __restrict__ out, uint8_t* sm) {
   constexpr int C = 4 * V;
-  extern __shared__ __align__(16) uint8_t sm[];
   const SortedLayout<NT> L(N);
   unsigned long long* scan64 = reinterpret_cast<unsigned long long*>(sm + L.red);
-  const int t = blockIdx.x;
   const size_t row = static_cast<size_t>(t) * N;
-  if (blockIdx.x == 0 && threadIdx.x == 0) *rp.fb_count = 0;
   float r[C];
   load_row_f32<NT, V, true>(R + row, N, r);
   uint32_t fmb = 0u, rvb = 0u;  // per-cell bits: factor mask, returns valid
@@ -381,7 +381,6 @@ __global__ void __launch_bounds__(NT) k_ric_prep(const float* __restrict__ R, co
     W[is[p]] = static_cast<uint32_t>(p) | (static_cast<uint32_t>(carry) << kGidShift) | kRetValid;
   }
   __syncthreads();
-  uint32_t* out = rp.word + static_cast<size_t>(t) * rp.ld;
 #pragma unroll
   for (int j = 0; j < V; ++j) {
     const int i0c = 4 * (j * NT + static_cast<int>(threadIdx.x));
@@ -401,14 +400,23 @@ __global__ void __launch_bounds__(NT) k_ric_prep(const float* __restrict__ R, co
   }
 }
 
+template <int NT, int V>
+__global__ void __launch_bounds__(NT) k_ric_prep(const float* __restrict__ R, const uint8_t* __restrict__ rmask,
+                                                 const uint8_t* __restrict__ fmask, int N, RicPrep rp) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *rp.fb_count = 0;
+  ric_prep_body<NT, V>(R, rmask, fmask, N, blockIdx.x, rp.word + static_cast<size_t>(blockIdx.x) * rp.ld, sm);
+}
+
 // ---------------------------------------------------------------------------
 // learned splitters
 // ---------------------------------------------------------------------------
+// Section (t, f); item_id is what a fallback queues on fb.
 template <int NT, int V>
-__global__ void __launch_bounds__(NT) k_ric_learned(RankIcArgs<float, float> a, RicPrep rp) {
+FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& rp, const int t, const int f,
+                              const int item_id, RicList fb, uint8_t* sm) {
   constexpr int C = 4 * V, NW = NT / 32;
-  extern __shared__ __align__(16) uint8_t sm[];
-  const int N = a.N, F = a.F;
+  const int N = a.N;
   const BucketLayout L(N);
   uint32_t* red = reinterpret_cast<uint32_t*>(sm + L.red);
   float* tab = reinterpret_cast<float*>(sm + L.tab);
@@ -416,7 +424,6 @@ __global__ void __launch_bounds__(NT) k_ric_learned(RankIcArgs<float, float> a, 
   const unsigned long long* dw = reinterpret_cast<const unsigned long long*>(sm + L.dw);
   uint32_t* cnt = reinterpret_cast<uint32_t*>(sm + L.cnt);
   unsigned long long* mem = reinterpret_cast<unsigned long long*>(sm + L.mem);
-  const int t = blockIdx.x / F, f = blockIdx.x % F;
   const int tid = static_cast<int>(threadIdx.x), wi = tid >> 5, lane = tid & 31;
   const size_t frow = (static_cast<size_t>(f) * a.T + t) * N;
   int* stats = a.learn_stats != nullptr ? a.learn_stats + (static_cast<size_t>(f) * a.T + t) * 4 : nullptr;
@@ -509,7 +516,7 @@ __global__ void __launch_bounds__(NT) k_ric_learned(RankIcArgs<float, float> a, 
         stats[2] = 0;
         stats[3] = m;
       }
-      rp.fb_items[atomicAdd(rp.fb_count, 1)] = blockIdx.x;
+      fb.items[atomicAdd(fb.count, 1)] = item_id;
     }
     return;
   }
@@ -572,7 +579,7 @@ __global__ void __launch_bounds__(NT) k_ric_learned(RankIcArgs<float, float> a, 
         stats[2] = static_cast<int>(sqall);
         stats[3] = m;
       }
-      rp.fb_items[atomicAdd(rp.fb_count, 1)] = blockIdx.x;
+      fb.items[atomicAdd(fb.count, 1)] = item_id;
     }
     return;
   }
@@ -630,19 +637,25 @@ __global__ void __launch_bounds__(NT) k_ric_learned(RankIcArgs<float, float> a, 
   __syncthreads();  // B7
   int bad = 0;
   for (int p = tid + 1; p < m; p += NT) bad |= (kS[p - 1] > kS[p]) ? 1 : 0;
-  ric_epilogue<NT, V, true>(a, rp, t, f, P, key, 0u, 0u, mj, dw, red, bad, stats);
+  ric_epilogue<NT, V, true>(a, rp, t, f, P, key, 0u, 0u, mj, dw, red, bad, stats, item_id, fb);
+}
+
+template <int NT, int V>
+__global__ void __launch_bounds__(NT) k_ric_learned(RankIcArgs<float, float> a, RicPrep rp) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  const int item = static_cast<int>(blockIdx.x);
+  ric_learned_body<NT, V>(a, rp, item / a.F, item % a.F, item, RicList{rp.fb_count, rp.fb_items}, sm);
 }
 
 // ---------------------------------------------------------------------------
 // radix (plain path and the learned path's fallback)
 // ---------------------------------------------------------------------------
-// LIST: sections come from the learned kernel's fallback list (persistent
-// CTAs stride over it); otherwise blockIdx.x = t * F + f.
-template <int NT, int V, bool LIST>
-__global__ void __launch_bounds__(NT) k_ric_radix(RankIcArgs<float, float> a, RicPrep rp) {
+// Section (t, f) by the radix sort.
+template <int NT, int V, bool STREAM>
+FCB_DEV void ric_radix_body(const RankIcArgs<float, float>& a, const RicPrep& rp, const int t, const int f,
+                            uint8_t* sm) {
   constexpr int C = 4 * V;
-  extern __shared__ __align__(16) uint8_t sm[];
-  const int N = a.N, F = a.F;
+  const int N = a.N;
   const SortedLayout<NT> L(N);
   uint32_t* red = reinterpret_cast<uint32_t*>(sm + L.red);
   unsigned long long* scan64 = reinterpret_cast<unsigned long long*>(sm + L.red);
@@ -654,15 +667,12 @@ __global__ void __launch_bounds__(NT) k_ric_radix(RankIcArgs<float, float> a, Ri
   uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
   const int tid = static_cast<int>(threadIdx.x);
   const int nwd = (N + 31) / 32 + 1;
-  const int nitems = LIST ? *static_cast<volatile int*>(rp.fb_count) : static_cast<int>(gridDim.x);
-  for (int it = blockIdx.x; it < nitems; it += static_cast<int>(gridDim.x)) {
-    const int item = LIST ? rp.fb_items[it] : it;
-    const int t = item / F, f = item % F;
+  {
     const size_t frow = (static_cast<size_t>(f) * a.T + t) * N;
     for (int k = tid; k < nwd; k += NT) reinterpret_cast<unsigned long long*>(dw32)[k] = 0ull;
     float x[C];
     uint32_t w[C];
-    load_row_f32<NT, V, !LIST>(a.X + frow, N, x);
+    load_row_f32<NT, V, STREAM>(a.X + frow, N, x);
     load_words<NT, V>(rp.word + static_cast<size_t>(t) * rp.ld, N, w);
     uint32_t valid = 0u, joint = 0u;  // bit c: cell c is factor-valid / in the joint set
 #pragma unroll
@@ -723,8 +733,282 @@ __global__ void __launch_bounds__(NT) k_ric_radix(RankIcArgs<float, float> a, Ri
     uint32_t P[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) P[c] = ((valid >> c) & 1u) ? RK[4 * ((c >> 2) * NT + tid) + (c & 3)] : 0u;
-    ric_epilogue<NT, V, false>(a, rp, t, f, P, P, fkmin, fkmax, mj, dw, red, 0, nullptr);
+    ric_epilogue<NT, V, false>(a, rp, t, f, P, P, fkmin, fkmax, mj, dw, red, 0, nullptr, 0, RicList{nullptr, nullptr});
+  }
+}
+
+// LIST: sections come from the learned kernel's fallback list (persistent
+// CTAs stride over it); otherwise blockIdx.x = t * F + f.
+template <int NT, int V, bool LIST>
+__global__ void __launch_bounds__(NT) k_ric_radix(RankIcArgs<float, float> a, RicPrep rp) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  if (!LIST) {
+    ric_radix_body<NT, V, true>(a, rp, static_cast<int>(blockIdx.x) / a.F, static_cast<int>(blockIdx.x) % a.F, sm);
+    return;
+  }
+  const int nitems = *static_cast<volatile int*>(rp.fb_count);
+  for (int it = blockIdx.x; it < nitems; it += static_cast<int>(gridDim.x)) {
+    const int item = rp.fb_items[it];
+    ric_radix_body<NT, V, false>(a, rp, item / a.F, item % a.F, sm);
     __syncthreads();  // the next section reuses the shared memory
+  }
+}
+
+// ---------------------------------------------------------------------------
+// many panels per launch (the batch)
+// ---------------------------------------------------------------------------
+// The panels of one size variant share a launch: one CTA per item (a date of
+// a panel for the returns pass, a (date, factor) section for the rank pass),
+// the item's panel found by binary search over the exclusive prefix `off` of
+// the panels' item counts.  Sections handed back by the learned body go on
+// the variant's list as global item ids.  Panels without a model are ranked
+// by the radix body in the learned launch.
+FCB_DEV int panel_of(const int* __restrict__ off, int np, int item) {
+  int lo = 0, hi = np - 1;  // the last panel whose first item is <= item
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(off + mid) <= item) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int NT, int V>
+__global__ void __launch_bounds__(NT) k_ric_prep_batch(const RicPanel* __restrict__ P, const int* __restrict__ off,
+                                                       int np, RicList fb) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  const int item = static_cast<int>(blockIdx.x);
+  if (item == 0 && threadIdx.x == 0 && fb.count != nullptr) *fb.count = 0;
+  const int q = panel_of(off, np, item);
+  const RankIcArgs<float, float> a = P[q].a;
+  const RicPrep rp = P[q].rp;
+  const int t = item - __ldg(off + q);
+  ric_prep_body<NT, V>(a.R, a.rmask, a.fmask, a.N, t, rp.word + static_cast<size_t>(t) * rp.ld, sm);
+}
+
+template <int NT, int V, bool LEARNED>
+__global__ void __launch_bounds__(NT) k_ric_items_batch(const RicPanel* __restrict__ P, const int* __restrict__ off,
+                                                        int np, RicList fb) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  const int item = static_cast<int>(blockIdx.x);
+  const int q = panel_of(off, np, item);
+  const RankIcArgs<float, float> a = P[q].a;
+  const RicPrep rp = P[q].rp;
+  const int l = item - __ldg(off + q);
+  if (LEARNED && a.cdf_table != nullptr)
+    ric_learned_body<NT, V>(a, rp, l / a.F, l % a.F, item, fb, sm);
+  else
+    ric_radix_body<NT, V, true>(a, rp, l / a.F, l % a.F, sm);
+}
+
+template <int NT, int V>
+__global__ void __launch_bounds__(NT) k_ric_list_batch(const RicPanel* __restrict__ P, const int* __restrict__ off,
+                                                       int np, RicList fb) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  const int nitems = *static_cast<volatile int*>(fb.count);
+  for (int it = blockIdx.x; it < nitems; it += static_cast<int>(gridDim.x)) {
+    const int item = fb.items[it];
+    const int q = panel_of(off, np, item);
+    const RankIcArgs<float, float> a = P[q].a;
+    const RicPrep rp = P[q].rp;
+    const int l = item - __ldg(off + q);
+    ric_radix_body<NT, V, false>(a, rp, l / a.F, l % a.F, sm);
+    __syncthreads();  // the next section reuses the shared memory
+  }
+}
+
+// ---------------------------------------------------------------------------
+// cs_rank and parameter_scan of one plane: one CTA per date
+// ---------------------------------------------------------------------------
+// cs_rank: valid = finite & mask; the valid cells are compacted in column
+// order, radix-sorted by key (of -x for descending), and each cell's rank is
+// its sorted position + 1 (replaces cs_rank_gpu, src/cross_sectional_rank.cu:
+// 228-372, which runs CUB's global segmented sort).
+template <int NT, int V>
+__global__ void __launch_bounds__(NT) k_csr(const float* __restrict__ X, const uint8_t* __restrict__ mask, int N,
+                                            int desc, float* __restrict__ out) {
+  constexpr int C = 4 * V;
+  extern __shared__ __align__(16) uint8_t sm[];
+  const SortedLayout<NT> L(N);
+  unsigned long long* scan64 = reinterpret_cast<unsigned long long*>(sm + L.red);
+  uint32_t* k0 = reinterpret_cast<uint32_t*>(sm + L.k0);
+  uint32_t* k1 = reinterpret_cast<uint32_t*>(sm + L.k1);
+  uint16_t* i0 = reinterpret_cast<uint16_t*>(sm + L.i0);
+  uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
+  const int tid = static_cast<int>(threadIdx.x);
+  const size_t row = static_cast<size_t>(blockIdx.x) * N;
+  float x[C];
+  uint32_t mk[C];
+  load_row_f32<NT, V, true>(X + row, N, x);
+  load_mask4<NT, V>(mask != nullptr ? mask + row : nullptr, N, mk);
+  uint32_t valid = 0u;
+#pragma unroll
+  for (int c = 0; c < C; ++c) valid |= ((finite_f32(x[c]) && mk[c]) ? 1u : 0u) << c;
+  int base[V];
+  const int m = compact_bases<NT, V>(valid, base, scan64);
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    int p = base[j];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int c = 4 * j + k;
+      if ((valid >> c) & 1u) {
+        k0[p] = key_f32(desc ? -x[c] : x[c]);
+        i0[p] = static_cast<uint16_t>(4 * (j * NT + tid) + k);
+        ++p;
+      }
+    }
+  }
+  __syncthreads();
+  uint32_t* ks;
+  uint16_t* is;
+  block_radix_sort<NT, C, uint32_t>(k0, i0, k1, i1, m, sm + L.scratch, &ks, &is);
+  uint32_t* RK = (ks == k0) ? k1 : k0;
+  for (int p = tid; p < m; p += NT) RK[is[p]] = static_cast<uint32_t>(p + 1);
+  __syncthreads();
+  const float qnan = __uint_as_float(kQuietNanBits);
+  float v[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c)
+    v[c] = ((valid >> c) & 1u) ? static_cast<float>(RK[4 * ((c >> 2) * NT + tid) + (c & 3)]) : qnan;
+  store_row_f32v<NT, V>(out + row, N, v);
+}
+
+// parameter_scan: one ascending sort of the finite cells serves all four
+// groups (asc / desc x masked / unmasked).  With S the start and E the end of
+// a cell's tie group in sorted order, C the count of masked-valid cells before
+// a sorted position and m / mt the finite / masked-valid totals:
+//   asc unmasked  p + 1                  asc masked   C[p] + 1
+//   desc unmasked m - E + (p - S) + 1    desc masked  mt - C[E] + (C[p] - C[S]) + 1
+// (descending ranks keep ties by ascending column, the contract of
+// fc/_cpu_core.py:57-78 / :295-301; replaces the reference's four rank
+// pipelines, src/cross_sectional_rank.cu:401-664).
+template <int NT>
+struct ScanLayout2 {
+  size_t s_cnt, s_ge, total;
+  __host__ __device__ explicit ScanLayout2(int n) {
+    size_t o = SortedLayout<NT>(n).total;
+    s_cnt = o; o = al16(o + size_t(n + 1) * 2);
+    s_ge = o; o = al16(o + size_t(n) * 2);
+    total = o;
+  }
+};
+
+template <int NT, int V>
+__global__ void __launch_bounds__(NT) k_pscan(const float* __restrict__ X, const uint8_t* __restrict__ mask, int N,
+                                              ScanOut outs) {
+  constexpr int C = 4 * V;
+  extern __shared__ __align__(16) uint8_t sm[];
+  const SortedLayout<NT> L(N);
+  const ScanLayout2<NT> L2(N);
+  unsigned long long* scan64 = reinterpret_cast<unsigned long long*>(sm + L.red);
+  uint32_t* scan32 = reinterpret_cast<uint32_t*>(sm + L.red);
+  uint32_t* k0 = reinterpret_cast<uint32_t*>(sm + L.k0);
+  uint32_t* k1 = reinterpret_cast<uint32_t*>(sm + L.k1);
+  uint16_t* i0 = reinterpret_cast<uint16_t*>(sm + L.i0);
+  uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
+  uint16_t* Cn = reinterpret_cast<uint16_t*>(sm + L2.s_cnt);
+  uint16_t* GE = reinterpret_cast<uint16_t*>(sm + L2.s_ge);
+  const int tid = static_cast<int>(threadIdx.x);
+  const size_t row = static_cast<size_t>(blockIdx.x) * N;
+  float x[C];
+  uint32_t mk[C];
+  load_row_f32<NT, V, true>(X + row, N, x);
+  load_mask4<NT, V>(mask != nullptr ? mask + row : nullptr, N, mk);
+  uint32_t fin = 0u, msk = 0u;
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    fin |= (finite_f32(x[c]) ? 1u : 0u) << c;
+    msk |= (mk[c] ? 1u : 0u) << c;
+  }
+  int base[V];
+  const int m = compact_bases<NT, V>(fin, base, scan64);
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    int p = base[j];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int c = 4 * j + k;
+      if ((fin >> c) & 1u) {
+        k0[p] = key_f32(x[c]);
+        i0[p] = static_cast<uint16_t>((4 * (j * NT + tid) + k) | (((msk >> c) & 1u) << 15));
+        ++p;
+      }
+    }
+  }
+  __syncthreads();
+  uint32_t* ks;
+  uint16_t* is;
+  block_radix_sort<NT, C, uint32_t>(k0, i0, k1, i1, m, sm + L.scratch, &ks, &is);
+  uint16_t* S = (is == i0) ? i1 : i0;                  // tie-group start per sorted position
+  uint32_t* O01 = (ks == k0) ? k1 : k0;                // (asc masked | asc unmasked << 16) per column
+  uint32_t* O23 = ks;                                   // (desc masked | desc unmasked << 16), after ks is read
+  // pass 1: per chunk, masked-valid count and the last group start
+  const int per = (m + NT - 1) / NT;
+  const int b0 = tid * per, b1 = min(m, b0 + per);
+  uint32_t cm = 0;
+  int last = -1;
+  for (int p = b0; p < b1; ++p) {
+    cm += is[p] >> 15;
+    if (p == 0 || ks[p] != ks[p - 1]) last = p;
+  }
+  uint32_t mt;
+  uint32_t c = block_exclusive_sum(cm, scan32, mt);
+  // exclusive max-scan of the chunks' last group starts (identity -1)
+  int inc = last;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(kFull, inc, o);
+    if (lane_id() >= static_cast<unsigned>(o)) inc = max(inc, u);
+  }
+  const int wi = tid >> 5;
+  int* sc = reinterpret_cast<int*>(scan64);
+  if (lane_id() == 31) sc[wi] = inc;
+  __syncthreads();
+  int carry = -1;
+  for (int i = 0; i < wi; ++i) carry = max(carry, sc[i]);
+  const int up = __shfl_up_sync(kFull, inc, 1);
+  if (lane_id() > 0) carry = max(carry, up);
+  // pass 2: S, the masked-valid prefix and the group ends
+  for (int p = b0; p < b1; ++p) {
+    if (p == 0 || ks[p] != ks[p - 1]) carry = p;
+    S[p] = static_cast<uint16_t>(carry);
+    Cn[p] = static_cast<uint16_t>(c);
+    c += is[p] >> 15;
+    if (p == m - 1 || ks[p] != ks[p + 1]) GE[carry] = static_cast<uint16_t>(p + 1);
+  }
+  if (tid == 0) Cn[m] = static_cast<uint16_t>(mt);
+  __syncthreads();
+  // pass 3: the four ranks of each sorted position, by column
+  for (int p = tid; p < m; p += NT) {
+    const uint32_t id = is[p];
+    const int col = static_cast<int>(id & 0x3FFFu);
+    const int s0 = S[p], e0 = GE[s0];
+    const uint32_t cp = Cn[p];
+    const uint32_t g1 = static_cast<uint32_t>(p + 1);
+    const uint32_t g3 = static_cast<uint32_t>(m - e0 + (p - s0) + 1);
+    uint32_t g0 = 0u, g2 = 0u;
+    if (id & 0x8000u) {
+      g0 = cp + 1u;
+      g2 = mt - Cn[e0] + (cp - Cn[s0]) + 1u;
+    }
+    O01[col] = g0 | (g1 << 16);
+    O23[col] = g2 | (g3 << 16);
+  }
+  __syncthreads();
+  const float qnan = __uint_as_float(kQuietNanBits);
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    if (outs.out[g] == nullptr) continue;  // uniform across the block
+    const uint32_t* src = (g < 2) ? O01 : O23;
+    const int sh = (g & 1) ? 16 : 0;
+    float v[C];
+#pragma unroll
+    for (int cc = 0; cc < C; ++cc) {
+      const uint32_t r =
+          ((fin >> cc) & 1u) ? ((src[4 * ((cc >> 2) * NT + tid) + (cc & 3)] >> sh) & 0xFFFFu) : 0u;
+      v[cc] = r ? static_cast<float>(r) : qnan;
+    }
+    store_row_f32v<NT, V>(outs.out[g] + row, N, v);
   }
 }
 
@@ -790,6 +1074,105 @@ RicPrep ric_prep_carve(void* base, int T, int N, int F) {
   rp.fb_items = reinterpret_cast<int*>(p);
   (void)F;
   return rp;
+}
+
+
+namespace {
+template <int NT, int V>
+cudaError_t csr_launch(const float* X, const uint8_t* mask, int T, int N, int desc, float* out, cudaStream_t st) {
+  const size_t smem = SortedLayout<NT>(N).total;
+  cudaError_t e = cudaFuncSetAttribute(k_csr<NT, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  k_csr<NT, V><<<T, NT, smem, st>>>(X, mask, N, desc, out);
+  return cudaGetLastError();
+}
+template <int NT, int V>
+cudaError_t pscan_launch(const float* X, const uint8_t* mask, int T, int N, ScanOut outs, cudaStream_t st) {
+  const size_t smem = ScanLayout2<NT>(N).total;
+  if (smem > kMaxSmemPerBlock) return cudaErrorInvalidValue;
+  cudaError_t e =
+      cudaFuncSetAttribute(k_pscan<NT, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  k_pscan<NT, V><<<T, NT, smem, st>>>(X, mask, N, outs);
+  return cudaGetLastError();
+}
+}  // namespace
+
+
+// The per-date rank kernels stage nothing through mbarriers, so `status` has
+// nothing to report; it is kept for the callers' uniform interface.
+cudaError_t launch_cs_rank(const float* X, const uint8_t* mask, int T, int N, int desc, float* out, int* status,
+                           cudaStream_t st) {
+  (void)status;
+  if (N < 1 || N > kSmemRankCap) return cudaErrorInvalidValue;
+  if (N <= 2048) return csr_launch<256, 2>(X, mask, T, N, desc, out, st);
+  if (N <= 5120) return csr_launch<256, 5>(X, mask, T, N, desc, out, st);
+  if (N <= 8192) return csr_launch<512, 4>(X, mask, T, N, desc, out, st);
+  return csr_launch<512, 8>(X, mask, T, N, desc, out, st);
+}
+
+cudaError_t launch_param_scan(const float* X, const uint8_t* mask, int T, int N, ScanOut outs, int* status,
+                              cudaStream_t st) {
+  (void)status;
+  if (N < 1 || N > kSmemRankCap) return cudaErrorInvalidValue;
+  if (N <= 2048) return pscan_launch<256, 2>(X, mask, T, N, outs, st);
+  if (N <= 5120) return pscan_launch<256, 5>(X, mask, T, N, outs, st);
+  if (N <= 8192) return pscan_launch<512, 4>(X, mask, T, N, outs, st);
+  return pscan_launch<512, 8>(X, mask, T, N, outs, st);
+}
+
+namespace {
+template <int NT, int V>
+cudaError_t ric_batch_launch(const RicBatchVariant& v, cudaStream_t st) {
+  const size_t smem_s = SortedLayout<NT>(v.maxN).total;
+  const size_t smem_b = BucketLayout(v.maxN).total;
+  const size_t smem_l = smem_s > smem_b ? smem_s : smem_b;
+  if (smem_l > kMaxSmemPerBlock) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_ric_prep_batch<NT, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem_s));
+  if (e != cudaSuccess) return e;
+  k_ric_prep_batch<NT, V><<<v.dates, NT, smem_s, st>>>(v.panels, v.off_dates, v.np, v.fb);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (!v.learned) {
+    if ((e = cudaFuncSetAttribute(k_ric_items_batch<NT, V, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem_s))) != cudaSuccess)
+      return e;
+    k_ric_items_batch<NT, V, false><<<v.items, NT, smem_s, st>>>(v.panels, v.off_items, v.np, v.fb);
+    return cudaGetLastError();
+  }
+  if ((e = cudaFuncSetAttribute(k_ric_items_batch<NT, V, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem_l))) != cudaSuccess)
+    return e;
+  k_ric_items_batch<NT, V, true><<<v.items, NT, smem_l, st>>>(v.panels, v.off_items, v.np, v.fb);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_ric_list_batch<NT, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem_s))) != cudaSuccess)
+    return e;
+  int occ = 0, dev = 0, sms = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ric_list_batch<NT, V>, NT, smem_s)) != cudaSuccess)
+    return e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  long long g = static_cast<long long>(occ > 0 ? occ : 1) * (sms > 0 ? sms : 1);
+  if (g > v.items) g = v.items;
+  k_ric_list_batch<NT, V><<<static_cast<unsigned>(g), NT, smem_s, st>>>(v.panels, v.off_items, v.np, v.fb);
+  return cudaGetLastError();
+}
+}  // namespace
+
+int ric_variant_cap(int variant) {
+  static const int caps[kRicVariants] = {2048, 5120, 8192, 16384};
+  return (variant >= 0 && variant < kRicVariants) ? caps[variant] : 0;
+}
+
+cudaError_t launch_rank_ic_items_batch(int variant, const RicBatchVariant& v, cudaStream_t st) {
+  if (v.np < 1 || v.items < 1 || v.maxN > ric_variant_cap(variant)) return cudaErrorInvalidValue;
+  switch (variant) {
+    case 0: return ric_batch_launch<256, 2>(v, st);
+    case 1: return ric_batch_launch<256, 5>(v, st);
+    case 2: return ric_batch_launch<512, 4>(v, st);
+    default: return ric_batch_launch<512, 8>(v, st);
+  }
 }
 
 bool ric_items_fit(int N) { return N >= 1 && N <= kSmemRankCap; }

@@ -1,14 +1,7 @@
 // rank_kernels.cu -- per-date in-shared-memory rank kernels for sm_100a.
 //
-//  k_cs_rank      one CTA per date: stage the row (bulk copy), compact the valid
-//                 cells, radix-sort (key, column) in shared memory, scatter
-//                 ordinal ranks, store the row.  Semantics of the reference's
-//                 cs_rank_gpu (src/cross_sectional_rank.cu:228-372).
-//  k_param_scan   one sort per date serves all four parameter_scan groups
-//                 (asc/desc x masked/unmasked): masked ranks are prefix counts
-//                 of mask flags in sorted order, descending ranks come from the
-//                 tie-group bounds of the ascending order.  Replaces four full
-//                 rank pipelines (src/cross_sectional_rank.cu:401-664).
+//  (cs_rank and parameter_scan of one plane: k_csr / k_pscan in
+//   rank_ic_bucket.cu.)
 //  k_rank_ic      one CTA per date, looping over F factor panels: the forward
 //                 returns are sorted once per date, each factor is sorted once;
 //                 cs_rank ranks (own valid set) and the joint-set ranks of the
@@ -148,175 +141,6 @@ FCB_DEV void store_row_f32(float* __restrict__ dst, const float* __restrict__ sr
     for (int i = h + nv * 4 + threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
   } else {
     for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
-  }
-}
-
-// ---------------------------------------------------------------------------
-// cs_rank
-// ---------------------------------------------------------------------------
-struct CsRankLayout {
-  size_t bars, scratch, k0, k1, i0, i1, total;
-  __host__ __device__ CsRankLayout(int n, size_t sort_scratch) {
-    size_t o = 0;
-    bars = o; o += 64;
-    scratch = o; o = align16(o + sort_scratch);
-    k0 = o; o = align16(o + size_t(n) * 4 + 16);
-    k1 = o; o = align16(o + size_t(n) * 4 + 16);
-    i0 = o; o = align16(o + size_t(n) * 2 + 16);
-    i1 = o; o = align16(o + size_t(n) * 2 + 16);
-    total = o;
-  }
-};
-
-template <int NT, int MAXIPT>
-__global__ void __launch_bounds__(NT, 2048 / NT) k_cs_rank(const float* __restrict__ X, const uint8_t* __restrict__ mask,
-                                                int N, int desc, float* __restrict__ out, int* status) {
-  extern __shared__ __align__(16) uint8_t sm[];
-  const CsRankLayout L(N, SortScratch<NT>::bytes);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L.bars);
-  uint32_t* scan = reinterpret_cast<uint32_t*>(sm + L.scratch + SortScratch<NT>::hist_bytes +
-                                               SortScratch<NT>::base_bytes);
-  const size_t row = static_cast<size_t>(blockIdx.x) * N;
-  if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  uint32_t ph0 = 0, ph1 = 0;
-  bool a0 = false, a1 = false;
-  const float* x = stage_issue(sm + L.k1, X + row, N, &bars[0], a0);
-  const uint8_t* mk = nullptr;
-  if (mask != nullptr) mk = stage_issue(sm + L.i1, mask + row, N, &bars[1], a1);
-  bool ok = stage_wait(&bars[0], ph0, a0);
-  ok = stage_wait(&bars[1], ph1, a1) && ok;
-  if (__syncthreads_or(!ok)) {
-    if (threadIdx.x == 0) atomicExch(status, 1);
-    return;
-  }
-  uint32_t* k0 = reinterpret_cast<uint32_t*>(sm + L.k0);
-  uint32_t* k1 = reinterpret_cast<uint32_t*>(sm + L.k1);
-  uint16_t* i0 = reinterpret_cast<uint16_t*>(sm + L.i0);
-  uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
-  const int m = compact_keys<uint32_t>(
-      N, [&](int i) { return finite_f32(x[i]) && (mk == nullptr || mk[i] != 0); },
-      [&](int i) { return key_f32(desc ? -x[i] : x[i]); }, k0, i0, scan);
-  uint32_t* ks;
-  uint16_t* is;
-  block_radix_sort<NT, MAXIPT, uint32_t>(k0, i0, k1, i1, m, sm + L.scratch, &ks, &is);
-  float* rbuf = reinterpret_cast<float*>(ks == k0 ? k1 : k0);
-  const float qnan = __uint_as_float(kQuietNanBits);
-  for (int i = threadIdx.x; i < N; i += NT) rbuf[i] = qnan;
-  __syncthreads();
-  for (int p = threadIdx.x; p < m; p += NT) rbuf[is[p]] = static_cast<float>(p + 1);
-  __syncthreads();
-  store_row_f32(out + row, rbuf, N);
-}
-
-// ---------------------------------------------------------------------------
-// parameter_scan: one ascending sort of the finite cells, four groups
-// ---------------------------------------------------------------------------
-struct ScanLayout {
-  size_t bars, scratch, k0, k1, i0, i1, mf, total;
-  __host__ __device__ ScanLayout(int n, size_t sort_scratch) {
-    size_t o = 0;
-    bars = o; o += 64;
-    scratch = o; o = align16(o + sort_scratch);
-    k0 = o; o = align16(o + size_t(n) * 4 + 16);
-    k1 = o; o = align16(o + size_t(n) * 4 + 16);
-    i0 = o; o = align16(o + size_t(n) * 2 + 16);
-    i1 = o; o = align16(o + size_t(n) * 2 + 16);
-    mf = o; o = align16(o + size_t(n) + 16);
-    total = o;
-  }
-};
-
-template <int NT, int MAXIPT>
-__global__ void __launch_bounds__(NT, 2048 / NT) k_param_scan(const float* __restrict__ X, const uint8_t* __restrict__ mask,
-                                                   int N, ScanOut outs, int* status) {
-  extern __shared__ __align__(16) uint8_t sm[];
-  const ScanLayout L(N, SortScratch<NT>::bytes);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L.bars);
-  uint32_t* scan = reinterpret_cast<uint32_t*>(sm + L.scratch + SortScratch<NT>::hist_bytes +
-                                               SortScratch<NT>::base_bytes);
-  const size_t row = static_cast<size_t>(blockIdx.x) * N;
-  if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  uint32_t ph0 = 0, ph1 = 0;
-  bool a0 = false, a1 = false;
-  const float* x = stage_issue(sm + L.k1, X + row, N, &bars[0], a0);
-  const uint8_t* mk = nullptr;
-  if (mask != nullptr) mk = stage_issue(sm + L.mf, mask + row, N, &bars[1], a1);
-  bool ok = stage_wait(&bars[0], ph0, a0);
-  ok = stage_wait(&bars[1], ph1, a1) && ok;
-  if (__syncthreads_or(!ok)) {
-    if (threadIdx.x == 0) atomicExch(status, 1);
-    return;
-  }
-  uint32_t* k0 = reinterpret_cast<uint32_t*>(sm + L.k0);
-  uint32_t* k1 = reinterpret_cast<uint32_t*>(sm + L.k1);
-  uint16_t* i0 = reinterpret_cast<uint16_t*>(sm + L.i0);
-  uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
-  const int m = compact_keys<uint32_t>(
-      N, [&](int i) { return finite_f32(x[i]); }, [&](int i) { return key_f32(x[i]); }, k0, i0, scan);
-  uint32_t* ks;
-  uint16_t* is;
-  block_radix_sort<NT, MAXIPT, uint32_t>(k0, i0, k1, i1, m, sm + L.scratch, &ks, &is);
-  // free buffers: the other key buffer (4n+16 B) and the other index buffer
-  uint8_t* kfree = reinterpret_cast<uint8_t*>(ks == k0 ? k1 : k0);
-  uint16_t* S = (is == i0) ? i1 : i0;                                   // 2n
-  uint16_t* C = reinterpret_cast<uint16_t*>(kfree);                     // 2(n+1)
-  uint16_t* GE = reinterpret_cast<uint16_t*>(kfree) + (N + 1);          // 2n  (fits 4n+16)
-  const bool need_desc = outs.out[2] != nullptr || outs.out[3] != nullptr;
-  const bool need_mask = outs.out[0] != nullptr || outs.out[2] != nullptr;
-  if (need_desc) tie_groups(ks, m, S, GE, reinterpret_cast<int*>(scan));
-  uint32_t mtot = static_cast<uint32_t>(m);
-  if (need_mask) {
-    int b, e;
-    uint32_t c = chunk_prefix(m, [&](int p) { return mk == nullptr || mk[is[p]] != 0; }, b, e, scan, mtot);
-    for (int p = b; p < e; ++p) {
-      C[p] = static_cast<uint16_t>(c);
-      c += (mk == nullptr || mk[is[p]] != 0) ? 1u : 0u;
-    }
-    if (threadIdx.x == 0) C[m] = static_cast<uint16_t>(mtot);
-    __syncthreads();
-  }
-  // ranks buffer aliases the sorted keys (no longer needed once S is built)
-  float* rbuf = reinterpret_cast<float*>(ks);
-  const float qnan = __uint_as_float(kQuietNanBits);
-  for (int g = 0; g < 4; ++g) {
-    if (outs.out[g] == nullptr) continue;
-    for (int i = threadIdx.x; i < N; i += NT) rbuf[i] = qnan;
-    __syncthreads();
-    for (int p = threadIdx.x; p < m; p += NT) {
-      const int i = is[p];
-      const bool mv = (mk == nullptr || mk[i] != 0);
-      switch (g) {
-        case 0:
-          if (mv) rbuf[i] = static_cast<float>(C[p] + 1);
-          break;
-        case 1:
-          rbuf[i] = static_cast<float>(p + 1);
-          break;
-        case 2:
-          if (mv) {
-            const int s = S[p], e = GE[s];
-            rbuf[i] = static_cast<float>(static_cast<int>(mtot) - C[e] + (C[p] - C[s]) + 1);
-          }
-          break;
-        default: {
-          const int s = S[p], e = GE[s];
-          rbuf[i] = static_cast<float>(m - e + (p - s) + 1);
-        }
-      }
-    }
-    __syncthreads();
-    store_row_f32(outs.out[g] + row, rbuf, N);
-    __syncthreads();
   }
 }
 
@@ -607,52 +431,6 @@ template <int NT>
 constexpr int cap_of() { return NT * 16; }
 
 static int pick_nt(int n) { return n <= 4096 ? 256 : (n <= 8192 ? 512 : 1024); }
-
-size_t cs_rank_smem(int N) {
-  return CsRankLayout(N, SortScratch<1024>::bytes).total;
-}
-
-template <int NT>
-static cudaError_t launch_cs_rank_nt(const float* X, const uint8_t* mask, int T, int N, int desc, float* out,
-                                     int* status, cudaStream_t st) {
-  const size_t smem = CsRankLayout(N, SortScratch<NT>::bytes).total;
-  cudaError_t e = cudaFuncSetAttribute(k_cs_rank<NT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
-  if (e != cudaSuccess) return e;
-  k_cs_rank<NT, 16><<<T, NT, smem, st>>>(X, mask, N, desc, out, status);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_cs_rank(const float* X, const uint8_t* mask, int T, int N, int desc, float* out,
-                           int* status, cudaStream_t st) {
-  if (N > kSmemRankCap) return cudaErrorInvalidValue;
-  switch (pick_nt(N)) {
-    case 256: return launch_cs_rank_nt<256>(X, mask, T, N, desc, out, status, st);
-    case 512: return launch_cs_rank_nt<512>(X, mask, T, N, desc, out, status, st);
-    default: return launch_cs_rank_nt<1024>(X, mask, T, N, desc, out, status, st);
-  }
-}
-
-template <int NT>
-static cudaError_t launch_scan_nt(const float* X, const uint8_t* mask, int T, int N, ScanOut outs, int* status,
-                                  cudaStream_t st) {
-  const size_t smem = ScanLayout(N, SortScratch<NT>::bytes).total;
-  cudaError_t e = cudaFuncSetAttribute(k_param_scan<NT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
-  if (e != cudaSuccess) return e;
-  k_param_scan<NT, 16><<<T, NT, smem, st>>>(X, mask, N, outs, status);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_param_scan(const float* X, const uint8_t* mask, int T, int N, ScanOut outs, int* status,
-                              cudaStream_t st) {
-  if (N > kSmemRankCap) return cudaErrorInvalidValue;
-  switch (pick_nt(N)) {
-    case 256: return launch_scan_nt<256>(X, mask, T, N, outs, status, st);
-    case 512: return launch_scan_nt<512>(X, mask, T, N, outs, status, st);
-    default: return launch_scan_nt<1024>(X, mask, T, N, outs, status, st);
-  }
-}
 
 template <typename TF, typename TR>
 size_t rank_ic_smem(int N) {

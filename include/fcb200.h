@@ -82,8 +82,9 @@ void fcb_host_free(void* p);
  * Replaces cs_rank_gpu (src/cross_sectional_rank.cuh:90-99).
  * Returns -1 null/dim, -2 N > 2^24, -3 T*N > INT32_MAX.
  * Every N up to the cap is served: sections that fit one CTA's shared memory
- * (N <= 16384 for cs_rank / parameter_scan; about 11000 f32 and 8192 f64 for
- * the fused rank + IC entry points) are sorted there, wider ones by a
+ * (N <= 16384 for cs_rank, parameter_scan and f32 rank + IC of several
+ * factors; about 11000 f32 and 8192 f64 for single-factor rolling_ic) are
+ * sorted there, wider ones by a
  * global-memory radix sort per date with the same results (scratch from the
  * workspace, or stream-ordered cudaMallocAsync for the fcb_dev_* variants). */
 int fcb_cs_rank_f32(const float* x, const uint8_t* mask, int T, int N, int descending, float* out,
@@ -346,16 +347,24 @@ int fcb_dev_factor_corr_noalloc(const void* d_x, int dtype, const uint8_t* d_mas
  * batch holds many panels of uneven T x N on the current device; each run
  * computes, for every panel, what fcb_dev_rank_ic_panel (cs_rank ranks +
  * rolling_ic) and fcb_factor_corr compute for it alone -- bit for bit.
- * Rank + IC runs as persistent kernels taking (panel, date) items from device
- * queues; factor_corr follows; the sequence is captured once into a CUDA
- * graph and replayed.  All pointers are DEVICE pointers owned by the caller
- * and must stay valid for the batch's lifetime; runs are asynchronous on
- * `stream` (NULL = legacy stream). */
+ * Rank + IC of f32 panels runs the single-panel per-(date, factor) kernels in
+ * batched form: per kernel variant (N up to 2048 / 5120 / 8192 / 16384), one
+ * returns launch over every date of its panels, one rank launch over every
+ * (date, factor) section and, with learned splitters, one launch ranking the
+ * sections handed back to the radix sort.  f64 panels run persistent kernels
+ * taking (panel, date) items from device queues.  factor_corr follows; the
+ * sequence is captured once into a CUDA graph and replayed.  All pointers are
+ * DEVICE pointers owned by the caller and must stay valid for the batch's
+ * lifetime; runs are asynchronous on `stream` (NULL = legacy stream).  Every
+ * device buffer a batch needs is allocated by fcb_batch_create (and, for the
+ * graph's launch tables, on the first run or the first run after a
+ * configuration change), so run it once before capturing it elsewhere. */
 typedef struct fcb_batch fcb_batch;
 
 typedef struct fcb_panel {
-  int T, N, F;                 /* N within one CTA's shared memory (rank + IC: about
-                                  11000 f32, 8192 f64), else FCB_ERR_UNSUPPORTED  */
+  int T, N, F;                 /* N within one CTA's shared memory (rank + IC:
+                                  16384 f32, about 8192 f64), else
+                                  FCB_ERR_UNSUPPORTED                            */
   const void* X;               /* F factor planes, each (T,N), dtype_x           */
   const void* R;               /* (T,N) forward returns, dtype_r                 */
   const uint8_t* fmask;        /* (T,N) factor mask or NULL                      */
@@ -368,15 +377,19 @@ typedef struct fcb_panel {
                                   (f32 only, fitted, model F == F) or NULL       */
 } fcb_panel;
 
-/* Scheduling knobs.  None of them changes a result. */
+/* Scheduling knobs.  None of them changes a result.  f32 panels: a panel of
+ * width N runs in the narrowest kernel variant whose range holds it, the
+ * first two ranges being N <= min(nt_small_max, 2048) and
+ * N <= min(nt_mid_max, 5120) (then 8192, 16384); ctas_per_sm is not used.
+ * f64 panels: size classes of 256 / 512 / 1024-thread persistent CTAs. */
 typedef struct fcb_batch_config {
-  int nt_small_max;  /* largest N ranked by 256-thread CTAs (1..4096)            */
-  int nt_mid_max;    /* largest N ranked by 512-thread CTAs (..8192); larger N
-                        use 1024-thread CTAs                                    */
-  int ctas_per_sm;   /* persistent CTAs per SM per size class, 0 = all that fit  */
-  int concurrent;    /* 1: size classes run side by side with grids split by
-                        work; 0: one after another, each on the whole GPU        */
-  int order;         /* 1: items longest first; 0: panel order                   */
+  int nt_small_max;  /* f64: largest N ranked by 256-thread CTAs (1..4096)       */
+  int nt_mid_max;    /* f64: largest N ranked by 512-thread CTAs (..8192);
+                        larger N use 1024-thread CTAs                           */
+  int ctas_per_sm;   /* f64: persistent CTAs per SM per class, 0 = all that fit */
+  int concurrent;    /* 1: size classes (variants) run side by side; 0: one
+                        after another, each on the whole GPU                    */
+  int order;         /* 1: longest panels / items first; 0: panel order         */
   int learn_cap;     /* largest learned bucket before the radix fallback         */
 } fcb_batch_config;
 
@@ -398,7 +411,8 @@ int fcb_batch_run_per_panel(fcb_batch* b, void* stream);
  * in any run since the last call did not land. */
 int fcb_batch_status(fcb_batch* b);
 /* Measures the batch under alternative configurations (coordinate descent,
- * `reps` replays each) and keeps the fastest; the size-class boundaries tried
+ * `reps` replays each) and keeps the fastest; f32: variant boundaries, order,
+ * concurrency and the learned bucket cap; f64: the size-class boundaries tried
  * include the occupancy steps of each block size within the batch's range of
  * N.  cache_path (or NULL): a text
  * file of "signature<TAB>config ms" lines; a batch whose signature is found
