@@ -494,17 +494,15 @@ extern "C" int fcb_dev_parameter_scan_f32(const float* d_x, const uint8_t* d_mas
 // ---------------------------------------------------------------------------
 template <typename TF, typename TR>
 static int run_rank_ic(const RankIcArgs<TF, TR>& a, int* dst, cudaStream_t s, fcb_workspace& ws) {
-  if (rank_ic_fits_smem<TF, TR>(a.N)) {
-    if constexpr (std::is_same<TF, float>::value && std::is_same<TR, float>::value) {
-      if (a.F >= 2 && ric_items_fit(a.N) && a.rank_f_out == nullptr) {
-        // several factors: returns prepared once per date, one CTA per (date, factor)
-        void* prep;
-        FCB_TRY(ws.get(S_RICPREP, ric_prep_bytes(a.T, a.N, a.F), &prep));
-        return rc(launch_rank_ic_items(a, ric_prep_carve(prep, a.T, a.N, a.F), false, s));
-      }
+  if constexpr (std::is_same<TF, float>::value && std::is_same<TR, float>::value) {
+    if (a.F >= 2 && ric_items_fit(a.N) && a.rank_f_out == nullptr) {
+      // several factors: returns prepared once per date, one CTA per (date, factor)
+      void* prep;
+      FCB_TRY(ws.get(S_RICPREP, ric_prep_bytes(a.T, a.N, a.F), &prep));
+      return rc(launch_rank_ic_items(a, ric_prep_carve(prep, a.T, a.N, a.F), false, s));
     }
-    return rc(launch_rank_ic<TF, TR>(a, dst, s));
   }
+  if (rank_ic_fits_smem<TF, TR>(a.N)) return rc(launch_rank_ic<TF, TR>(a, dst, s));
   const size_t bytes =
       rank_global_scratch(rank_global_bytes_per_date(2, a.N, a.F, sizeof(TF), sizeof(TR)), a.T);
   uint8_t* scr;
@@ -642,8 +640,7 @@ extern "C" int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const u
   FCB_TRY(dev_status_sink(&d_status));
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (rank_ic_fits_smem<float, float>(N)) {
-    if (F < 2 || !ric_items_fit(N)) return rc(launch_rank_ic<float, float>(a, d_status, s));
+  if (F >= 2 && ric_items_fit(N)) {
     // several factors: returns prepared once per date, one CTA per (date, factor)
     void* prep = nullptr;
     FCB_TRY(scratch_alloc(&prep, ric_prep_bytes(T, N, F), s));
@@ -651,6 +648,7 @@ extern "C" int fcb_dev_rank_ic_panel(const float* d_x, const float* d_r, const u
     FCB_TRY(scratch_free(prep, s));
     return rc(e);
   }
+  if (rank_ic_fits_smem<float, float>(N)) return rc(launch_rank_ic<float, float>(a, d_status, s));
   // global-memory path; scratch is stream-ordered (no host synchronisation)
   const size_t bytes = rank_global_scratch(rank_global_bytes_per_date(2, N, F, 4, 4), T);
   void* scr = nullptr;
@@ -718,9 +716,9 @@ extern "C" int fcb_rank_ic_panel(const float* x, const float* r, const uint8_t* 
     }
   }
   const int nchunk = static_cast<int>(chunk_tc.size());
-  // learned splitters need the shared-memory kernel; wider sections are ranked
+  // learned splitters need a shared-memory kernel; wider sections are ranked
   // by the global-memory radix path (identical results)
-  const bool learned = (method == 1) && rank_ic_fits_smem<float, float>(N);
+  const bool learned = (method == 1) && (F >= 2 ? ric_items_fit(N) : rank_ic_fits_smem<float, float>(N));
   const bool need_ranks = ranks != nullptr || learned;
   float* dx[NB];
   float* dr[NB];
@@ -1133,5 +1131,128 @@ extern "C" int fcb_stock_corr_prec(const float* x, const uint8_t* mask, int T, i
   if (e != FCB_OK) return e;
   FCB_TRY(cudaMemcpyAsync(out, dout, static_cast<size_t>(N) * N * 8, cudaMemcpyDeviceToHost, s));
   FCB_TRY(cudaStreamSynchronize(s));
+  return FCB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// memory budget model
+// ---------------------------------------------------------------------------
+// Device bytes the workspace of each host / device entry point requests for
+// one call of the given shape: the sum of its slots, written next to (and
+// checked on a GPU against the high-water accounting of) the entry points
+// above.  The counterpart of the reference's memory budget table
+// (docs/memory_budget_v1.json, src/mem_tracker.h:35-77).
+namespace {
+inline uint64_t slot_bytes(size_t b) { return b == 0 ? 16 : b; }
+
+uint64_t budget_dev_factor_corr(int dtype, long long R, int F) {
+  (void)dtype;
+  const int Fp = (F + 3) / 4 * 4;
+  const long long nbc = std::min<long long>(592, std::max<long long>(1, R / 2048));
+  const long long nbg = fc_gram_blocks(R, F);
+  return slot_bytes(static_cast<size_t>(nbc) * F * sizeof(FcColPart)) + slot_bytes(static_cast<size_t>(F) * sizeof(FcColStat)) +
+         slot_bytes(static_cast<size_t>(nbg) * 4 * Fp * Fp * 8) + slot_bytes(static_cast<size_t>(F) * F * 4) + 64 +
+         slot_bytes(fc_fb_part_doubles(R, F) * sizeof(double));
+}
+
+uint64_t budget_dev_stock_corr(int T, int N) {
+  const size_t Tp = static_cast<size_t>((T + 31) / 32 * 32);
+  const size_t upper = static_cast<size_t>(N) * (N - 1) / 2;
+  return 3 * slot_bytes(static_cast<size_t>(N) * Tp * 8) + slot_bytes(static_cast<size_t>(N) * sizeof(ColStat)) + 64 +
+         slot_bytes((upper > 0 ? upper : 1) * 4) + 64;
+}
+}  // namespace
+
+extern "C" int fcb_memory_budget(int op, int dtype, int T, int N, int F, int flags, uint64_t* bytes) {
+  if (bytes == nullptr || T < 1 || N < 1 || F < 1) return FCB_ERR_ARG;
+  if (static_cast<long long>(T) * N > INT32_MAX) return FCB_ERR_CAP3;
+  const bool m1 = (flags & FCB_BUDGET_MASK) != 0, m2 = (flags & FCB_BUDGET_MASK2) != 0;
+  const bool ranks = (flags & FCB_BUDGET_RANKS) != 0;
+  const size_t n = static_cast<size_t>(T) * N;
+  const long long R = static_cast<long long>(T) * N;
+  uint64_t b = 0;
+  switch (op) {
+    case FCB_OP_CS_RANK:
+      b = slot_bytes(n * 4) * 2 + 64 + (m1 ? slot_bytes(n) : 0);
+      if (N > kSmemRankCap) b += slot_bytes(rank_global_scratch(rank_global_bytes_per_date(0, N, 1, 4, 4), T));
+      break;
+    case FCB_OP_PARAMETER_SCAN: {
+      const int groups = (flags >> 8) & 0xF;
+      const int nact = groups == 0 ? 4 : __builtin_popcount(groups);
+      b = slot_bytes(n * 4) + 64 + (m1 ? slot_bytes(n) : 0) + static_cast<uint64_t>(nact) * slot_bytes(n * 4);
+      if (N > kSmemRankCap) b += slot_bytes(rank_global_scratch(rank_global_bytes_per_date(1, N, 1, 4, 4), T));
+      break;
+    }
+    case FCB_OP_ROLLING_IC: {
+      // dtype: the factor's; FCB_BUDGET_R_F64: the returns are f64
+      const int fsz = dtype == FCB_DTYPE_F64 ? 8 : 4, rsz = (flags & FCB_BUDGET_R_F64) ? 8 : 4;
+      b = slot_bytes(n * fsz) + slot_bytes(n * rsz) + slot_bytes(static_cast<size_t>(T) * 8) + 64 +
+          (m1 ? slot_bytes(n) : 0) + (m2 ? slot_bytes(n) : 0) + (ranks ? 2 * slot_bytes(n * 8) : 0);
+      const bool fits = (fsz == 4 && rsz == 4)   ? rank_ic_fits_smem<float, float>(N)
+                        : (fsz == 4)             ? rank_ic_fits_smem<float, double>(N)
+                        : (rsz == 4)             ? rank_ic_fits_smem<double, float>(N)
+                                                 : rank_ic_fits_smem<double, double>(N);
+      if (!fits) b += slot_bytes(rank_global_scratch(rank_global_bytes_per_date(2, N, 1, fsz, rsz), T));
+      break;
+    }
+    case FCB_OP_DEV_FACTOR_CORR:
+      if (F > 128) return FCB_ERR_CAP3;
+      b = budget_dev_factor_corr(dtype, R, F);
+      break;
+    case FCB_OP_FACTOR_CORR: {
+      if (F > 128) return FCB_ERR_CAP3;
+      const size_t esz = dtype == FCB_DTYPE_F64 ? 8 : 4;
+      b = budget_dev_factor_corr(dtype, R, F) + slot_bytes(static_cast<size_t>(R) * F * esz) +
+          (m1 ? slot_bytes(static_cast<size_t>(R)) : 0) + slot_bytes(static_cast<size_t>(F) * F * 8) +
+          ((flags & FCB_BUDGET_FALLBACK) ? slot_bytes(static_cast<size_t>(F) * F) : 0);
+      break;
+    }
+    case FCB_OP_DEV_STOCK_CORR:
+      if (static_cast<long long>(N) * N > INT32_MAX) return FCB_ERR_CAP3;
+      b = budget_dev_stock_corr(T, N);
+      break;
+    case FCB_OP_STOCK_CORR: {
+      if (static_cast<long long>(N) * N > INT32_MAX) return FCB_ERR_CAP3;
+      const size_t esz = dtype == FCB_DTYPE_F64 ? 8 : 4;
+      b = budget_dev_stock_corr(T, N) + slot_bytes(n * esz) + (m1 ? slot_bytes(n) : 0) +
+          slot_bytes(static_cast<size_t>(N) * N * 8);
+      break;
+    }
+    case FCB_OP_FACTOR_CORR_BF16X3:
+      if (F > kFcTcMaxF) return FCB_ERR_UNSUPPORTED;
+      b = slot_bytes(static_cast<size_t>(R) * F * 4) + (m1 ? slot_bytes(static_cast<size_t>(R)) : 0) +
+          slot_bytes(static_cast<size_t>(F) * F * 8) + slot_bytes(fc_tc_work_bytes(F)) + 64;
+      break;
+    case FCB_OP_STOCK_CORR_PREC: {
+      // dtype: the precision mode (FCB_PREC_BF16X3 / FCB_PREC_FP32)
+      if (static_cast<long long>(N) * N > INT32_MAX) return FCB_ERR_CAP3;
+      const size_t Np = static_cast<size_t>((N + 127) / 128 * 128), Tp = static_cast<size_t>((T + 31) / 32 * 32);
+      const size_t e = Np * Tp;
+      const int mode = dtype == FCB_PREC_FP32 ? 1 : 0;
+      b = slot_bytes(n * 4) + (m1 ? slot_bytes(n) : 0) + slot_bytes(static_cast<size_t>(N) * N * 8) +
+          slot_bytes(Np * 4) + 64 + (mode == 0 ? slot_bytes(e * 2 * 7) : 3 * slot_bytes(e * 4)) +
+          slot_bytes(static_cast<size_t>(prec_tile_count(mode, N)) * sizeof(int2)) +
+          slot_bytes(static_cast<size_t>(prec_colmean_chunks(T)) * Np * sizeof(double2));
+      break;
+    }
+    case FCB_OP_RANK_IC_PANEL: {
+      // method 0 (radix); the chunk schedule of fcb_rank_ic_panel
+      const size_t per_date = static_cast<size_t>(F) * N * 4;
+      int Tc = static_cast<int>((64ull << 20) / per_date);
+      Tc = std::max(1, std::min(Tc, T));
+      const size_t cn = static_cast<size_t>(Tc) * N;
+      b = 64 + slot_bytes(static_cast<size_t>(F) * T * 8) +
+          3 * (slot_bytes(cn * F * 4) + slot_bytes(cn * 4) + (m1 ? slot_bytes(cn) : 0) + (m2 ? slot_bytes(cn) : 0) +
+               (ranks ? slot_bytes(cn * F * 4) : 0));
+      if (F >= 2 && ric_items_fit(N))
+        b += slot_bytes(ric_prep_bytes(Tc, N, F));
+      else if (!rank_ic_fits_smem<float, float>(N))
+        b += slot_bytes(rank_global_scratch(rank_global_bytes_per_date(2, N, F, 4, 4), Tc));
+      break;
+    }
+    default:
+      return FCB_ERR_ARG;
+  }
+  *bytes = b;
   return FCB_OK;
 }

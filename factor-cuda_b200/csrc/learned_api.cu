@@ -252,8 +252,7 @@ int fcb::rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr,
                              model->table[model->cur], model->zrange[model->cur], cap > 0 ? cap : 64, d_stats,
                              ic_ld};
-  if (rank_ic_fits_smem<float, float>(N)) {
-    if (F < 2 || !ric_items_fit(N)) return rc(launch_rank_ic_learned(a, d_status, stream));
+  if (F >= 2 && ric_items_fit(N)) {
     // several factors: returns prepared once per date, one CTA per (date, factor)
     void* prep = nullptr;
     FCB_TRY(scratch_alloc(&prep, ric_prep_bytes(T, N, F), stream));
@@ -261,6 +260,7 @@ int fcb::rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d
     FCB_TRY(scratch_free(prep, stream));
     return rc(e);
   }
+  if (rank_ic_fits_smem<float, float>(N)) return rc(launch_rank_ic_learned(a, d_status, stream));
   // too wide for the shared-memory kernel: the global-memory radix path ranks
   // the section (identical results); statistics read outcome 0 (not learned)
   if (d_stats != nullptr)

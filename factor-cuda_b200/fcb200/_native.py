@@ -54,6 +54,7 @@ PROTOTYPES = {
     "fcb_workspace_clear": (None, [_p]),
     "fcb_workspace_destroy": (None, [_p]),
     "fcb_workspace_stats": (_i, [_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "fcb_memory_budget": (_i, [_i, _i, _i, _i, _i, _i, C.POINTER(C.c_uint64)]),
     "fcb_workspace_learned_state": (_i, [_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
     "fcb_version": (_i, []),
     "fcb_device_count": (_i, []),

@@ -62,6 +62,38 @@ void fcb_workspace_destroy(fcb_workspace* ws);
 int fcb_workspace_stats(const fcb_workspace* ws, uint64_t* live_bytes, uint64_t* peak_bytes,
                         uint64_t* n_allocs);
 
+/* Memory budget model (the counterpart of the reference's budget table,
+ * docs/memory_budget_v1.json, and of MemTracker's peak, src/mem_tracker.h:
+ * 35-77): *bytes = the device bytes the workspace of entry point `op` holds
+ * after one call of shape (T, N, F) -- the sum of its buffers, which is the
+ * workspace's peak (fcb_workspace_stats) for a fresh workspace.  Buffers the
+ * driver rounds up to its allocation granularity can occupy a little more of
+ * the device.  flags: FCB_BUDGET_MASK a (first) mask is passed,
+ * FCB_BUDGET_MASK2 a second mask (rolling_ic rmask, panel rmask),
+ * FCB_BUDGET_RANKS rank outputs (rolling_ic rank_f / rank_r, panel ranks),
+ * FCB_BUDGET_FALLBACK factor_corr fallback_out, FCB_BUDGET_R_F64 rolling_ic
+ * returns are f64; bits 8-11: parameter_scan active groups (0 = all four).
+ * dtype: the input dtype; for FCB_OP_STOCK_CORR_PREC the precision mode.
+ * FCB_OP_RANK_IC_PANEL covers method 0; FCB_OP_FACTOR_CORR and
+ * FCB_OP_STOCK_CORR count the host entry points' own temporary workspace.
+ * Returns -1 unknown op / bad shape, -3 size cap, -5 unsupported shape. */
+#define FCB_OP_CS_RANK 1
+#define FCB_OP_PARAMETER_SCAN 2
+#define FCB_OP_ROLLING_IC 3
+#define FCB_OP_FACTOR_CORR 4
+#define FCB_OP_DEV_FACTOR_CORR 5
+#define FCB_OP_STOCK_CORR 6
+#define FCB_OP_DEV_STOCK_CORR 7
+#define FCB_OP_FACTOR_CORR_BF16X3 8
+#define FCB_OP_STOCK_CORR_PREC 9
+#define FCB_OP_RANK_IC_PANEL 10
+#define FCB_BUDGET_MASK 1
+#define FCB_BUDGET_MASK2 2
+#define FCB_BUDGET_RANKS 4
+#define FCB_BUDGET_FALLBACK 8
+#define FCB_BUDGET_R_F64 16
+int fcb_memory_budget(int op, int dtype, int T, int N, int F, int flags, uint64_t* bytes);
+
 /* Learned-splitter state a workspace carries across fcb_rank_ic_panel calls
  * (method 1): ready = a fitted table is in use, fits = refits scheduled so
  * far, learned_chunks = date chunks ranked by the learned kernel so far. */

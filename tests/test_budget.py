@@ -1,0 +1,128 @@
+"""Memory budget model (fcb_memory_budget): predicted device bytes of each
+entry point's workspace for one call, the counterpart of the reference's
+budget table (docs/memory_budget_v1.json) and MemTracker peak
+(src/mem_tracker.h:35-77).
+
+CPU: the prediction is the documented sum of buffers (inputs, outputs,
+scratch) and rejects bad requests.  GPU: after one call through a fresh
+workspace, the workspace's high-water accounting equals the prediction, and
+the device's free memory dropped by at least that much."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+OP = {"cs_rank": 1, "parameter_scan": 2, "rolling_ic": 3, "factor_corr": 4, "dev_factor_corr": 5,
+      "stock_corr": 6, "dev_stock_corr": 7, "factor_corr_bf16x3": 8, "stock_corr_prec": 9, "rank_ic_panel": 10}
+MASK, MASK2, RANKS, FALLBACK, R_F64 = 1, 2, 4, 8, 16
+
+
+@pytest.fixture(scope="module")
+def nat():
+    import fcb_build
+    fcb_build.build()
+    from fcb200 import _native
+    return _native
+
+
+def budget(nat, op, dtype, T, N, F, flags=0):
+    out = C.c_uint64()
+    rc = nat.lib().fcb_memory_budget(OP[op], dtype, T, N, F, flags, C.byref(out))
+    return rc, out.value
+
+
+def test_budget_sums_the_documented_buffers(nat):
+    T, N = 1218, 5000
+    n = T * N
+    rc, b = budget(nat, "cs_rank", 0, T, N, 1, MASK)
+    assert rc == 0 and b == 2 * 4 * n + 64 + n          # x, ranks, status word, mask
+    rc, b_all = budget(nat, "parameter_scan", 0, T, N, 1, MASK)
+    rc2, b_two = budget(nat, "parameter_scan", 0, T, N, 1, MASK | (0b0101 << 8))
+    assert rc == rc2 == 0 and b_all - b_two == 2 * 4 * n  # two fewer group outputs
+    rc, b = budget(nat, "rolling_ic", 1, T, N, 1, MASK | MASK2 | RANKS | R_F64)
+    assert rc == 0 and b == 8 * n + 8 * n + 8 * T + 64 + 2 * n + 2 * 8 * n
+    rc, bh = budget(nat, "factor_corr", 0, T, N, 12, MASK)
+    rc2, bd = budget(nat, "dev_factor_corr", 0, T, N, 12, MASK)
+    assert rc == rc2 == 0 and bh - bd == n * 12 * 4 + n + 12 * 12 * 8
+    rc, bh = budget(nat, "stock_corr", 1, T, 2000, 1, MASK)
+    rc2, bd = budget(nat, "dev_stock_corr", 1, T, 2000, 1, 0)
+    assert rc == rc2 == 0 and bh - bd == T * 2000 * 8 + T * 2000 + 2000 * 2000 * 8
+    # the prepared returns of the per-(date, factor) kernels are part of the panel's budget
+    rc, b = budget(nat, "rank_ic_panel", 0, T, N, 12, MASK | MASK2 | RANKS)
+    assert rc == 0 and b > 3 * (2 * 12 * 4 + 4 + 2) * 5000
+    rc, b16 = budget(nat, "factor_corr_bf16x3", 0, T, N, 16, 0)
+    assert rc == 0 and b16 > n * 16 * 4
+    assert budget(nat, "factor_corr_bf16x3", 0, T, N, 17, 0)[0] == -5
+    assert budget(nat, "factor_corr", 0, T, N, 129, 0)[0] == -3
+    assert budget(nat, "stock_corr", 0, 10, 46341, 1, 0)[0] == -3
+    assert nat.lib().fcb_memory_budget(99, 0, 2, 2, 1, 0, C.byref(C.c_uint64())) == -1
+    assert nat.lib().fcb_memory_budget(1, 0, 2, 2, 1, 0, None) == -1
+
+
+@pytest.mark.gpu
+def test_budget_matches_workspace_peak(nat):
+    torch = pytest.importorskip("torch")
+    if nat.device_count() < 1:
+        pytest.skip("no CUDA device")
+    lib = nat.lib()
+    rng = np.random.default_rng(5)
+    P = nat.ptr
+    T, N, F = 300, 2500, 6
+    x = rng.standard_normal((T, N)).astype(np.float32)
+    m = (rng.random((T, N)) < 0.9).astype(np.uint8)
+    outs = [np.empty((T, N), np.float32) for _ in range(4)]
+
+    def peak_after(call):
+        ws = lib.fcb_workspace_create()
+        try:
+            torch.cuda.synchronize()
+            free0, _ = torch.cuda.mem_get_info()
+            nat.check(call(ws), "call")
+            free1, _ = torch.cuda.mem_get_info()
+            live, peak, nal = C.c_uint64(), C.c_uint64(), C.c_uint64()
+            lib.fcb_workspace_stats(ws, C.byref(live), C.byref(peak), C.byref(nal))
+            return peak.value, free0 - free1
+        finally:
+            lib.fcb_workspace_destroy(ws)
+
+    checks = []
+    checks.append(("cs_rank", 0, T, N, 1, MASK,
+                   lambda ws: lib.fcb_cs_rank_f32(P(x), P(m), T, N, 0, P(outs[0]), ws)))
+    optr = (C.c_void_p * 4)(*[P(o) for o in outs])
+    st = (C.c_int * 4)()
+    checks.append(("parameter_scan", 0, T, N, 1, MASK,
+                   lambda ws: lib.fcb_parameter_scan_f32(P(x), P(m), T, N, optr, st, None, None, None, ws)))
+    r64 = rng.standard_normal((T, N))
+    ic = np.empty(T)
+    rf, rr = np.empty((T, N)), np.empty((T, N))
+    checks.append(("rolling_ic", 0, T, N, 1, MASK | MASK2 | RANKS | R_F64,
+                   lambda ws: lib.fcb_rolling_ic(P(x), 0, P(r64), 1, P(m), P(m), T, N, 30, P(ic), P(rf), P(rr), ws)))
+    X3 = rng.standard_normal((T, N, F)).astype(np.float32)
+    fo = np.empty((F, F))
+    checks.append(("factor_corr_bf16x3", 0, T, N, F, MASK,
+                   lambda ws: lib.fcb_factor_corr_bf16x3(P(X3), P(m), T, N, F, P(fo), ws)))
+    XF = np.ascontiguousarray(np.moveaxis(X3, -1, 0))
+    rk = np.empty((F, T, N), np.float32)
+    icp = np.empty((F, T))
+    checks.append(("rank_ic_panel", 0, T, N, F, MASK | MASK2 | RANKS,
+                   lambda ws: lib.fcb_rank_ic_panel(P(XF), P(x), P(m), P(m), F, T, N, 30, P(rk), P(icp), 0, ws)))
+    S = rng.standard_normal((T, 700)).astype(np.float32)
+    sm = (rng.random((T, 700)) < 0.95).astype(np.uint8)
+    so = np.empty((700, 700))
+    checks.append(("stock_corr_prec", 0, T, 700, 1, MASK,
+                   lambda ws: lib.fcb_stock_corr_prec(P(S), P(sm), T, 700, 0, P(so), ws)))
+    dX = torch.from_numpy(X3).cuda()
+    dm = torch.from_numpy(m).cuda()
+    dfo = torch.empty((F, F), dtype=torch.float64, device="cuda")
+    s0 = torch.cuda.current_stream().cuda_stream
+    checks.append(("dev_factor_corr", 0, T, N, F, MASK,
+                   lambda ws: lib.fcb_dev_factor_corr(dX.data_ptr(), 0, dm.data_ptr(), T, N, F, 0, dfo.data_ptr(),
+                                                      ws, s0)))
+    for op, dt, t, n, f, flags, call in checks:
+        rc, pred = budget(nat, op, dt, t, n, f, flags)
+        assert rc == 0, op
+        peak, dropped = peak_after(call)
+        assert peak == pred, (op, peak, pred)
+        # the driver rounds large buffers up to its granularity; a few small
+        # ones (status words) may land in memory it had already reserved
+        assert dropped >= pred - 65536, (op, dropped, pred)
