@@ -881,35 +881,26 @@ __global__ void __launch_bounds__(NT) k_csr(const float* __restrict__ X, const u
 //   desc unmasked m - E + (p - S) + 1    desc masked  mt - C[E] + (C[p] - C[S]) + 1
 // (descending ranks keep ties by ascending column, the contract of
 // fc/_cpu_core.py:57-78 / :295-301; replaces the reference's four rank
-// pipelines, src/cross_sectional_rank.cu:401-664).
-template <int NT>
-struct ScanLayout2 {
-  size_t s_cnt, s_ge, total;
-  __host__ __device__ explicit ScanLayout2(int n) {
-    size_t o = SortedLayout<NT>(n).total;
-    s_cnt = o; o = al16(o + size_t(n + 1) * 2);
-    s_ge = o; o = al16(o + size_t(n) * 2);
-    total = o;
-  }
-};
-
+// pipelines, src/cross_sectional_rank.cu:401-664).  Shared memory stays at
+// the sort's 12 bytes per cell: tie-group starts go to a bitmap (the sorted
+// keys are then free for C and E), and the ascending and descending pairs of
+// ranks pass through one per-column buffer in turn.
 template <int NT, int V>
 __global__ void __launch_bounds__(NT) k_pscan(const float* __restrict__ X, const uint8_t* __restrict__ mask, int N,
                                               ScanOut outs) {
   constexpr int C = 4 * V;
   extern __shared__ __align__(16) uint8_t sm[];
   const SortedLayout<NT> L(N);
-  const ScanLayout2<NT> L2(N);
   unsigned long long* scan64 = reinterpret_cast<unsigned long long*>(sm + L.red);
   uint32_t* scan32 = reinterpret_cast<uint32_t*>(sm + L.red);
+  uint32_t* bits = reinterpret_cast<uint32_t*>(sm + L.dw);  // tie-group start per sorted position
   uint32_t* k0 = reinterpret_cast<uint32_t*>(sm + L.k0);
   uint32_t* k1 = reinterpret_cast<uint32_t*>(sm + L.k1);
   uint16_t* i0 = reinterpret_cast<uint16_t*>(sm + L.i0);
   uint16_t* i1 = reinterpret_cast<uint16_t*>(sm + L.i1);
-  uint16_t* Cn = reinterpret_cast<uint16_t*>(sm + L2.s_cnt);
-  uint16_t* GE = reinterpret_cast<uint16_t*>(sm + L2.s_ge);
   const int tid = static_cast<int>(threadIdx.x);
   const size_t row = static_cast<size_t>(blockIdx.x) * N;
+  for (int k = tid; k < (N + 31) / 32 + 1; k += NT) bits[k] = 0u;
   float x[C];
   uint32_t mk[C];
   load_row_f32<NT, V, true>(X + row, N, x);
@@ -921,7 +912,7 @@ __global__ void __launch_bounds__(NT) k_pscan(const float* __restrict__ X, const
     msk |= (mk[c] ? 1u : 0u) << c;
   }
   int base[V];
-  const int m = compact_bases<NT, V>(fin, base, scan64);
+  const int m = compact_bases<NT, V>(fin, base, scan64);  // its barriers publish the bitmap clear
 #pragma unroll
   for (int j = 0; j < V; ++j) {
     int p = base[j];
@@ -939,20 +930,24 @@ __global__ void __launch_bounds__(NT) k_pscan(const float* __restrict__ X, const
   uint32_t* ks;
   uint16_t* is;
   block_radix_sort<NT, C, uint32_t>(k0, i0, k1, i1, m, sm + L.scratch, &ks, &is);
-  uint16_t* S = (is == i0) ? i1 : i0;                  // tie-group start per sorted position
-  uint32_t* O01 = (ks == k0) ? k1 : k0;                // (asc masked | asc unmasked << 16) per column
-  uint32_t* O23 = ks;                                   // (desc masked | desc unmasked << 16), after ks is read
-  // pass 1: per chunk, masked-valid count and the last group start
+  uint16_t* S = (is == i0) ? i1 : i0;                                // group start per sorted position
+  uint32_t* O = (ks == k0) ? k1 : k0;                                // two ranks per column
+  uint16_t* Cn = reinterpret_cast<uint16_t*>(ks);                    // m + 1 entries, over the sorted keys
+  uint16_t* GE = reinterpret_cast<uint16_t*>(ks) + (N + 1);          // group end by group start
+  // pass 1: per chunk, masked-valid count, last group start, start bits
   const int per = (m + NT - 1) / NT;
   const int b0 = tid * per, b1 = min(m, b0 + per);
   uint32_t cm = 0;
   int last = -1;
   for (int p = b0; p < b1; ++p) {
     cm += is[p] >> 15;
-    if (p == 0 || ks[p] != ks[p - 1]) last = p;
+    if (p == 0 || ks[p] != ks[p - 1]) {
+      last = p;
+      atomicOr(&bits[p >> 5], 1u << (p & 31));
+    }
   }
   uint32_t mt;
-  uint32_t c = block_exclusive_sum(cm, scan32, mt);
+  uint32_t c = block_exclusive_sum(cm, scan32, mt);  // barriers: ks reads done, bits complete
   // exclusive max-scan of the chunks' last group starts (identity -1)
   int inc = last;
 #pragma unroll
@@ -968,47 +963,52 @@ __global__ void __launch_bounds__(NT) k_pscan(const float* __restrict__ X, const
   for (int i = 0; i < wi; ++i) carry = max(carry, sc[i]);
   const int up = __shfl_up_sync(kFull, inc, 1);
   if (lane_id() > 0) carry = max(carry, up);
-  // pass 2: S, the masked-valid prefix and the group ends
+  // pass 2: S, the masked-valid prefix C and the group ends E
+  auto is_start = [&](int p) { return ((bits[p >> 5] >> (p & 31)) & 1u) != 0u; };
   for (int p = b0; p < b1; ++p) {
-    if (p == 0 || ks[p] != ks[p - 1]) carry = p;
+    if (is_start(p)) carry = p;
     S[p] = static_cast<uint16_t>(carry);
     Cn[p] = static_cast<uint16_t>(c);
     c += is[p] >> 15;
-    if (p == m - 1 || ks[p] != ks[p + 1]) GE[carry] = static_cast<uint16_t>(p + 1);
+    if (p == m - 1 || is_start(p + 1)) GE[carry] = static_cast<uint16_t>(p + 1);
   }
   if (tid == 0) Cn[m] = static_cast<uint16_t>(mt);
   __syncthreads();
-  // pass 3: the four ranks of each sorted position, by column
-  for (int p = tid; p < m; p += NT) {
-    const uint32_t id = is[p];
-    const int col = static_cast<int>(id & 0x3FFFu);
-    const int s0 = S[p], e0 = GE[s0];
-    const uint32_t cp = Cn[p];
-    const uint32_t g1 = static_cast<uint32_t>(p + 1);
-    const uint32_t g3 = static_cast<uint32_t>(m - e0 + (p - s0) + 1);
-    uint32_t g0 = 0u, g2 = 0u;
-    if (id & 0x8000u) {
-      g0 = cp + 1u;
-      g2 = mt - Cn[e0] + (cp - Cn[s0]) + 1u;
-    }
-    O01[col] = g0 | (g1 << 16);
-    O23[col] = g2 | (g3 << 16);
-  }
-  __syncthreads();
   const float qnan = __uint_as_float(kQuietNanBits);
-#pragma unroll
-  for (int g = 0; g < 4; ++g) {
-    if (outs.out[g] == nullptr) continue;  // uniform across the block
-    const uint32_t* src = (g < 2) ? O01 : O23;
-    const int sh = (g & 1) ? 16 : 0;
-    float v[C];
-#pragma unroll
-    for (int cc = 0; cc < C; ++cc) {
-      const uint32_t r =
-          ((fin >> cc) & 1u) ? ((src[4 * ((cc >> 2) * NT + tid) + (cc & 3)] >> sh) & 0xFFFFu) : 0u;
-      v[cc] = r ? static_cast<float>(r) : qnan;
+  // pass 3, twice: the ascending pair (groups 0 | 1), then the descending pair
+  // (groups 2 | 3), each stored by column and written out
+  for (int half = 0; half < 2; ++half) {
+    if (outs.out[2 * half] == nullptr && outs.out[2 * half + 1] == nullptr) continue;  // uniform
+    for (int p = tid; p < m; p += NT) {
+      const uint32_t id = is[p];
+      const uint32_t cp = Cn[p];
+      uint32_t lo = 0u, hi;
+      if (half == 0) {
+        hi = static_cast<uint32_t>(p + 1);
+        if (id & 0x8000u) lo = cp + 1u;
+      } else {
+        const int s0 = S[p], e0 = GE[s0];
+        hi = static_cast<uint32_t>(m - e0 + (p - s0) + 1);
+        if (id & 0x8000u) lo = mt - Cn[e0] + (cp - Cn[s0]) + 1u;
+      }
+      O[id & 0x3FFFu] = lo | (hi << 16);
     }
-    store_row_f32v<NT, V>(outs.out[g] + row, N, v);
+    __syncthreads();
+#pragma unroll
+    for (int g2 = 0; g2 < 2; ++g2) {
+      float* dst = outs.out[2 * half + g2];
+      if (dst == nullptr) continue;  // uniform
+      const int sh = g2 ? 16 : 0;
+      float v[C];
+#pragma unroll
+      for (int cc = 0; cc < C; ++cc) {
+        const uint32_t r =
+            ((fin >> cc) & 1u) ? ((O[4 * ((cc >> 2) * NT + tid) + (cc & 3)] >> sh) & 0xFFFFu) : 0u;
+        v[cc] = r ? static_cast<float>(r) : qnan;
+      }
+      store_row_f32v<NT, V>(dst + row, N, v);
+    }
+    __syncthreads();  // O is rewritten by the second half
   }
 }
 
@@ -1088,7 +1088,7 @@ cudaError_t csr_launch(const float* X, const uint8_t* mask, int T, int N, int de
 }
 template <int NT, int V>
 cudaError_t pscan_launch(const float* X, const uint8_t* mask, int T, int N, ScanOut outs, cudaStream_t st) {
-  const size_t smem = ScanLayout2<NT>(N).total;
+  const size_t smem = SortedLayout<NT>(N).total;
   if (smem > kMaxSmemPerBlock) return cudaErrorInvalidValue;
   cudaError_t e =
       cudaFuncSetAttribute(k_pscan<NT, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
