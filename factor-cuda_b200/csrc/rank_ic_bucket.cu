@@ -455,7 +455,7 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
   // (mean and mean absolute deviation of up to 256 valid cells; they only
   // shape the bucket map -- the order is exact whatever they are)
   if (wi == 0) {
-    const int S = min(N, 256);
+    const int S = min(N, 256);  // i = s*N/S: s*N/256 when N >= 256, else s
     float xs[8];
     uint32_t vs = 0u;
     int ns = 0;
@@ -465,7 +465,7 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
       const int s = q * 32 + lane;
       xs[q] = 0.0f;
       if (s < S) {
-        const int i = static_cast<int>((static_cast<long long>(s) * N) / S);
+        const int i = N >= 256 ? (s * N) >> 8 : s;
         const float v = a.X[frow + i];
         if (finite_f32(v) && (rp.word[static_cast<size_t>(t) * rp.ld + i] & kFacMask)) {
           xs[q] = v;
@@ -534,18 +534,20 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
     }
   }
   __syncthreads();  // B2
-  // ---- scan of the m + 1 counters (the last is the total), warp segments
-  const int E = m + 1;
-  const int seg = ((E + NW - 1) / NW + 31) & ~31;
-  const int s0 = min(E, wi * seg), s1 = min(E, s0 + seg);
+  // ---- scan of the m + 1 counters (the last is the total): each warp takes a
+  // segment in 128-counter steps, four counters per lane (one 16-byte access);
+  // counters past m + 1 up to the next multiple of four are zero
+  const int E4 = (m + 1 + 3) & ~3;
+  const int seg = ((E4 + NW - 1) / NW + 127) & ~127;
+  const int s0 = min(E4, wi * seg), s1 = min(E4, s0 + seg);
   {
     uint32_t tot = 0, mx = 0, sq = 0;
-    for (int i = s0 + lane; i < s1; i += 32) {
-      const uint32_t v = cnt[i];
-      const uint32_t lo16 = v & 0xFFFFu;
-      tot += v;
-      mx = max(mx, lo16);
-      sq += lo16 * lo16;
+    for (int i = s0 + 4 * lane; i < s1; i += 128) {
+      const uint4 v = *reinterpret_cast<const uint4*>(cnt + i);
+      tot += v.x + v.y + v.z + v.w;
+      const uint32_t a = v.x & 0xFFFFu, b = v.y & 0xFFFFu, c2 = v.z & 0xFFFFu, d = v.w & 0xFFFFu;
+      mx = max(mx, max(max(a, b), max(c2, d)));
+      sq += a * a + b * b + c2 * c2 + d * d;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -589,11 +591,14 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
     stats[2] = static_cast<int>(sqall);
     stats[3] = m;
   }
-  for (int base = s0; base < s1; base += 32) {
-    const int i = base + lane;
-    const uint32_t v = i < s1 ? cnt[i] : 0u;
-    const uint32_t inc = warp_inclusive_sum(v);
-    if (i < s1) cnt[i] = off + inc - v;
+  for (int base = s0; base < s1; base += 128) {
+    const int i = base + 4 * lane;
+    const bool in = i < s1;
+    const uint4 v = in ? *reinterpret_cast<const uint4*>(cnt + i) : make_uint4(0u, 0u, 0u, 0u);
+    const uint32_t a0 = v.x, a1 = a0 + v.y, a2 = a1 + v.z, a3 = a2 + v.w;
+    const uint32_t inc = warp_inclusive_sum(a3);
+    const uint32_t ex = off + inc - a3;
+    if (in) *reinterpret_cast<uint4*>(cnt + i) = make_uint4(ex, ex + a0, ex + a1, ex + a2);
     off += __shfl_sync(kFull, inc, 31);
   }
   __syncthreads();  // B4
@@ -619,6 +624,8 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
           (static_cast<unsigned long long>(key[c]) << 32) | (i << 1) | (joint ? 1u : 0u);
       const uint32_t s = cnt[b], e = cnt[b + 1];
       uint32_t r = 0, rj = 0;
+      // a bucket of one is the cell itself
+      if ((e & 0xFFFFu) - (s & 0xFFFFu) > 1u)
       for (uint32_t p = s & 0xFFFFu; p < (e & 0xFFFFu); ++p) {
         const unsigned long long o = mem[p];
         const uint32_t lt = o < mine ? 1u : 0u;
@@ -640,8 +647,10 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
   ric_epilogue<NT, V, true>(a, rp, t, f, P, key, 0u, 0u, mj, dw, red, bad, stats, item_id, fb);
 }
 
+// 256-thread CTAs keep to 80 registers so that three fit an SM (the shared
+// memory of N <= 5120 allows three)
 template <int NT, int V>
-__global__ void __launch_bounds__(NT) k_ric_learned(RankIcArgs<float, float> a, RicPrep rp) {
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_ric_learned(RankIcArgs<float, float> a, RicPrep rp) {
   extern __shared__ __align__(16) uint8_t sm[];
   const int item = static_cast<int>(blockIdx.x);
   ric_learned_body<NT, V>(a, rp, item / a.F, item % a.F, item, RicList{rp.fb_count, rp.fb_items}, sm);
@@ -786,7 +795,7 @@ __global__ void __launch_bounds__(NT) k_ric_prep_batch(const RicPanel* __restric
 }
 
 template <int NT, int V, bool LEARNED>
-__global__ void __launch_bounds__(NT) k_ric_items_batch(const RicPanel* __restrict__ P, const int* __restrict__ off,
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_ric_items_batch(const RicPanel* __restrict__ P, const int* __restrict__ off,
                                                         int np, RicList fb) {
   extern __shared__ __align__(16) uint8_t sm[];
   const int item = static_cast<int>(blockIdx.x);
