@@ -83,17 +83,20 @@ FCB_DEV void radix_pass(const K* __restrict__ ks, const uint16_t* __restrict__ i
   __syncwarp();
   const unsigned lt = lanemask_lt();
 
-  // only the within-warp offsets stay in registers (two per word); keys and
-  // column ids are re-read from shared memory for the scatter
+  // the keys and the within-warp offsets (two per word) stay in registers
+  // between the ranking and the scatter; column ids are re-read for the scatter
   uint32_t loc[(MAXIPT + 1) / 2];
+  K kreg[MAXIPT];
 #pragma unroll
   for (int k = 0; k < (MAXIPT + 1) / 2; ++k) loc[k] = 0;
 #pragma unroll
   for (int k = 0; k < MAXIPT; ++k) {
+    kreg[k] = K(0);
     if (k < ipt) {
       const int pos = base + k * 32 + lane;
       const bool v = pos < n;
       const K key = v ? ks[pos] : K(0);
+      kreg[k] = key;
       const uint32_t d = v ? static_cast<uint32_t>((key >> shift) & K(kRadix - 1)) : uint32_t(kRadix);
       const unsigned peers = __match_any_sync(kFull, d);
       const uint32_t r = __popc(peers & lt);
@@ -126,7 +129,7 @@ FCB_DEV void radix_pass(const K* __restrict__ ks, const uint16_t* __restrict__ i
     if (k < ipt) {
       const int pos = base + k * 32 + lane;
       if (pos < n) {
-        const K key = ks[pos];
+        const K key = kreg[k];
         const uint32_t d = static_cast<uint32_t>((key >> shift) & K(kRadix - 1));
         const uint32_t dst = dbase[d] + wh[d] + ((loc[k >> 1] >> ((k & 1) * 16)) & 0xFFFFu);
         kd[dst] = key;

@@ -33,8 +33,6 @@
 // rolling_ic_gpu (src/rolling_ic.cu:306-540) / np_rolling_ic
 // (fc/_cpu_core.py:271-293) for the IC; the reference sorts with CUB's global
 // segmented radix sort instead.
-#include <mutex>
-
 #include "block_sort.cuh"
 #include "fcb_kernels.h"
 #include "learned_sort.cuh"
@@ -212,12 +210,15 @@ FCB_DEV void drop_prefix(uint32_t* dw32, int nwd) {
 // The shared epilogue.  P[c] = cs rank (bits 0-15, 0 = not ranked) | joint
 // factor rank (bits 16-31, 0 = not joint).  Writes the rank row, and the IC
 // unless `bad` (then the section, item_id, is queued on `fb` for the radix
-// kernel).  kmin / kmax: this thread's smallest / largest key of a joint cell
-// (the factor-constant test takes their block extremes).
-template <int NT, int V>
+// kernel).  With
+// KEYS the factor-constant test takes the min / max of the joint cells' keys
+// (key[]); otherwise fkmin / fkmax are the keys at the first and last joint
+// positions of the sorted order, provided by the caller.
+template <int NT, int V, bool KEYS>
 FCB_DEV void ric_epilogue(const RankIcArgs<float, float>& a, const RicPrep& rp, int t, int f, const uint32_t (&P)[4 * V],
-                          uint32_t kmin, uint32_t kmax, uint32_t mj, const unsigned long long* dw, uint32_t* red,
-                          int bad, int* stats, int item_id, RicList fb) {
+                          const uint32_t (&key)[4 * V], uint32_t fkmin, uint32_t fkmax, uint32_t mj,
+                          const unsigned long long* dw, uint32_t* red, int bad, int* stats, int item_id,
+                          RicList fb) {
   constexpr int C = 4 * V;
   const int N = a.N;
   const size_t frow = (static_cast<size_t>(f) * a.T + t) * N;
@@ -234,7 +235,7 @@ FCB_DEV void ric_epilogue(const RankIcArgs<float, float>& a, const RicPrep& rp, 
   uint32_t w[C];
   load_words<NT, V>(rp.word + static_cast<size_t>(t) * rp.ld, N, w);
   unsigned long long sum = 0;
-  uint32_t gmin = 0xFFFFFFFFu, gmax = 0u;
+  uint32_t kmin = 0xFFFFFFFFu, kmax = 0u, gmin = 0xFFFFFFFFu, gmax = 0u;
 #pragma unroll
   for (int c = 0; c < C; ++c) {
     const uint32_t rfj = P[c] >> 16;
@@ -248,6 +249,10 @@ FCB_DEV void ric_epilogue(const RankIcArgs<float, float>& a, const RicPrep& rp, 
       const uint32_t g = (w[c] >> kGidShift) & kPosBits;
       gmin = min(gmin, g);
       gmax = max(gmax, g);
+      if (KEYS) {
+        kmin = min(kmin, key[c]);
+        kmax = max(kmax, key[c]);
+      }
     }
   }
 #pragma unroll
@@ -281,6 +286,10 @@ FCB_DEV void ric_epilogue(const RankIcArgs<float, float>& a, const RicPrep& rp, 
       gmin = min(gmin, red[128 + i]);
       gmax = max(gmax, red[160 + i]);
       b |= static_cast<int>(red[192 + i]);
+    }
+    if (!KEYS) {
+      kmin = fkmin;
+      kmax = fkmax;
     }
     if (b) {
       // the learned order failed its judge: the radix kernel redoes the section
@@ -391,16 +400,12 @@ FCB_DEV void ric_prep_body(const float* __restrict__ R, const uint8_t* __restric
   }
 }
 
-// Dates t0 + blockIdx.x; `reset` clears the fallback list (the first launch of
-// a call).
 template <int NT, int V>
 __global__ void __launch_bounds__(NT) k_ric_prep(const float* __restrict__ R, const uint8_t* __restrict__ rmask,
-                                                 const uint8_t* __restrict__ fmask, int N, RicPrep rp, int t0,
-                                                 int reset) {
+                                                 const uint8_t* __restrict__ fmask, int N, RicPrep rp) {
   extern __shared__ __align__(16) uint8_t sm[];
-  if (reset && blockIdx.x == 0 && threadIdx.x == 0) *rp.fb_count = 0;
-  const int t = t0 + static_cast<int>(blockIdx.x);
-  ric_prep_body<NT, V>(R, rmask, fmask, N, t, rp.word + static_cast<size_t>(t) * rp.ld, sm);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *rp.fb_count = 0;
+  ric_prep_body<NT, V>(R, rmask, fmask, N, blockIdx.x, rp.word + static_cast<size_t>(blockIdx.x) * rp.ld, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -597,82 +602,57 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
     off += __shfl_sync(kFull, inc, 31);
   }
   __syncthreads();  // B4
-  // ---- scatter words [bucket:14 | key:32 | column:14 | joint:1] into their
-  // bucket slots (within a bucket the words order by (key, column))
-  uint32_t vbits = 0u;
+  // ---- scatter (key, column, joint) words into their bucket slots
 #pragma unroll
   for (int c = 0; c < C; ++c) {
     if (P[c] & kCellValid) {
       const uint32_t b = P[c] & kPosBits;
       const uint32_t pos = (cnt[b] & 0xFFFFu) + ((P[c] >> 14) & 0xFFFu);
       const uint32_t i = 4u * ((c >> 2) * NT + tid) + (c & 3);
-      mem[pos] = (static_cast<unsigned long long>(b) << 47) | (static_cast<unsigned long long>(key[c]) << 15) |
-                 (i << 1) | ((P[c] & kCellJoint) ? 1u : 0u);
-      vbits |= 1u << c;
+      mem[pos] = (static_cast<unsigned long long>(key[c]) << 32) | (i << 1) | ((P[c] & kCellJoint) ? 1u : 0u);
     }
   }
   __syncthreads();  // B5
-  // ---- ranks, by bucket position: thread tid takes positions tid, tid + NT,
-  // ... (neighbouring lanes mostly share a bucket, so their loops and loads
-  // agree); rank = bucket start + smaller words in the bucket.  The judge:
-  // the largest word of each bucket must hold a smaller key than every word
-  // of the next non-empty bucket (equal keys always share a bucket).
-  uint32_t res[C], rcol[C];
-  uint32_t kmin = 0xFFFFFFFFu, kmax = 0u;
-  int bad = 0;
+  // ---- ranks: bucket start + smaller words in the bucket
 #pragma unroll
-  for (int k = 0; k < C; ++k) {
-    const int p = tid + k * NT;
-    res[k] = 0u;
-    rcol[k] = 0u;
-    if (p < m) {
-      const unsigned long long w = mem[p];
-      const uint32_t b = static_cast<uint32_t>(w >> 47);
+  for (int c = 0; c < C; ++c) {
+    if (P[c] & kCellValid) {
+      const uint32_t b = P[c] & kPosBits;
+      const bool joint = (P[c] & kCellJoint) != 0u;
+      const uint32_t i = 4u * ((c >> 2) * NT + tid) + (c & 3);
+      const unsigned long long mine =
+          (static_cast<unsigned long long>(key[c]) << 32) | (i << 1) | (joint ? 1u : 0u);
       const uint32_t s = cnt[b], e = cnt[b + 1];
-      const uint32_t sa = s & 0xFFFFu, ea = e & 0xFFFFu;
       uint32_t r = 0, rj = 0;
-      if (ea - sa > 1u)
-        for (uint32_t q = sa; q < ea; ++q) {
-          const unsigned long long o = mem[q];
-          const uint32_t lt = o < w ? 1u : 0u;
-          r += lt;
-          rj += lt & static_cast<uint32_t>(o);
-        }
-      const uint32_t kw = static_cast<uint32_t>(w >> 15);
-      const bool joint = (w & 1ull) != 0ull;
-      res[k] = (sa + r + 1u) | (joint ? (((s >> 16) + rj + 1u) << 16) : 0u);
-      rcol[k] = static_cast<uint32_t>(w >> 1) & 0x3FFFu;
-      if (joint) {
-        kmin = min(kmin, kw);
-        kmax = max(kmax, kw);
+      // a bucket of one is the cell itself
+      if ((e & 0xFFFFu) - (s & 0xFFFFu) > 1u)
+      for (uint32_t p = s & 0xFFFFu; p < (e & 0xFFFFu); ++p) {
+        const unsigned long long o = mem[p];
+        const uint32_t lt = o < mine ? 1u : 0u;
+        r += lt;
+        rj += lt & static_cast<uint32_t>(o);
       }
-      if (r + 1u == ea - sa && ea < static_cast<uint32_t>(m)) {
-        const unsigned long long w2 = mem[ea];
-        const uint32_t e2 = cnt[static_cast<uint32_t>(w2 >> 47) + 1u] & 0xFFFFu;
-        uint32_t nmin = static_cast<uint32_t>(w2 >> 15);
-        for (uint32_t q = ea + 1u; q < e2; ++q) nmin = min(nmin, static_cast<uint32_t>(mem[q] >> 15));
-        bad |= (kw >= nmin) ? 1 : 0;
-      }
+      P[c] = ((s & 0xFFFFu) + r + 1u) | (joint ? (((s >> 16) + rj + 1u) << 16) : 0u);
     }
   }
-  __syncthreads();  // B6: every word has been read
-  uint32_t* RK = reinterpret_cast<uint32_t*>(mem);  // rank | joint rank << 16, by column
+  __syncthreads();  // B6
+  // ---- judge: the keys placed at their ranks must be non-decreasing
+  uint32_t* kS = cnt;
 #pragma unroll
-  for (int k = 0; k < C; ++k)
-    if (tid + k * NT < m) RK[rcol[k]] = res[k];
+  for (int c = 0; c < C; ++c)
+    if (P[c] != 0u) kS[(P[c] & 0xFFFFu) - 1u] = key[c];
   __syncthreads();  // B7
-#pragma unroll
-  for (int c = 0; c < C; ++c) P[c] = ((vbits >> c) & 1u) ? RK[4 * ((c >> 2) * NT + tid) + (c & 3)] : 0u;
-  ric_epilogue<NT, V>(a, rp, t, f, P, kmin, kmax, mj, dw, red, bad, stats, item_id, fb);
+  int bad = 0;
+  for (int p = tid + 1; p < m; p += NT) bad |= (kS[p - 1] > kS[p]) ? 1 : 0;
+  ric_epilogue<NT, V, true>(a, rp, t, f, P, key, 0u, 0u, mj, dw, red, bad, stats, item_id, fb);
 }
 
 // 256-thread CTAs keep to 80 registers so that three fit an SM (the shared
 // memory of N <= 5120 allows three)
 template <int NT, int V>
-__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_ric_learned(RankIcArgs<float, float> a, RicPrep rp,
-                                                                      int item0) {
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_ric_learned(RankIcArgs<float, float> a, RicPrep rp) {
   extern __shared__ __align__(16) uint8_t sm[];
-  const int item = item0 + static_cast<int>(blockIdx.x);
+  const int item = static_cast<int>(blockIdx.x);
   ric_learned_body<NT, V>(a, rp, item / a.F, item % a.F, item, RicList{rp.fb_count, rp.fb_items}, sm);
 }
 
@@ -762,18 +742,17 @@ FCB_DEV void ric_radix_body(const RankIcArgs<float, float>& a, const RicPrep& rp
     uint32_t P[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) P[c] = ((valid >> c) & 1u) ? RK[4 * ((c >> 2) * NT + tid) + (c & 3)] : 0u;
-    ric_epilogue<NT, V>(a, rp, t, f, P, fkmin, fkmax, mj, dw, red, 0, nullptr, 0, RicList{nullptr, nullptr});
+    ric_epilogue<NT, V, false>(a, rp, t, f, P, P, fkmin, fkmax, mj, dw, red, 0, nullptr, 0, RicList{nullptr, nullptr});
   }
 }
 
 // LIST: sections come from the learned kernel's fallback list (persistent
 // CTAs stride over it); otherwise blockIdx.x = t * F + f.
 template <int NT, int V, bool LIST>
-__global__ void __launch_bounds__(NT) k_ric_radix(RankIcArgs<float, float> a, RicPrep rp, int item0) {
+__global__ void __launch_bounds__(NT) k_ric_radix(RankIcArgs<float, float> a, RicPrep rp) {
   extern __shared__ __align__(16) uint8_t sm[];
   if (!LIST) {
-    const int item = item0 + static_cast<int>(blockIdx.x);
-    ric_radix_body<NT, V, true>(a, rp, item / a.F, item % a.F, sm);
+    ric_radix_body<NT, V, true>(a, rp, static_cast<int>(blockIdx.x) / a.F, static_cast<int>(blockIdx.x) % a.F, sm);
     return;
   }
   const int nitems = *static_cast<volatile int*>(rp.fb_count);
@@ -1046,86 +1025,30 @@ __global__ void __launch_bounds__(NT) k_pscan(const float* __restrict__ X, const
 // host side
 // ---------------------------------------------------------------------------
 namespace {
-// A library-private stream per device: the returns pass of the second half of
-// a panel's dates runs there while the first half's rank pass runs on the
-// caller's stream (created on a device's first call; make that call before
-// any stream capture on the device).
-cudaError_t side_stream(cudaStream_t* out) {
-  static std::mutex mu;
-  static cudaStream_t streams[64] = {};
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> g(mu);
-  if (streams[dev] == nullptr) {
-    e = cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
-    if (e != cudaSuccess) return e;
-  }
-  *out = streams[dev];
-  return cudaSuccess;
-}
-
 template <int NT, int V>
 cudaError_t ric_launch(const RankIcArgs<float, float>& a, RicPrep rp, bool learned, cudaStream_t st) {
   const size_t smem_s = SortedLayout<NT>(a.N).total;
   const size_t smem_b = BucketLayout(a.N).total;
   if (smem_s > kMaxSmemPerBlock || smem_b > kMaxSmemPerBlock) return cudaErrorInvalidValue;
-  const long long grid = static_cast<long long>(a.T) * a.F;
-  if (grid > 2147483647LL) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_ric_prep<NT, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem_s));
   if (e != cudaSuccess) return e;
-  if (learned) e = cudaFuncSetAttribute(k_ric_learned<NT, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(smem_b));
-  else e = cudaFuncSetAttribute(k_ric_radix<NT, V, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(smem_s));
-  if (e != cudaSuccess) return e;
-  auto ranks = [&](int t0, int t1) -> cudaError_t {
-    const unsigned g = static_cast<unsigned>((t1 - t0) * a.F);
-    if (learned) k_ric_learned<NT, V><<<g, NT, smem_b, st>>>(a, rp, t0 * a.F);
-    else k_ric_radix<NT, V, false><<<g, NT, smem_s, st>>>(a, rp, t0 * a.F);
-    return cudaGetLastError();
-  };
-  // Long panels: the dates are split in two halves, and the second half's
-  // returns pass runs on a side stream while the first half is ranked (the
-  // returns pass alone fills the GPU for only a few waves).
-  const int Th = a.T >= 64 ? a.T / 2 : a.T;
-  cudaStream_t side = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
-  if (Th < a.T) {
-    if ((e = side_stream(&side)) != cudaSuccess) return e;
-    if ((e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming)) != cudaSuccess) return e;
-    if ((e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming)) != cudaSuccess) {
-      cudaEventDestroy(fork);
-      return e;
-    }
-  }
-  struct Ev {
-    cudaEvent_t a, b;
-    ~Ev() {
-      if (a) cudaEventDestroy(a);
-      if (b) cudaEventDestroy(b);
-    }
-  } ev{fork, join};
-  if (Th < a.T) {
-    // the side stream starts after everything the caller queued before this call
-    if ((e = cudaEventRecord(fork, st)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(side, fork, 0)) != cudaSuccess) return e;
-  }
-  k_ric_prep<NT, V><<<Th, NT, smem_s, st>>>(a.R, a.rmask, a.fmask, a.N, rp, 0, 1);
+  k_ric_prep<NT, V><<<a.T, NT, smem_s, st>>>(a.R, a.rmask, a.fmask, a.N, rp);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if (Th < a.T) {
-    k_ric_prep<NT, V><<<a.T - Th, NT, smem_s, side>>>(a.R, a.rmask, a.fmask, a.N, rp, Th, 0);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = cudaEventRecord(join, side)) != cudaSuccess) return e;
+  const long long grid = static_cast<long long>(a.T) * a.F;
+  if (grid > 2147483647LL) return cudaErrorInvalidValue;
+  if (!learned) {
+    if ((e = cudaFuncSetAttribute(k_ric_radix<NT, V, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem_s))) != cudaSuccess)
+      return e;
+    k_ric_radix<NT, V, false><<<static_cast<unsigned>(grid), NT, smem_s, st>>>(a, rp);
+    return cudaGetLastError();
   }
-  if ((e = ranks(0, Th)) != cudaSuccess) return e;
-  if (Th < a.T) {
-    if ((e = cudaStreamWaitEvent(st, join, 0)) != cudaSuccess) return e;
-    if ((e = ranks(Th, a.T)) != cudaSuccess) return e;
-  }
-  if (!learned) return cudaSuccess;
+  if ((e = cudaFuncSetAttribute(k_ric_learned<NT, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem_b))) != cudaSuccess)
+    return e;
+  k_ric_learned<NT, V><<<static_cast<unsigned>(grid), NT, smem_b, st>>>(a, rp);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   // the radix kernel takes the sections the learned kernel handed back;
   // persistent CTAs (one wave) read the list length on the device and exit at
   // once when it is empty
@@ -1139,7 +1062,7 @@ cudaError_t ric_launch(const RankIcArgs<float, float>& a, RicPrep rp, bool learn
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
   long long fb_grid = static_cast<long long>(occ > 0 ? occ : 1) * (sms > 0 ? sms : 1);
   if (fb_grid > grid) fb_grid = grid;
-  k_ric_radix<NT, V, true><<<static_cast<unsigned>(fb_grid), NT, smem_s, st>>>(a, rp, 0);
+  k_ric_radix<NT, V, true><<<static_cast<unsigned>(fb_grid), NT, smem_s, st>>>(a, rp);
   return cudaGetLastError();
 }
 }  // namespace
