@@ -73,18 +73,29 @@ FCB_DEV void split3(float v0, float v1, uint32_t& h, uint32_t& m, uint32_t& l) {
 
 // Per-factor shift c_f: the mean of the valid cells among 4096 rows spread
 // evenly over the pool (the moment formulas are shift invariant; a shift near
-// the mean keeps the FP32 sums well conditioned).  One block per factor.
-__global__ void k_fct_shift(const float* __restrict__ X, const uint8_t* __restrict__ mask, long long R, long long sr,
-                            long long sf, float* __restrict__ shift) {
+// the mean keeps the FP32 sums well conditioned).  One block per factor; each
+// thread issues its 16 sample loads before it adds them (row q*R/4096 is a
+// shift, not a 64-bit division).
+__global__ void __launch_bounds__(256) k_fct_shift(const float* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                   long long R, long long sr, long long sf, float* __restrict__ shift) {
+  constexpr int kPer = 4096 / 256;
   __shared__ double red[66];
   const int f = blockIdx.x;
+  float v[kPer];
+  bool ok[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const long long q = threadIdx.x + 256LL * u;
+    ok[u] = q < R;
+    const long long r = R >= 4096 ? (q * R) >> 12 : q;
+    v[u] = ok[u] ? X[r * sr + f * sf] : 0.0f;
+    if (ok[u] && mask != nullptr) ok[u] = mask[r] != 0;
+  }
   double s = 0.0, c = 0.0;
-  const long long S = R < 4096 ? R : 4096;
-  for (long long q = threadIdx.x; q < S; q += blockDim.x) {
-    const long long r = q * R / S;
-    const float v = X[r * sr + f * sf];
-    if (finite_f32(v) && (mask == nullptr || mask[r] != 0)) {
-      s += v;
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    if (ok[u] && finite_f32(v[u])) {
+      s += v[u];
       c += 1.0;
     }
   }
@@ -299,19 +310,22 @@ __global__ void __launch_bounds__(kFtThreads, 1)
   if (threadIdx.x == 0 && S.err != 0) atomicExch(status, 1);
 }
 
-// Merge of the CTAs' sums in CTA order and the FP64 finalize, one thread per
-// pair f <= g:  cov = Sxy - Sx Sy / n,  vx = Sx2 - Sx^2 / n,  vy likewise,
-// r = (cov / sqrt(vx)) / sqrt(vy); NaN for n < 2 or a non-positive variance;
+// Merge of the CTAs' sums and the FP64 finalize, one warp per pair f <= g:
+// lane l adds the partials of CTAs l, l + 32, ... in order, then a fixed xor
+// tree adds the lanes (the same order on every call).  Then
+//   cov = Sxy - Sx Sy / n,  vx = Sx2 - Sx^2 / n,  vy likewise,
+//   r = (cov / sqrt(vx)) / sqrt(vy); NaN for n < 2 or a non-positive variance;
 // the diagonal is 1.0 iff the self-correlation is finite; the lower triangle
 // mirrors the upper.
 __global__ void k_fct_final(const double* __restrict__ part, int nblk, int F, double* __restrict__ out) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = static_cast<int>(threadIdx.x & 31);
   if (p >= F * F) return;
   const int f = p / F, g = p % F;
   if (f > g) return;
   const int fg = f * kFtFp + g, gf = g * kFtFp + f;
   double n = 0.0, sx = 0.0, sy = 0.0, sxy = 0.0, sx2 = 0.0, sy2 = 0.0;
-  for (int b = 0; b < nblk; ++b) {
+  for (int b = lane; b < nblk; b += 32) {
     const double* q = part + static_cast<size_t>(b) * 4 * kFtPairs;
     n += q[fg];
     sx += q[kFtPairs + fg];
@@ -320,6 +334,16 @@ __global__ void k_fct_final(const double* __restrict__ part, int nblk, int F, do
     sx2 += q[3 * kFtPairs + fg];
     sy2 += q[3 * kFtPairs + gf];
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n += __shfl_xor_sync(kFull, n, o);
+    sx += __shfl_xor_sync(kFull, sx, o);
+    sy += __shfl_xor_sync(kFull, sy, o);
+    sxy += __shfl_xor_sync(kFull, sxy, o);
+    sx2 += __shfl_xor_sync(kFull, sx2, o);
+    sy2 += __shfl_xor_sync(kFull, sy2, o);
+  }
+  if (lane != 0) return;
   double r = __longlong_as_double(0x7ff8000000000000ll);
   if (n >= 2.0) {
     const double cov = sxy - sx * sy / n;
@@ -365,7 +389,7 @@ cudaError_t launch_factor_corr_bf16x3(const float* X, const uint8_t* mask, long 
     return e;
   k_fct_gram<<<static_cast<unsigned>(grid), kFtThreads, smem, s>>>(X, mask, R, F, sr, sf, shift, part, status);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_fct_final<<<(F * F + 127) / 128, 128, 0, s>>>(part, static_cast<int>(grid), F, out);
+  k_fct_final<<<(F * F + 3) / 4, 128, 0, s>>>(part, static_cast<int>(grid), F, out);
   return cudaGetLastError();
 }
 

@@ -400,8 +400,10 @@ FCB_DEV void ric_prep_body(const float* __restrict__ R, const uint8_t* __restric
   }
 }
 
+// 256-thread sort CTAs keep to 80 registers so that three fit an SM (the
+// shared memory of N <= 5120 allows three)
 template <int NT, int V>
-__global__ void __launch_bounds__(NT) k_ric_prep(const float* __restrict__ R, const uint8_t* __restrict__ rmask,
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_ric_prep(const float* __restrict__ R, const uint8_t* __restrict__ rmask,
                                                  const uint8_t* __restrict__ fmask, int N, RicPrep rp) {
   extern __shared__ __align__(16) uint8_t sm[];
   if (blockIdx.x == 0 && threadIdx.x == 0) *rp.fb_count = 0;
@@ -648,9 +650,10 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
 }
 
 // 256-thread CTAs keep to 80 registers so that three fit an SM (the shared
-// memory of N <= 5120 allows three)
+// memory of N <= 5120 allows three); the 512-thread form of three cells per
+// vector (N <= 6144) keeps to 64 so that two fit
 template <int NT, int V>
-__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_ric_learned(RankIcArgs<float, float> a, RicPrep rp) {
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : (V == 3 ? 2 : 1)) k_ric_learned(RankIcArgs<float, float> a, RicPrep rp) {
   extern __shared__ __align__(16) uint8_t sm[];
   const int item = static_cast<int>(blockIdx.x);
   ric_learned_body<NT, V>(a, rp, item / a.F, item % a.F, item, RicList{rp.fb_count, rp.fb_items}, sm);
@@ -749,7 +752,7 @@ FCB_DEV void ric_radix_body(const RankIcArgs<float, float>& a, const RicPrep& rp
 // LIST: sections come from the learned kernel's fallback list (persistent
 // CTAs stride over it); otherwise blockIdx.x = t * F + f.
 template <int NT, int V, bool LIST>
-__global__ void __launch_bounds__(NT) k_ric_radix(RankIcArgs<float, float> a, RicPrep rp) {
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_ric_radix(RankIcArgs<float, float> a, RicPrep rp) {
   extern __shared__ __align__(16) uint8_t sm[];
   if (!LIST) {
     ric_radix_body<NT, V, true>(a, rp, static_cast<int>(blockIdx.x) / a.F, static_cast<int>(blockIdx.x) % a.F, sm);
@@ -1025,11 +1028,13 @@ __global__ void __launch_bounds__(NT) k_pscan(const float* __restrict__ X, const
 // host side
 // ---------------------------------------------------------------------------
 namespace {
-template <int NT, int V>
+// NT, V: the returns pass and the radix kernel; LT, LV: the learned kernel.
+template <int NT, int V, int LT, int LV>
 cudaError_t ric_launch(const RankIcArgs<float, float>& a, RicPrep rp, bool learned, cudaStream_t st) {
   const size_t smem_s = SortedLayout<NT>(a.N).total;
   const size_t smem_b = BucketLayout(a.N).total;
   if (smem_s > kMaxSmemPerBlock || smem_b > kMaxSmemPerBlock) return cudaErrorInvalidValue;
+  if (a.N > 4 * NT * V || a.N > 4 * LT * LV) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_ric_prep<NT, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem_s));
   if (e != cudaSuccess) return e;
@@ -1044,10 +1049,10 @@ cudaError_t ric_launch(const RankIcArgs<float, float>& a, RicPrep rp, bool learn
     k_ric_radix<NT, V, false><<<static_cast<unsigned>(grid), NT, smem_s, st>>>(a, rp);
     return cudaGetLastError();
   }
-  if ((e = cudaFuncSetAttribute(k_ric_learned<NT, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if ((e = cudaFuncSetAttribute(k_ric_learned<LT, LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem_b))) != cudaSuccess)
     return e;
-  k_ric_learned<NT, V><<<static_cast<unsigned>(grid), NT, smem_b, st>>>(a, rp);
+  k_ric_learned<LT, LV><<<static_cast<unsigned>(grid), LT, smem_b, st>>>(a, rp);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   // the radix kernel takes the sections the learned kernel handed back;
   // persistent CTAs (one wave) read the list length on the device and exit at
@@ -1189,10 +1194,13 @@ bool ric_items_fit(int N) { return N >= 1 && N <= kSmemRankCap; }
 cudaError_t launch_rank_ic_items(const RankIcArgs<float, float>& a, RicPrep rp, bool learned, cudaStream_t st) {
   if (!ric_items_fit(a.N) || a.rank_f_out != nullptr || a.rank_r_out != nullptr) return cudaErrorInvalidValue;
   if (learned && (a.cdf_table == nullptr || a.cdf_zrange == nullptr)) return cudaErrorInvalidValue;
-  if (a.N <= 2048) return ric_launch<256, 2>(a, rp, learned, st);
-  if (a.N <= 5120) return ric_launch<256, 5>(a, rp, learned, st);
-  if (a.N <= 8192) return ric_launch<512, 4>(a, rp, learned, st);
-  return ric_launch<512, 8>(a, rp, learned, st);
+  // the learned kernel runs 512 threads of three cells per vector from 2049 to
+  // 6144 columns (shorter per-thread chains than 256 threads of five)
+  if (a.N <= 2048) return ric_launch<256, 2, 256, 2>(a, rp, learned, st);
+  if (a.N <= 5120) return ric_launch<256, 5, 512, 3>(a, rp, learned, st);
+  if (a.N <= 6144) return ric_launch<512, 4, 512, 3>(a, rp, learned, st);
+  if (a.N <= 8192) return ric_launch<512, 4, 512, 4>(a, rp, learned, st);
+  return ric_launch<512, 8, 512, 8>(a, rp, learned, st);
 }
 
 }  // namespace fcb
