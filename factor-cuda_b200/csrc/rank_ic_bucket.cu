@@ -13,10 +13,12 @@
 //                 one scatter of (key, column) words into bucket slots, and
 //                 each cell's rank is its bucket's start plus the number of
 //                 smaller (key, column) words in its bucket.  The joint-set
-//                 rank comes from the same counters' second half.  A judge
-//                 re-checks the final order; a bucket above the cap, an
-//                 unusable scale or a failed judge hands the section to the
-//                 radix kernel through a device list.
+//                 rank comes from the same counters' second half.  The map
+//                 is monotone in the key whenever the table is
+//                 non-decreasing, which each CTA checks as it stages the
+//                 table; a bucket above the cap, an unusable scale or a
+//                 rejected table hands the section to the radix kernel
+//                 through a device list.
 //  k_ric_radix    the plain path (and the learned path's fallback): the valid
 //                 cells are compacted in column order and radix-sorted in
 //                 shared memory; ranks are sorted positions.
@@ -431,9 +433,18 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
   int* stats = a.learn_stats != nullptr ? a.learn_stats + (static_cast<size_t>(f) * a.T + t) * 4 : nullptr;
   const int nwd = (N + 31) / 32 + 1;
 
-  // ---- stage the table, clear the counters and the drop bitmap
-  for (int k = tid; k < kCdfKnots / 4; k += NT)
-    reinterpret_cast<float4*>(tab)[k] = __ldg(reinterpret_cast<const float4*>(a.cdf_table + static_cast<size_t>(f) * kCdfKnots) + k);
+  // ---- stage the table (checking that it is non-decreasing within [0, 1]: a
+  // NaN fails every comparison), clear the counters and the drop bitmap
+  int tab_bad = 0;
+  {
+    const float* tg = a.cdf_table + static_cast<size_t>(f) * kCdfKnots;
+    for (int k = tid; k < kCdfKnots / 4; k += NT) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(tg) + k);
+      reinterpret_cast<float4*>(tab)[k] = v;
+      const float nx = (4 * k + 4 < kCdfKnots) ? __ldg(tg + 4 * k + 4) : 1.0f;
+      tab_bad |= (0.0f <= v.x && v.x <= v.y && v.y <= v.z && v.z <= v.w && v.w <= nx && nx <= 1.0f) ? 0 : 1;
+    }
+  }
   for (int k = tid; k < (N + 2 + 3) / 4; k += NT) reinterpret_cast<uint4*>(cnt)[k] = make_uint4(0u, 0u, 0u, 0u);
   for (int k = tid; k < nwd; k += NT) reinterpret_cast<unsigned long long*>(dw32)[k] = 0ull;
 
@@ -491,7 +502,7 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
   }
   nval = warp_sum(nval);
   if (lane == 0) red[wi] = static_cast<uint32_t>(nval);
-  __syncthreads();  // B1
+  tab_bad = __syncthreads_or(tab_bad);  // B1
   int m = 0;
   for (int i = 0; i < NW; ++i) m += static_cast<int>(red[i]);
   const float loc = __uint_as_float(red[96]), mad = __uint_as_float(red[97]);
@@ -510,10 +521,10 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
   bm.Bf = static_cast<float>(bm.B);
   const bool scale_ok = (mad > 0.0f) && isfinite(loc) && isfinite(bm.inv_scale) && (bm.inv_scale > 0.0f) &&
                         isfinite(bm.inv_dz) && (bm.inv_dz > 0.0f);
-  if (m >= 2 && !scale_ok) {  // uniform across the block
+  if (m >= 2 && (!scale_ok || tab_bad)) {  // uniform across the block
     if (tid == 0) {
       if (stats != nullptr) {
-        stats[0] = kLearnScale;
+        stats[0] = tab_bad ? kLearnJudge : kLearnScale;
         stats[1] = 0;
         stats[2] = 0;
         stats[3] = m;
@@ -637,16 +648,14 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
       P[c] = ((s & 0xFFFFu) + r + 1u) | (joint ? (((s >> 16) + rj + 1u) << 16) : 0u);
     }
   }
-  __syncthreads();  // B6
-  // ---- judge: the keys placed at their ranks must be non-decreasing
-  uint32_t* kS = cnt;
-#pragma unroll
-  for (int c = 0; c < C; ++c)
-    if (P[c] != 0u) kS[(P[c] & 0xFFFFu) - 1u] = key[c];
-  __syncthreads();  // B7
-  int bad = 0;
-  for (int p = tid + 1; p < m; p += NT) bad |= (kS[p - 1] > kS[p]) ? 1 : 0;
-  ric_epilogue<NT, V, true>(a, rp, t, f, P, key, 0u, 0u, mj, dw, red, bad, stats, item_id, fb);
+  // No order check is needed: the bucket map is non-decreasing in the key
+  // (each step -- the exact key-to-value inverse, the affine standardisation
+  // by a positive scale, the clamped knot position, the two knots' buckets
+  // of a non-decreasing table and the fraction below one between them -- is
+  // monotone under round-to-nearest, and a bucket ends at or below the next
+  // knot's), so every bucket holds smaller keys than the next, and the table
+  // was checked above.
+  ric_epilogue<NT, V, true>(a, rp, t, f, P, key, 0u, 0u, mj, dw, red, 0, stats, item_id, fb);
 }
 
 // 256-thread CTAs keep to 80 registers so that three fit an SM (the shared

@@ -299,7 +299,9 @@ int fcb_cdf_model_load(fcb_cdf_model* m, const float* params, const float* zrang
 int fcb_cdf_grad(const float* params, const float* z, const float* u, int n, float* grad, float* loss);
 /* Learned rank + IC over device panels (as fcb_dev_rank_ic_panel); d_stats
  * (NULL = off) receives (F,T,4) ints: outcome (1 learned, 2 bucket overflow,
- * 3 judge rejected, 4 unusable scale; 2-4 fell back to radix), the largest
+ * 3 order check rejected -- with several factors, a staged CDF table that
+ * is not non-decreasing within [0, 1]; with one factor, the ranked keys out
+ * of order --, 4 unusable scale; 2-4 fell back to radix), the largest
  * bucket, the sum of squared bucket sizes (the per-date comparison work; m
  * for perfectly even buckets of one) and m, the number of ranked cells.
  * Sections too wide for the shared-memory kernel are ranked by the

@@ -169,3 +169,31 @@ def test_model_state_roundtrip(nat):
     st2 = b.state()
     for k in ("params", "zrange", "table"):
         assert np.array_equal(st[k], st2[k])
+
+
+def test_rejected_table_falls_back_to_radix(nat):
+    """A loaded table that is not non-decreasing (one factor's knots reversed
+    over a stretch, another holding a NaN) is rejected by the per-section
+    table check: those sections take the radix path (outcome 3) and every
+    output stays bit-identical; the untouched factor is still learned."""
+    import fcb200
+    F, T, N = 3, 30, 4000
+    X, R, fm, rm = drift_panel(F, T, N, seed=13)
+    dev = torch.device("cuda", 0)
+    dX = torch.from_numpy(X).to(dev)
+    dR, dfm, drm = (torch.from_numpy(a).to(dev) for a in (R, fm, rm))
+    rk0, ic0, _ = _run(nat, dX, dR, dfm, drm, F, T, N)
+    m = fcb200.CdfModel(F, seed=6)
+    m.fit(dX, rk0, T, N, 0, T, steps=300)
+    st = m.state()
+    tab = st["table"].copy()
+    tab[0, 400:420] = tab[0, 400:420][::-1].copy()
+    tab[1, 700] = np.nan
+    st["table"] = tab
+    m.load(st)
+    rk1, ic1, st1 = _run(nat, dX, dR, dfm, drm, F, T, N, model=m)
+    assert bitwise_f32(rk1.cpu().numpy(), rk0.cpu().numpy())
+    a, b = ic1.cpu().numpy(), ic0.cpu().numpy()
+    assert np.array_equal(np.isnan(a), np.isnan(b)) and np.array_equal(a[~np.isnan(a)], b[~np.isnan(b)])
+    assert np.all(st1[0, :, 0] == 3) and np.all(st1[1, :, 0] == 3), st1[:2, :, 0]
+    assert (st1[2, :, 0] == 1).mean() >= 0.9
