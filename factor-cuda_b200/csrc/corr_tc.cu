@@ -10,19 +10,24 @@
 //
 // BF16x3: x' and x'^2 are each split into three bf16 limbs (hi + mid + lo,
 // 24 significant bits -- exact for an f32 value); the mask M is exact in bf16.
-// The B operand of a tile is the stack [M; H; Mm; L; Qh; Qm; Ql] of the j
-// block, so one MMA against a stacked B yields several moment blocks at once.
-// Per 16-deep k step (tcgen05.mma kind::f16, bf16 in, fp32 accumulate in TMEM):
-//   D1 (N=128) += a . [M; H; Mm; L]^T    for a in {H, Mm, L}   -> sx | sum of
-//                 the 9 limb products of sxy in three column blocks
-//   D2 (N=224)  = M . [M; H; Mm; L; Qh; Qm; Ql]^T             -> n | sy (3) | sy2 (3)
-//   D3 (N=32)  += q . M^T                for q in {Qh, Qm, Ql} -> sx2
+// An output tile is 128 stocks i (the A operand) by 64 stocks j (B); the
+// operand stage of each side is the stack [M; H; Mm; L; Qh; Qm; Ql] of its
+// stocks.  Per 16-deep k step (tcgen05.mma kind::f16, bf16 in, fp32
+// accumulate in TMEM), with every limb of a sum accumulated into the same
+// TMEM columns:
+//   D1  (256 cols) += a . [M; H; Mm; L]_j^T   for a in {H, Mm, L}_i
+//                     -> sx | three column blocks whose sum is sxy
+//   Dn|Dsy (128)    = M_i . [M; H]_j^T, then Dsy += M_i . Mm_j^T, M_i . L_j^T
+//   Dsy2 (64)      += M_i . q_j^T            for q in {Qh, Qm, Ql}
+//   Dsx2 (64)      += q_i . M_j^T            for q in {Qh, Qm, Ql}
+// 512 TMEM columns in all.  Each stage's operands (84 KB) serve 8192 outputs.
 // Operands are staged by TMA (cp.async.bulk.tensor, no cluster multicast) in
 // the canonical K-major 64-byte-swizzle layout: each stock row holds the stage's
 // 32 dates as one 64-byte line, 8-row groups 512 bytes apart, and the seven
-// matrices of an operand follow one another, so the stacked B operand is just
-// 224 consecutive rows.  One 3D box per operand fills a stage with full 64-byte
-// row reads (a 16-byte-wide box would fetch a 32-byte sector per 16 bytes used).
+// matrices of an operand follow one another, so a sub-stack of the B operand
+// is a run of consecutive rows.  One 3D box per operand fills a stage with full
+// 64-byte row reads (a 16-byte-wide box would fetch a 32-byte sector per 16
+// bytes used).
 // The FP64 finalize is
 //   cov = sxy - sx sy / n, vx = sx2 - sx^2/n, vy = sy2 - sy^2/n,
 //   r = (cov/sqrt(vx))/sqrt(vy),  NaN for n < 2 or a non-positive variance.
@@ -37,10 +42,10 @@
 
 namespace fcb {
 
-constexpr int kTcM = 128;      // output rows per tile (stocks i)
-constexpr int kTcN = 32;       // output columns per tile (stocks j)
-constexpr int kTcK = 32;       // k depth per pipeline stage
-constexpr int kTcStages = 3;
+constexpr int kTcM = kPrecTileTcM;  // output rows per tile (stocks i)
+constexpr int kTcN = kPrecTileTcN;  // output columns per tile (stocks j)
+constexpr int kTcK = 32;            // k depth per pipeline stage
+constexpr int kTcStages = 2;
 constexpr int kTcMats = 7;     // operand matrices, order M H Mm L Qh Qm Ql
 constexpr int kRowBytes = kTcK * 2;                   // one stock's dates of a stage (64 B)
 constexpr int kAMat = kTcM * kRowBytes;               // one A matrix of a stage
@@ -48,8 +53,10 @@ constexpr int kBMat = kTcN * kRowBytes;               // one B matrix of a stage
 constexpr int kABytesStage = kTcMats * kAMat;
 constexpr int kBBytesStage = kTcMats * kBMat;
 constexpr int kStageBytes = kABytesStage + kBBytesStage;
-constexpr int kD1 = 0, kD2 = 128, kD3 = 352;          // TMEM column of each accumulator
-constexpr int kTmemCols = 512;                        // 384 used, rounded to a power of two
+// TMEM columns of the accumulators (64 columns = one tile width each)
+constexpr int kD1 = 0, kDn = 4 * kTcN, kDsy = 5 * kTcN, kDsy2 = 6 * kTcN, kDsx2 = 7 * kTcN;
+constexpr int kTmemCols = 8 * kTcN;
+static_assert(kTmemCols == 512, "the accumulators fill the TMEM of one CTA");
 
 // ---------------------------------------------------------------------------
 // prep: (T,N) f32 + mask -> K-major (Np, Tp) operands
@@ -183,18 +190,6 @@ struct TcMaps {
   CUtensorMap b;  // box {32, 32, 7}
 };
 
-// sum of `nb` 16-column TMEM blocks spaced 32 columns apart, in f64
-FCB_DEV void tmem_sum_blocks(uint32_t taddr, int nb, double* acc) {
-#pragma unroll
-  for (int u = 0; u < 16; ++u) acc[u] = 0.0;
-  for (int b = 0; b < nb; ++b) {
-    float v[16];
-    tmem_ld16(taddr + b * kTcN, v);
-#pragma unroll
-    for (int u = 0; u < 16; ++u) acc[u] += static_cast<double>(v[u]);
-  }
-}
-
 __global__ void __launch_bounds__(192, 1)
     k_corr_bf16x3(const __grid_constant__ TcMaps maps, const int2* __restrict__ tiles, int N, int Tp,
                   double* __restrict__ out, int* __restrict__ status) {
@@ -245,9 +240,9 @@ __global__ void __launch_bounds__(192, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t id128 = idesc_bf16(kTcM, 4 * kTcN);
-      constexpr uint32_t id224 = idesc_bf16(kTcM, 7 * kTcN);
-      constexpr uint32_t id32 = idesc_bf16(kTcM, kTcN);
+      constexpr uint32_t id256 = idesc_bf16(kTcM, 4 * kTcN);
+      constexpr uint32_t id128 = idesc_bf16(kTcM, 2 * kTcN);
+      constexpr uint32_t id64 = idesc_bf16(kTcM, kTcN);
       for (int kt = 0; kt < nkt; ++kt) {
         const int s = kt % kTcStages, round = kt / kTcStages;
         if (!mbar_wait(&full[s], round & 1)) {
@@ -259,19 +254,26 @@ __global__ void __launch_bounds__(192, 1)
         const uint32_t bbase = abase + kABytesStage;
 #pragma unroll
         for (int ks = 0; ks < kTcK / 16; ++ks) {
-          const uint32_t ak = abase + ks * 32;
-          const uint64_t bstack = smem_desc_sw64(bbase + ks * 32);  // [M; H; Mm; L; Qh; Qm; Ql] rows
+          const uint32_t ak = abase + ks * 32, bk = bbase + ks * 32;
+          auto A = [&](int m) { return smem_desc_sw64(ak + m * kAMat); };  // rows of matrix m, stocks i
+          auto B = [&](int m) { return smem_desc_sw64(bk + m * kBMat); };  // from matrix m on, stocks j
           const uint32_t first = (kt == 0 && ks == 0) ? 0u : 1u;
           // D1: x limbs against [M; H; Mm; L]
-          mma_bf16(tmem + kD1, smem_desc_sw64(ak + 1 * kAMat), bstack, id128, first);
-          mma_bf16(tmem + kD1, smem_desc_sw64(ak + 2 * kAMat), bstack, id128, 1u);
-          mma_bf16(tmem + kD1, smem_desc_sw64(ak + 3 * kAMat), bstack, id128, 1u);
-          // D2: mask against the whole stack
-          mma_bf16(tmem + kD2, smem_desc_sw64(ak + 0 * kAMat), bstack, id224, first);
-          // D3: x'^2 limbs against M
-          mma_bf16(tmem + kD3, smem_desc_sw64(ak + 4 * kAMat), bstack, id32, first);
-          mma_bf16(tmem + kD3, smem_desc_sw64(ak + 5 * kAMat), bstack, id32, 1u);
-          mma_bf16(tmem + kD3, smem_desc_sw64(ak + 6 * kAMat), bstack, id32, 1u);
+          mma_bf16(tmem + kD1, A(1), B(0), id256, first);
+          mma_bf16(tmem + kD1, A(2), B(0), id256, 1u);
+          mma_bf16(tmem + kD1, A(3), B(0), id256, 1u);
+          // n | sy: the mask against [M; H], then the other two y limbs into sy
+          mma_bf16(tmem + kDn, A(0), B(0), id128, first);
+          mma_bf16(tmem + kDsy, A(0), B(2), id64, 1u);
+          mma_bf16(tmem + kDsy, A(0), B(3), id64, 1u);
+          // sy2: the mask against the y'^2 limbs
+          mma_bf16(tmem + kDsy2, A(0), B(4), id64, first);
+          mma_bf16(tmem + kDsy2, A(0), B(5), id64, 1u);
+          mma_bf16(tmem + kDsy2, A(0), B(6), id64, 1u);
+          // sx2: the x'^2 limbs against the mask
+          mma_bf16(tmem + kDsx2, A(4), B(0), id64, first);
+          mma_bf16(tmem + kDsx2, A(5), B(0), id64, 1u);
+          mma_bf16(tmem + kDsx2, A(6), B(0), id64, 1u);
         }
         mma_commit(&empty[s]);  // frees the stage when these MMAs complete
       }
@@ -285,16 +287,23 @@ __global__ void __launch_bounds__(192, 1)
     tc_fence_after();
     if (!ok) atomicExch(err, 1);
     const int i = i0 + row;
-    const uint32_t lrow = static_cast<uint32_t>(quad * 32) << 16;
+    const uint32_t t0 = tmem + (static_cast<uint32_t>(quad * 32) << 16);
     for (int c0 = 0; c0 < kTcN; c0 += 16) {
-      float sx[16], n[16], sx2[16];
-      double sxy[16], sy[16], sy2[16];
-      tmem_ld16(tmem + lrow + kD1 + c0, sx);
-      tmem_sum_blocks(tmem + lrow + kD1 + kTcN + c0, 3, sxy);
-      tmem_ld16(tmem + lrow + kD2 + c0, n);
-      tmem_sum_blocks(tmem + lrow + kD2 + kTcN + c0, 3, sy);
-      tmem_sum_blocks(tmem + lrow + kD2 + 4 * kTcN + c0, 3, sy2);
-      tmem_ld16(tmem + lrow + kD3 + c0, sx2);
+      float sx[16], n[16], sy[16], sy2[16], sx2[16], v[16];
+      double sxy[16];
+      tmem_ld16(t0 + kD1 + c0, sx);
+#pragma unroll
+      for (int u = 0; u < 16; ++u) sxy[u] = 0.0;
+#pragma unroll
+      for (int b = 1; b <= 3; ++b) {
+        tmem_ld16(t0 + kD1 + b * kTcN + c0, v);
+#pragma unroll
+        for (int u = 0; u < 16; ++u) sxy[u] += static_cast<double>(v[u]);
+      }
+      tmem_ld16(t0 + kDn + c0, n);
+      tmem_ld16(t0 + kDsy + c0, sy);
+      tmem_ld16(t0 + kDsy2 + c0, sy2);
+      tmem_ld16(t0 + kDsx2 + c0, sx2);
       if (ok && *err == 0 && i < N) {
 #pragma unroll
         for (int u = 0; u < 16; ++u) {
@@ -387,17 +396,18 @@ __global__ void __launch_bounds__(256) k_corr_fp32(const float* __restrict__ X, 
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-// Tile lists on the device (no host vector, no upload).  BF16x3: 128 x 32
-// tiles (ti, tj) that reach the upper triangle, tj >= 4 ti, row-major; row ti
-// starts at ti*ntj - 2 ti (ti-1).  FP32: 64 x 64 tiles tj >= ti; row ti starts
+// Tile lists on the device (no host vector, no upload).  BF16x3: 128 x 64
+// tiles (ti, tj) that reach the upper triangle, tj >= 2 ti, row-major; row ti
+// starts at ti*ntj - ti (ti-1).  FP32: 64 x 64 tiles tj >= ti; row ti starts
 // at ti*n - ti (ti-1) / 2.  One thread per tile row.
 __global__ void k_prec_tiles(int mode, int N, int2* __restrict__ tiles) {
   const int ti = blockIdx.x * blockDim.x + threadIdx.x;
   if (mode == 0) {
     const int nti = (N + kTcM - 1) / kTcM, ntj = (N + kTcN - 1) / kTcN;
     if (ti >= nti) return;
-    const long long off = static_cast<long long>(ti) * ntj - 2LL * ti * (ti - 1);
-    for (int tj = 4 * ti; tj < ntj; ++tj) tiles[off + (tj - 4 * ti)] = make_int2(ti, tj);
+    static_assert(kTcM == 2 * kTcN, "tile row ti starts at column tile 2 ti");
+    const long long off = static_cast<long long>(ti) * ntj - static_cast<long long>(ti) * (ti - 1);
+    for (int tj = 2 * ti; tj < ntj; ++tj) tiles[off + (tj - 2 * ti)] = make_int2(ti, tj);
   } else {
     const int n = (N + kPrecTileFp32 - 1) / kPrecTileFp32;
     if (ti >= n) return;
@@ -409,7 +419,7 @@ __global__ void k_prec_tiles(int mode, int N, int2* __restrict__ tiles) {
 int prec_tile_count(int mode, int N) {
   if (mode == 0) {
     const long long nti = (N + kTcM - 1) / kTcM, ntj = (N + kTcN - 1) / kTcN;
-    return static_cast<int>(nti * ntj - 2 * nti * (nti - 1));
+    return static_cast<int>(nti * ntj - nti * (nti - 1));
   }
   const long long n = (N + kPrecTileFp32 - 1) / kPrecTileFp32;
   return static_cast<int>(n * (n + 1) / 2);

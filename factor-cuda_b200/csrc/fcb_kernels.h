@@ -109,7 +109,7 @@ struct PrecOperands {
 };
 
 // corr_tc.cu
-constexpr int kPrecTileTcM = 128, kPrecTileTcN = 32, kPrecTileFp32 = 64;
+constexpr int kPrecTileTcM = 128, kPrecTileTcN = 64, kPrecTileFp32 = 64;
 size_t prec_tc_smem();
 // Tile list of a precision form (mode 0 BF16x3, 1 FP32) built on the device;
 // prec_tile_count gives its length.
