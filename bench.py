@@ -586,22 +586,46 @@ def make_batch_panels(dev, n=64, F=8, seed=20261205):
 
 
 def bench_batch(dev, steps=5, warmup=2, tune_cache=None, cpu_sample=True):
-    """Batched uneven panels: one autotuned CUDA-graph replay of the
-    persistent rank+IC kernels + per-panel factor_corr, against the same work
-    issued one panel at a time.  Device-resident inputs (8.8 GB of factors,
-    far above L2)."""
+    """Batched uneven panels: one autotuned CUDA-graph replay of the batched
+    rank+IC kernels + per-panel factor_corr, against the same work issued one
+    panel at a time.  Device-resident inputs (8.8 GB of factors, far above
+    L2).  Rank + IC use learned splitters: one CdfModel for the 8 factors,
+    fitted once (timed, outside the replays) on the exact radix ranks of
+    panel 0's first 250 dates and shared by every panel (the model works on
+    per-date standardised values, so it does not depend on a panel's T or N);
+    the same batch without the model is timed as the radix replay."""
     import torch
     import fcb200
+    from fcb200 import _native as nat
     panels = make_batch_panels(dev)
     cells = sum(int(p["X"].numel()) for p in panels)
     torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    # the radix batch first (its replay is the comparison), then the model
+    # fitted on panel 0's exact ranks
+    b_rx = fcb200.Batch(panels, min_valid=MIN_VALID)
+    p0 = panels[0]
+    F0, T0, N0 = (int(v) for v in p0["X"].shape)
+    nat.check(nat.lib().fcb_dev_rank_ic_panel(p0["X"].data_ptr(), p0["R"].data_ptr(), p0["fmask"].data_ptr(),
+                                              p0["rmask"].data_ptr(), F0, T0, N0, MIN_VALID,
+                                              p0["ranks"].data_ptr(), p0["ic"].data_ptr(), 0, stream.cuda_stream),
+              "fcb_dev_rank_ic_panel")
+    model = fcb200.CdfModel(F0, seed=20261205)
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    model.fit(p0["X"], p0["ranks"], T0, N0, 0, min(T0, 250), steps=1500, lr=3e-3, stream=stream.cuda_stream)
+    f1.record(stream)
+    torch.cuda.synchronize(dev)
+    fit_ms = f0.elapsed_time(f1)
+    for p in panels:
+        p["model"] = model
     b = fcb200.Batch(panels, min_valid=MIN_VALID)
     t0 = time.perf_counter()
     # with a cache file, a second run takes the tuned configuration without
     # measuring alternatives (so a profiler sees only the timed launches)
     cfg, tuned_ms, cached = b.autotune(reps=2, cache_path=tune_cache)
     tune_s = time.perf_counter() - t0
-    stream = torch.cuda.current_stream(dev)
 
     def timed(fn):
         for _ in range(warmup):
@@ -616,6 +640,10 @@ def bench_batch(dev, steps=5, warmup=2, tune_cache=None, cpu_sample=True):
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1) / steps
 
+    b_rx.config = cfg
+    ms_graph_rx = timed(b_rx.run)
+    b_rx.status()
+    b_rx.close()
     ms_graph = timed(b.run)
     b.status()
     ic_g = [p["ic"].clone() for p in panels]
@@ -637,15 +665,20 @@ def bench_batch(dev, steps=5, warmup=2, tune_cache=None, cpu_sample=True):
     res = {"workload": "64 uneven panels (N ~ U[300,6000], T ~ U[250,2500], F=8, gaps ~ U[0,0.2]): "
                        "cs_rank + rolling_ic(30) + factor_corr per panel",
            "cells": cells, "unit": "Gelem/s",
-           # kernels: per kernel variant, the returns pass and the rank pass over all its
-           # panels; per panel, factor_corr's column pass + merge, Gram + finalize and the
-           # four fallback kernels (launched for every pool of 4096 rows or more; they exit at
-           # once when no pair is flagged); the per-panel arm runs the returns kernel and the
-           # per-(date, factor) kernel of each panel (F >= 2)
+           # kernels: per kernel variant, the returns pass, the rank pass over all its
+           # panels and the pass over the sections the learned buckets handed back; for all
+           # panels together, factor_corr's column pass + merge, Gram pass + finalize and the
+           # four fallback kernels (every pool here has 4096 rows or more; they exit at once
+           # when no pair is flagged); the per-panel arm runs, for each panel, those three
+           # rank kernels and the eight factor_corr kernels
+           "method": "learned splitters, one CdfModel (F=8) fitted on panel 0 and shared by every panel",
+           "fit_ms": fit_ms,
            "graph": {"ms": ms_graph, "value": cells / (ms_graph / 1e3) / 1e9,
-                     "kernels_per_replay": 2 * len(variants) + 8 * len(panels)},
+                     "kernels_per_replay": 3 * len(variants) + 8},
+           "graph_radix": {"ms": ms_graph_rx, "value": cells / (ms_graph_rx / 1e3) / 1e9},
+           "learned_speedup_vs_radix_graph": ms_graph_rx / ms_graph,
            "per_panel": {"ms": ms_pp, "value": cells / (ms_pp / 1e3) / 1e9,
-                         "kernels_per_step": sum((2 if p["X"].shape[0] >= 2 else 1) + 8 for p in panels)},
+                         "kernels_per_step": sum((3 if p["X"].shape[0] >= 2 else 1) + 8 for p in panels)},
            "speedup_graph_vs_per_panel": ms_pp / ms_graph,
            "bit_exact_graph_vs_per_panel": bool(same),
            "autotune": {"config": cfg, "tuned_ms": tuned_ms, "tuning_s": tune_s, "from_cache": cached}}
@@ -707,23 +740,25 @@ def make_c5_block(dev, g, rng, state, F, Tb, N, start):
     return X.contiguous(), R.float().contiguous(), listed.to(torch.uint8), torch.isfinite(R).to(torch.uint8)
 
 
-def bench_c5(dev, T=5000, N=8000, F=128, Tb=250, seed=20261206, cpu_sample=True):
+def bench_c5(dev, T=5000, N=8000, F=128, Tb=250, seed=20261206, cpu_sample=True, head=1, fit_steps=300,
+             refit_every=4, overlap_fit=False):
     """Learned splitters on the streaming configuration (T=5000, N=8000,
     F=128: 5.12 G cells, 20.5 GB of f32 factors, device-resident in blocks of
     250 dates), two end-to-end runs timed by CUDA events around the whole
     block loop:
       radix    every block ranked by the plain radix path;
-      learned  blocks 0 and 1 ranked by radix and the networks fitted on their
-               exact ranks (1500 + 300 Adam steps, in line: nothing else is
-               ready to run); every later block ranked by the learned path;
-               after block b the training samples are drawn from its (exact)
-               ranks on the ranking stream and a 100-step refit runs on a
-               second stream into the idle table slot while block b + 1 is
-               ranked; block b + 2 waits for the refit on the device and
-               ranks with the new table, and the next refit starts after it
-               (one refit per two blocks, each overlapped with ranking).
-    The learned figures include the fitting.  An untimed pass then compares
-    the learned output of every block with the radix output bit for bit."""
+      learned  the first `head` blocks are ranked by radix; the training
+               samples are drawn from block 0's exact ranks and the networks
+               are fitted (`fit_steps` Adam steps) on a second stream while
+               blocks 1 .. head-1 are ranked (overlap_fit; otherwise in line
+               on the ranking stream); block `head` waits for that fit on the
+               device, and every later block is ranked by the learned path.  After every `refit_every`-th learned block b, samples
+               of its (exact) ranks feed a 100-step refit on the second stream
+               into the idle table slot while block b + 1 is ranked; block
+               b + 2 waits for it on the device and ranks with the new table.
+    Every fit is inside the learned figure.  An untimed pass then compares
+    the learned output of every learned block with the radix output bit for
+    bit."""
     import torch
     import fcb200
     from fcb200 import _native as nat
@@ -762,27 +797,34 @@ def bench_c5(dev, T=5000, N=8000, F=128, Tb=250, seed=20261206, cpu_sample=True)
         bev[b + 1].record(stream)
     torch.cuda.synchronize(dev)
     t_radix = bev[0].elapsed_time(bev[nb])
-    t_radix_lb = bev[2].elapsed_time(bev[nb])
-    # ---- learned run, fitting included
+    t_radix_lb = bev[head].elapsed_time(bev[nb])
+    # ---- learned run, every fit included
     model = fcb200.CdfModel(F, seed=seed)
     fit_done = torch.cuda.Event()
     swap_at = -1
     refits = swaps = 0
     ev[0].record(stream)
     for b, (X, R, fm, rm) in enumerate(blocks):
-        if b < 2:
+        if b < head:
             radix(X, R, fm, rm, ranks)
-            model.fit(X, ranks, Tb, N, 0, Tb, steps=1500 if b == 0 else 300, lr=3e-3 if b == 0 else 1e-3, stream=s)
-            if b == 1:
+            if b == 0:
+                model.sample(X, ranks, Tb, N, 0, Tb, stream=s)
+                fit_stream = side if overlap_fit else stream
+                fit_stream.wait_stream(stream)
+                model.train(fit_steps, 3e-3, into_idle=False, stream=fit_stream.cuda_stream)
+                fit_done.record(fit_stream)
+            if b == head - 1:
                 ev[1].record(stream)
             continue
+        if b == head:
+            stream.wait_event(fit_done)  # on the device: the first fit has landed
         if b == swap_at:
             stream.wait_event(fit_done)  # on the device: the refit has landed
             model.swap()
             swaps += 1
             swap_at = -1
         learned(model, b, X, R, fm, rm, ranks)
-        if swap_at < 0 and b + 2 < nb:
+        if swap_at < 0 and (b - head) % refit_every == refit_every - 1 and b + 2 < nb:
             model.sample(X, ranks, Tb, N, 0, Tb, stream=s)
             side.wait_stream(stream)
             model.train(100, 1e-3, into_idle=True, stream=side.cuda_stream)
@@ -795,11 +837,11 @@ def bench_c5(dev, T=5000, N=8000, F=128, Tb=250, seed=20261206, cpu_sample=True)
     t_learn_all = ev[0].elapsed_time(ev[2])
     t_learn_lb = ev[1].elapsed_time(ev[2])
     t_fit0 = ev[0].elapsed_time(ev[1])
-    codes = stats[2:, ..., 0].flatten().cpu().numpy()
+    codes = stats[head:, ..., 0].flatten().cpu().numpy()
     # ---- untimed exactness pass: learned (final model) vs radix, every block
     exact = True
     for b, (X, R, fm, rm) in enumerate(blocks):
-        if b < 2:
+        if b < head:
             continue
         radix(X, R, fm, rm, ranks)
         ic_r = ic.clone()
@@ -807,10 +849,13 @@ def bench_c5(dev, T=5000, N=8000, F=128, Tb=250, seed=20261206, cpu_sample=True)
         exact = exact and bool(torch.equal(ranks.view(torch.int32), ranks2.view(torch.int32))) and \
             bool(torch.equal(torch.nan_to_num(ic_r, nan=7.0), torch.nan_to_num(ic, nan=7.0)))
     torch.cuda.synchronize(dev)
-    lb_cells = F * (T - 2 * Tb) * N
+    lb_cells = F * (T - head * Tb) * N
     res = {"workload": f"learned splitters, streaming: T={T}, N={N}, F={F} ({F * T * N / 1e9:.2f} G cells, "
-                       f"{F * T * N * 4 / 1e9:.1f} GB f32), blocks of {Tb} dates; fit on dates [0, {2 * Tb}), "
-                       f"a 100-step refit after every other block, overlapped with the next block",
+                       f"{F * T * N * 4 / 1e9:.1f} GB f32), blocks of {Tb} dates; a {fit_steps}-step fit on "
+                       f"block 0's exact ranks " + (f"overlapped with radix blocks 1-{head - 1}" if overlap_fit
+                                                    else "in line") +
+                       f", learned from block {head}; a 100-step refit after every {refit_every}th learned "
+                       f"block, overlapped with the next block",
            "radix_gelem_s": F * T * N / (t_radix / 1e3) / 1e9,
            "learned_incl_fit_gelem_s": F * T * N / (t_learn_all / 1e3) / 1e9,
            "learned_blocks_gelem_s": lb_cells / (t_learn_lb / 1e3) / 1e9,

@@ -15,10 +15,12 @@
 // kernel per group (k_rank_ic_batch) runs as many CTAs as fit, each taking
 // items from its queue until it is empty -- so a short panel does not leave
 // SMs idle while a long one finishes, and there is one launch per group
-// instead of one per panel.  factor_corr of each panel (its factor planes
+// instead of one per panel.  factor_corr of every panel (its factor planes
 // pooled over the panel's (t, i) rows, the factor mask broadcast per column)
-// follows on three graph branches.  The whole sequence is captured once into a
-// CUDA graph and replayed by fcb_batch_run.
+// runs as one batched launch per kernel kind (column pass, merge, Gram pass,
+// finalize, the fallback passes: launch_factor_corr_batch) on a graph branch
+// alongside rank + IC.  The whole sequence is captured once into a CUDA graph
+// and replayed by fcb_batch_run.
 //
 // Outputs do not depend on the scheduling knobs: ranks and IC are exact
 // integer/ordinal results, and factor_corr's row blocking is fixed by each
@@ -89,6 +91,13 @@ struct fcb_batch {
   RicBatchVariant var[kRicVariants] = {};
   std::vector<FcWork> fcw;
   std::vector<void*> fc_mem;
+  // factor_corr of every panel with an output, batched: panel descriptors,
+  // the prefix offsets of each kind of grid, and the grid sizes
+  FcBatchPanel* d_fcb = nullptr;
+  int* d_fcb_off = nullptr;
+  int fcb_np = 0;
+  int fcb_total[kFcbGrids] = {};
+  size_t fcb_gram_smem = 0;
   // current schedule
   int cls_off[kClasses] = {}, cls_cnt[kClasses] = {}, cls_maxN[kClasses] = {}, cls_grid[kClasses] = {};
   size_t cls_smem[kClasses] = {};
@@ -119,6 +128,11 @@ struct fcb_batch {
     ric_cap = 0;
     for (void* m : fc_mem) cudaFree(m);
     fc_mem.clear();
+    cudaFree(d_fcb);
+    cudaFree(d_fcb_off);
+    d_fcb = nullptr;
+    d_fcb_off = nullptr;
+    fcb_np = 0;
     for (int k = 0; k < kClasses; ++k) {
       if (s[k] != nullptr) cudaStreamDestroy(s[k]);
       if (ev_join[k] != nullptr) cudaEventDestroy(ev_join[k]);
@@ -364,20 +378,12 @@ int enqueue(fcb_batch& b, cudaStream_t s0) {
                                                     b.cls_cnt[k], b.d_ctr + k, b.cls_grid[k], b.cls_smem[k],
                                                     b.d_status, st, nullptr));
   }
-  // join, then factor_corr of every panel spread over three branches
-  for (int k = 1; k < kClasses; ++k) {
-    FCB_BTRY(cudaEventRecord(b.ev_join[k], b.s[k]));
-    FCB_BTRY(cudaStreamWaitEvent(s0, b.ev_join[k], 0));
-  }
-  FCB_BTRY(cudaEventRecord(b.ev_fork, s0));
-  for (int k = 1; k < kClasses; ++k) FCB_BTRY(cudaStreamWaitEvent(b.s[k], b.ev_fork, 0));
-  for (size_t i = 0; i < b.p.size(); ++i) {
-    const fcb_panel& q = b.p[i];
-    if (q.corr_out == nullptr) continue;
-    cudaStream_t st = (i % kClasses == 0) ? s0 : b.s[i % kClasses];
-    const long long R = static_cast<long long>(q.T) * q.N;
-    FCB_BTRY(launch_factor_corr_strided(q.X, b.dtx, q.fmask, R, q.F, 1, R, b.fcw[i], q.corr_out, nullptr, st));
-  }
+  // factor_corr of every panel: one batched launch per kernel kind, on the
+  // last branch, alongside the rank + IC kernels (it reads only the factor
+  // planes and masks)
+  if (b.fcb_np > 0)
+    FCB_BTRY(launch_factor_corr_batch(b.d_fcb, b.fcb_np, b.d_fcb_off, b.fcb_total, b.dtx == FCB_DTYPE_F32 ? 0 : 1,
+                                      b.fcb_gram_smem, b.s[kClasses - 1]));
   for (int k = 1; k < kClasses; ++k) {
     FCB_BTRY(cudaEventRecord(b.ev_join[k], b.s[k]));
     FCB_BTRY(cudaStreamWaitEvent(s0, b.ev_join[k], 0));
@@ -559,6 +565,35 @@ extern "C" int fcb_batch_create(const fcb_panel* panels, int npanels, int dtype_
     w.fb_count = reinterpret_cast<int*>(c8);
     c8 += 256;
     w.fb_part = reinterpret_cast<double*>(c8);
+  }
+  {
+    // batched factor_corr: descriptors and per-kind prefix offsets
+    std::vector<FcBatchPanel> q;
+    for (int i = 0; i < npanels; ++i) {
+      const fcb_panel& p = panels[i];
+      if (p.corr_out == nullptr) continue;
+      q.push_back(fc_batch_panel(p.X, p.fmask, static_cast<long long>(p.T) * p.N, p.F, b->fcw[i], p.corr_out));
+    }
+    const int np = static_cast<int>(q.size());
+    if (np > 0) {
+      std::vector<int> off(static_cast<size_t>(kFcbGrids) * (np + 1), 0);
+      for (int k = 0; k < np; ++k) {
+        int blocks[kFcbGrids];
+        fc_batch_grids(q[k], blocks);
+        for (int g = 0; g < kFcbGrids; ++g)
+          off[static_cast<size_t>(g) * (np + 1) + k + 1] = off[static_cast<size_t>(g) * (np + 1) + k] + blocks[g];
+        b->fcb_gram_smem = std::max(b->fcb_gram_smem,
+                                    fc_gram_smem(q[k].Fp, q[k].tasks_per_block, dtype_x == FCB_DTYPE_F32 ? 4 : 8));
+      }
+      for (int g = 0; g < kFcbGrids; ++g) b->fcb_total[g] = off[static_cast<size_t>(g) * (np + 1) + np];
+      e = cudaMalloc(&b->d_fcb, q.size() * sizeof(FcBatchPanel));
+      if (e == cudaSuccess) e = cudaMalloc(&b->d_fcb_off, off.size() * sizeof(int));
+      if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_fcb, q.data(), q.size() * sizeof(FcBatchPanel), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = cudaMemcpy(b->d_fcb_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return fail(rcode(e));
+      b->fcb_np = np;
+    }
   }
   if (dtype_x == FCB_DTYPE_F32) {
     // prepared returns of every panel (ric_prep_bytes each, 256-byte aligned),

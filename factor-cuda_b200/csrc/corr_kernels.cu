@@ -505,13 +505,24 @@ cudaError_t launch_corr_domain(const void* X, int dtype, const uint8_t* mask, lo
 // layout), (1, T*N) for F stacked (T,N) factor planes.
 // ---------------------------------------------------------------------------
 
+// Block coordinates of a factor_corr body: the CUDA block of a single-panel
+// launch, or a panel's own block inside a batched launch (see the batched
+// kernels below).
+struct Blk {
+  int x, y, gx;
+};
+FCB_DEV Blk launch_blk() {
+  return Blk{static_cast<int>(blockIdx.x), static_cast<int>(blockIdx.y), static_cast<int>(gridDim.x)};
+}
+
 // Per-block column partials over a contiguous row range: count, Kahan sum,
 // min, max.  Rows are visited in increasing order within each thread's
 // strided slice; partials are merged in a fixed order by k_fc_colfinal.
 template <typename TIN, bool UNIT_ROWS>
-__global__ void k_fc_colpart(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
-                             long long sr, long long sf, long long rows_per_block, FcColPart* __restrict__ part) {
-  const long long r0 = blockIdx.x * rows_per_block;
+FCB_DEV void fc_colpart_body(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
+                             long long sr, long long sf, long long rows_per_block, FcColPart* __restrict__ part,
+                             const Blk bk) {
+  const long long r0 = bk.x * rows_per_block;
   const long long r1 = min(R, r0 + rows_per_block);
   for (int f = threadIdx.y; f < F; f += blockDim.y) {
     Kahan k;
@@ -567,15 +578,22 @@ __global__ void k_fc_colpart(const TIN* __restrict__ X, const uint8_t* __restric
       p.c = k.c;
       p.min = mn;
       p.max = mx;
-      part[static_cast<size_t>(blockIdx.x) * F + f] = p;
+      part[static_cast<size_t>(bk.x) * F + f] = p;
     }
   }
 }
 
+template <typename TIN, bool UNIT_ROWS>
+__global__ void k_fc_colpart(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
+                             long long sr, long long sf, long long rows_per_block, FcColPart* __restrict__ part) {
+  fc_colpart_body<TIN, UNIT_ROWS>(X, mask, R, F, sr, sf, rows_per_block, part, launch_blk());
+}
+
 // One warp per column: lane l merges partials l, l+32, ... in order, then a
 // fixed shuffle tree merges the lanes.
-__global__ void k_fc_colfinal(const FcColPart* __restrict__ part, int nblk, int F, FcColStat* __restrict__ st) {
-  const int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+FCB_DEV void fc_colfinal_body(const FcColPart* __restrict__ part, int nblk, int F, FcColStat* __restrict__ st,
+                              const Blk bk) {
+  const int f = (bk.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (f >= F) return;  // whole warps exit together
   Kahan k;
@@ -611,6 +629,10 @@ __global__ void k_fc_colfinal(const FcColPart* __restrict__ part, int nblk, int 
   s.min = mn;
   s.max = mx;
   st[f] = s;
+}
+
+__global__ void k_fc_colfinal(const FcColPart* __restrict__ part, int nblk, int F, FcColStat* __restrict__ st) {
+  fc_colfinal_body(part, nblk, F, st, launch_blk());
 }
 
 // Gram partials over a row range.  Products p: 0 n=(m,m), 1 sx=(x',m),
@@ -680,11 +702,11 @@ FCB_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memo
 FCB_DEV void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 template <typename TIN>
-__global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+FCB_DEV void fc_gram_body(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
                                                  long long R, int F, long long sr, long long sf, int Fp,
                                                  long long rows_per_block,
                                                  const FcColStat* __restrict__ st, int tasks_total,
-                                                 int tasks_per_block, double* __restrict__ part) {
+                                                 int tasks_per_block, double* __restrict__ part, const Blk bk) {
   extern __shared__ __align__(16) double fsm[];
   const int chunk = fc_rows_chunk(Fp);
   const int pitch = fc_stage_pitch(Fp);
@@ -692,7 +714,7 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
   double* sm = sx + fc_stage_sm_offset(Fp);          // [Fp][pitch] validity
   double* red = fsm;  // [slices][tasks_per_block][16], over the staging tile once it is idle
   const int tb = Fp / 4;
-  const int task0 = blockIdx.y * tasks_per_block;
+  const int task0 = bk.y * tasks_per_block;
   const int ntask = min(tasks_per_block, tasks_total - task0);
   const int slices = 256 / tasks_per_block;
   const int my_task = threadIdx.x % tasks_per_block;
@@ -703,7 +725,7 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
   double acc[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-  const long long r0 = blockIdx.x * rows_per_block;
+  const long long r0 = bk.x * rows_per_block;
   const long long r1 = min(R, r0 + rows_per_block);
   // Row chunks are pipelined: while chunk k is centred and multiplied, the raw
   // elements of chunk k + 1 are in flight into the other raw buffer
@@ -821,17 +843,26 @@ __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, c
     int pp = 0, f0 = 0, g0 = 0;
     fc_gram_task(task0 + tk, tb, pp, f0, g0);
     const int f = f0 + q / 4, g = g0 + q % 4;
-    part[((static_cast<size_t>(blockIdx.x) * 4 + pp) * Fp + f) * Fp + g] = s;
+    part[((static_cast<size_t>(bk.x) * 4 + pp) * Fp + f) * Fp + g] = s;
   }
+}
+
+template <typename TIN>
+__global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                 long long R, int F, long long sr, long long sf, int Fp,
+                                                 long long rows_per_block,
+                                                 const FcColStat* __restrict__ st, int tasks_total,
+                                                 int tasks_per_block, double* __restrict__ part) {
+  fc_gram_body<TIN>(X, mask, R, F, sr, sf, Fp, rows_per_block, st, tasks_total, tasks_per_block, part, launch_blk());
 }
 
 // Sum the per-block Gram partials in block order, finalize each pair.
 // One warp per (i <= j) pair: lane l sums blocks l, l+32, ..., a fixed
 // shuffle tree sums the lanes, lane 0 finalizes.
-__global__ void k_fc_final(const double* __restrict__ part, int nblk, int F, int Fp,
+FCB_DEV void fc_final_body(const double* __restrict__ part, int nblk, int F, int Fp,
                            const FcColStat* __restrict__ st, double* __restrict__ out, int* __restrict__ fb_list,
-                           int* __restrict__ fb_count, uint8_t* __restrict__ flags) {
-  const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+                           int* __restrict__ fb_count, uint8_t* __restrict__ flags, const Blk bk) {
+  const int e = (bk.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (e >= F * F) return;  // whole warps exit together
   const int i = e / F, j = e % F;
@@ -873,16 +904,22 @@ __global__ void k_fc_final(const double* __restrict__ part, int nblk, int F, int
   }
 }
 
+__global__ void k_fc_final(const double* __restrict__ part, int nblk, int F, int Fp,
+                           const FcColStat* __restrict__ st, double* __restrict__ out, int* __restrict__ fb_list,
+                           int* __restrict__ fb_count, uint8_t* __restrict__ flags) {
+  fc_final_body(part, nblk, F, Fp, st, out, fb_list, fb_count, flags, launch_blk());
+}
+
 // One block per flagged pair: two-pass over the pooled joint rows.  Small
 // pools run serially in row order (bit-compatible with the serial-Kahan
 // reference); large pools use per-thread Kahan partials merged in a fixed
 // tree (the reference's kahan_reduce kernels, src/factor_corr.cu:188-322).
 template <typename TIN>
-__global__ void k_fc_fallback(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
+FCB_DEV void fc_fallback_body(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
                               long long sr, long long sf, const int* __restrict__ fb_list,
-                              const int* __restrict__ fb_count, double* __restrict__ out) {
-  if (static_cast<int>(blockIdx.x) >= *fb_count) return;
-  const int e = fb_list[blockIdx.x];
+                              const int* __restrict__ fb_count, double* __restrict__ out, const Blk bk) {
+  if (static_cast<int>(bk.x) >= *fb_count) return;
+  const int e = fb_list[bk.x];
   const int i = e / F, j = e % F;
   __shared__ double sh[6][256];
   __shared__ double res[8];
@@ -1001,6 +1038,13 @@ __global__ void k_fc_fallback(const TIN* __restrict__ X, const uint8_t* __restri
   }
 }
 
+template <typename TIN>
+__global__ void k_fc_fallback(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
+                              long long sr, long long sf, const int* __restrict__ fb_list,
+                              const int* __restrict__ fb_count, double* __restrict__ out) {
+  fc_fallback_body<TIN>(X, mask, R, F, sr, sf, fb_list, fb_count, out, launch_blk());
+}
+
 // Multi-block fallback for large pools: the rows are split into `nblk` fixed
 // ranges (blockIdx.y); each block forms per-range Kahan partials (threads stride the range,
 // a fixed binary tree merges them), a per-pair kernel merges the ranges in
@@ -1032,17 +1076,17 @@ FCB_DEV void fb_tree_kahan(double (*sh)[kFbThreads], int q0, int nq) {
 }
 
 template <typename TIN>
-__global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass1(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+FCB_DEV void fc_fb_pass1_body(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
                                                             long long R, int F, long long sr, long long sf, int nblk,
                                                             const int* __restrict__ fb_list,
                                                             const int* __restrict__ fb_count,
-                                                            double* __restrict__ part) {
+                                                            double* __restrict__ part, const Blk bk) {
   __shared__ double sh[5][kFbThreads];
   __shared__ double mm[4][kFbThreads / 32];
   const long long rpb = (R + nblk - 1) / nblk;
-  const long long r0 = blockIdx.y * rpb, r1 = min(R, r0 + rpb);
+  const long long r0 = bk.y * rpb, r1 = min(R, r0 + rpb);
   const int tid = threadIdx.x;
-  for (int slot = blockIdx.x; slot < *fb_count; slot += gridDim.x) {
+  for (int slot = bk.x; slot < *fb_count; slot += bk.gx) {
     const int e = fb_list[slot];
     const int i = e / F, j = e % F;
     Kahan kx, ky;
@@ -1115,7 +1159,7 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass1(const TIN* __restric
         mny = fmin(mny, mm[2][w]);
         mxy = fmax(mxy, mm[3][w]);
       }
-      double* P = part + (static_cast<size_t>(slot) * nblk + blockIdx.y) * kFbP1;
+      double* P = part + (static_cast<size_t>(slot) * nblk + bk.y) * kFbP1;
       P[0] = sh[4][0];
       P[1] = sh[0][0];
       P[2] = sh[1][0];
@@ -1130,15 +1174,25 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass1(const TIN* __restric
   }
 }
 
+template <typename TIN>
+__global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass1(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                            long long R, int F, long long sr, long long sf, int nblk,
+                                                            const int* __restrict__ fb_list,
+                                                            const int* __restrict__ fb_count,
+                                                            double* __restrict__ part) {
+  fc_fb_pass1_body<TIN>(X, mask, R, F, sr, sf, nblk, fb_list, fb_count, part, launch_blk());
+}
+
 // Per flagged pair: merge the pass-1 ranges in order -> (n, mean x, mean y,
 // degenerate flag) in pair[slot*4 ..]; a degenerate pair is finished here.
 // One warp per flagged pair: the lanes load up to 32 range partials at once and
 // every lane merges them in range order from shuffled copies (the same
 // sequence of operations as a single thread walking the ranges), so the
 // merged values do not depend on the warp; lane 0 writes.
-__global__ void k_fc_fb_mid(int F, int nblk, const int* __restrict__ fb_list, const int* __restrict__ fb_count,
-                            const double* __restrict__ part, double* __restrict__ pair, double* __restrict__ out) {
-  const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+FCB_DEV void fc_fb_mid_body(int F, int nblk, const int* __restrict__ fb_list, const int* __restrict__ fb_count,
+                            const double* __restrict__ part, double* __restrict__ pair, double* __restrict__ out,
+                            const Blk bk) {
+  const int slot = (bk.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (slot >= *fb_count) return;  // whole warps exit together
   Kahan kx, ky;
@@ -1183,18 +1237,23 @@ __global__ void k_fc_fb_mid(int F, int nblk, const int* __restrict__ fb_list, co
   }
 }
 
+__global__ void k_fc_fb_mid(int F, int nblk, const int* __restrict__ fb_list, const int* __restrict__ fb_count,
+                            const double* __restrict__ part, double* __restrict__ pair, double* __restrict__ out) {
+  fc_fb_mid_body(F, nblk, fb_list, fb_count, part, pair, out, launch_blk());
+}
+
 template <typename TIN>
-__global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass2(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+FCB_DEV void fc_fb_pass2_body(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
                                                             long long R, int F, long long sr, long long sf, int nblk,
                                                             const int* __restrict__ fb_list,
                                                             const int* __restrict__ fb_count,
                                                             const double* __restrict__ pair,
-                                                            double* __restrict__ part) {
+                                                            double* __restrict__ part, const Blk bk) {
   __shared__ double sh[6][kFbThreads];
   const long long rpb = (R + nblk - 1) / nblk;
-  const long long r0 = blockIdx.y * rpb, r1 = min(R, r0 + rpb);
+  const long long r0 = bk.y * rpb, r1 = min(R, r0 + rpb);
   const int tid = threadIdx.x;
-  for (int slot = blockIdx.x; slot < *fb_count; slot += gridDim.x) {
+  for (int slot = bk.x; slot < *fb_count; slot += bk.gx) {
     const double* Q = pair + static_cast<size_t>(slot) * 4;
     if (Q[3] != 0.0) continue;  // degenerate: finished by k_fc_fb_mid (uniform per block)
     const int e = fb_list[slot];
@@ -1231,16 +1290,26 @@ __global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass2(const TIN* __restric
     sh[5][tid] = c.c;
     __syncthreads();
     fb_tree_kahan(sh, 0, 3);
-    if (tid < kFbP2) part[(static_cast<size_t>(slot) * nblk + blockIdx.y) * kFbP2 + tid] = sh[tid][0];
+    if (tid < kFbP2) part[(static_cast<size_t>(slot) * nblk + bk.y) * kFbP2 + tid] = sh[tid][0];
     __syncthreads();
   }
 }
 
+template <typename TIN>
+__global__ void __launch_bounds__(kFbThreads) k_fc_fb_pass2(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                            long long R, int F, long long sr, long long sf, int nblk,
+                                                            const int* __restrict__ fb_list,
+                                                            const int* __restrict__ fb_count,
+                                                            const double* __restrict__ pair,
+                                                            double* __restrict__ part) {
+  fc_fb_pass2_body<TIN>(X, mask, R, F, sr, sf, nblk, fb_list, fb_count, pair, part, launch_blk());
+}
+
 // Pass-2 partials merged per flagged pair, one warp per pair as in k_fc_fb_mid.
-__global__ void k_fc_fb_final(int F, int nblk, const int* __restrict__ fb_list, const int* __restrict__ fb_count,
+FCB_DEV void fc_fb_final_body(int F, int nblk, const int* __restrict__ fb_list, const int* __restrict__ fb_count,
                               const double* __restrict__ pair, const double* __restrict__ part,
-                              double* __restrict__ out) {
-  const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+                              double* __restrict__ out, const Blk bk) {
+  const int slot = (bk.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (slot >= *fb_count) return;  // whole warps exit together
   if (pair[static_cast<size_t>(slot) * 4 + 3] != 0.0) return;
@@ -1274,6 +1343,12 @@ __global__ void k_fc_fb_final(int F, int nblk, const int* __restrict__ fb_list, 
   const double r = safe_pearson(c.s - c.c, a.s - a.c, b.s - b.c);
   out[i * F + j] = r;
   out[j * F + i] = r;
+}
+
+__global__ void k_fc_fb_final(int F, int nblk, const int* __restrict__ fb_list, const int* __restrict__ fb_count,
+                              const double* __restrict__ pair, const double* __restrict__ part,
+                              double* __restrict__ out) {
+  fc_fb_final_body(F, nblk, fb_list, fb_count, pair, part, out, launch_blk());
 }
 
 size_t fc_fb_part_doubles(long long R, int F) {
@@ -1381,6 +1456,196 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
 cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
                                double* out, uint8_t* flags, cudaStream_t s) {
   return launch_factor_corr_strided(X, dtype, mask, R, F, F, 1, w, out, flags, s);
+}
+
+// ---------------------------------------------------------------------------
+// batched factor_corr: many factor-plane panels per launch.  Each batched
+// kernel's grid is the concatenation of the panels' own grids (prefix offsets
+// per kernel kind); a block finds its panel by binary search and runs the
+// single-panel body with its block coordinates inside that panel's grid, so
+// every panel is computed exactly as by launch_factor_corr_strided.
+// ---------------------------------------------------------------------------
+namespace {
+
+FCB_DEV int fcb_panel_of(const int* __restrict__ off, int np, int b) {
+  int lo = 0, hi = np - 1;  // largest p with off[p] <= b
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct FcbAt {
+  const FcBatchPanel* q;
+  int local;
+};
+FCB_DEV FcbAt fcb_at(const FcBatchPanel* __restrict__ P, const int* __restrict__ off, int np) {
+  const int b = static_cast<int>(blockIdx.x);
+  const int p = fcb_panel_of(off, np, b);
+  return FcbAt{P + p, b - off[p]};
+}
+
+template <typename TIN>
+__global__ void k_fcb_colpart(const FcBatchPanel* __restrict__ P, const int* __restrict__ off, int np) {
+  const FcbAt a = fcb_at(P, off, np);
+  const FcBatchPanel& q = *a.q;
+  fc_colpart_body<TIN, true>(static_cast<const TIN*>(q.X), q.mask, q.R, q.F, 1, q.R, q.rpb_cols, q.w.colpart,
+                             Blk{a.local, 0, q.w.nblk_cols});
+}
+
+__global__ void k_fcb_colfinal(const FcBatchPanel* __restrict__ P, const int* __restrict__ off, int np) {
+  const FcbAt a = fcb_at(P, off, np);
+  const FcBatchPanel& q = *a.q;
+  if (a.local == 0 && threadIdx.x == 0) *q.w.fb_count = 0;  // read by the finalize after the Gram pass
+  fc_colfinal_body(q.w.colpart, q.w.nblk_cols, q.F, q.w.colstat, Blk{a.local, 0, 0});
+}
+
+template <typename TIN>
+__global__ void __launch_bounds__(256, 3) k_fcb_gram(const FcBatchPanel* __restrict__ P, const int* __restrict__ off,
+                                                  int np) {
+  const FcbAt a = fcb_at(P, off, np);
+  const FcBatchPanel& q = *a.q;
+  fc_gram_body<TIN>(static_cast<const TIN*>(q.X), q.mask, q.R, q.F, 1, q.R, q.Fp, q.rpb_gram, q.w.colstat,
+                    q.tasks_total, q.tasks_per_block, q.w.gram,
+                    Blk{a.local % q.w.nblk_gram, a.local / q.w.nblk_gram, q.w.nblk_gram});
+}
+
+__global__ void k_fcb_final(const FcBatchPanel* __restrict__ P, const int* __restrict__ off, int np) {
+  const FcbAt a = fcb_at(P, off, np);
+  const FcBatchPanel& q = *a.q;
+  fc_final_body(q.w.gram, q.w.nblk_gram, q.F, q.Fp, q.w.colstat, q.out, q.w.fb_list, q.w.fb_count, nullptr,
+                Blk{a.local, 0, 0});
+}
+
+template <typename TIN>
+__global__ void k_fcb_fallback(const FcBatchPanel* __restrict__ P, const int* __restrict__ off, int np) {
+  const FcbAt a = fcb_at(P, off, np);
+  const FcBatchPanel& q = *a.q;
+  fc_fallback_body<TIN>(static_cast<const TIN*>(q.X), q.mask, q.R, q.F, 1, q.R, q.w.fb_list, q.w.fb_count, q.out,
+                        Blk{a.local, 0, 0});
+}
+
+FCB_DEV double* fcb_pair(const FcBatchPanel& q) {
+  return q.w.fb_part + static_cast<size_t>(q.maxpairs) * q.fb_nblk * kFbP1;
+}
+
+template <typename TIN>
+__global__ void __launch_bounds__(kFbThreads) k_fcb_fb_pass1(const FcBatchPanel* __restrict__ P,
+                                                             const int* __restrict__ off, int np) {
+  const FcbAt a = fcb_at(P, off, np);
+  const FcBatchPanel& q = *a.q;
+  fc_fb_pass1_body<TIN>(static_cast<const TIN*>(q.X), q.mask, q.R, q.F, 1, q.R, q.fb_nblk, q.w.fb_list,
+                        q.w.fb_count, q.w.fb_part, Blk{a.local % q.fb_ysl, a.local / q.fb_ysl, q.fb_ysl});
+}
+
+__global__ void k_fcb_fb_mid(const FcBatchPanel* __restrict__ P, const int* __restrict__ off, int np) {
+  const FcbAt a = fcb_at(P, off, np);
+  const FcBatchPanel& q = *a.q;
+  fc_fb_mid_body(q.F, q.fb_nblk, q.w.fb_list, q.w.fb_count, q.w.fb_part, fcb_pair(q), q.out, Blk{a.local, 0, 0});
+}
+
+template <typename TIN>
+__global__ void __launch_bounds__(kFbThreads) k_fcb_fb_pass2(const FcBatchPanel* __restrict__ P,
+                                                             const int* __restrict__ off, int np) {
+  const FcbAt a = fcb_at(P, off, np);
+  const FcBatchPanel& q = *a.q;
+  fc_fb_pass2_body<TIN>(static_cast<const TIN*>(q.X), q.mask, q.R, q.F, 1, q.R, q.fb_nblk, q.w.fb_list,
+                        q.w.fb_count, fcb_pair(q), q.w.fb_part, Blk{a.local % q.fb_ysl, a.local / q.fb_ysl, q.fb_ysl});
+}
+
+__global__ void k_fcb_fb_final(const FcBatchPanel* __restrict__ P, const int* __restrict__ off, int np) {
+  const FcbAt a = fcb_at(P, off, np);
+  const FcBatchPanel& q = *a.q;
+  fc_fb_final_body(q.F, q.fb_nblk, q.w.fb_list, q.w.fb_count, fcb_pair(q), q.w.fb_part, q.out, Blk{a.local, 0, 0});
+}
+
+}  // namespace
+
+FcBatchPanel fc_batch_panel(const void* X, const uint8_t* mask, long long R, int F, const FcWork& w, double* out) {
+  FcBatchPanel q{};
+  q.X = X;
+  q.mask = mask;
+  q.R = R;
+  q.F = F;
+  q.Fp = (F + 3) / 4 * 4;
+  q.w = w;
+  q.out = out;
+  const int tb = q.Fp / 4;
+  q.tasks_total = fc_gram_tasks(tb);
+  q.tasks_per_block = q.tasks_total <= 256 ? q.tasks_total : 256;
+  q.ytiles = (q.tasks_total + q.tasks_per_block - 1) / q.tasks_per_block;
+  q.rpb_cols = (R + w.nblk_cols - 1) / w.nblk_cols;
+  q.rpb_gram = (R + w.nblk_gram - 1) / w.nblk_gram;
+  q.maxpairs = F * (F - 1) / 2 > 0 ? F * (F - 1) / 2 : 1;
+  q.fb_nblk = fc_fb_nblk(R, F);
+  // the same choice of fallback as launch_factor_corr_strided
+  q.large = (w.fb_part != nullptr && R >= 4096 && q.fb_nblk > 1) ? 1 : 0;
+  q.fb_ysl = std::max(1, std::min(q.maxpairs, 2048 / q.fb_nblk));
+  return q;
+}
+
+void fc_batch_grids(const FcBatchPanel& q, int (&blocks)[kFcbGrids]) {
+  blocks[kFcbCols] = q.w.nblk_cols;
+  blocks[kFcbColFinal] = (q.F * 32 + 127) / 128;
+  blocks[kFcbGram] = q.w.nblk_gram * q.ytiles;
+  blocks[kFcbFinal] = (q.F * q.F * 32 + 255) / 256;
+  blocks[kFcbFbPass] = q.large ? q.fb_ysl * q.fb_nblk : 0;
+  blocks[kFcbFbPair] = q.large ? (q.maxpairs * 32 + 127) / 128 : 0;
+  blocks[kFcbSmall] = q.large ? 0 : q.maxpairs;
+}
+
+cudaError_t launch_factor_corr_batch(const FcBatchPanel* d_panels, int np, const int* d_off, const int* total,
+                                     int dtype, size_t gram_smem, cudaStream_t s) {
+  auto off = [&](int g) { return d_off + static_cast<size_t>(g) * (np + 1); };
+  cudaError_t e = cudaSuccess;
+  auto chk = [&]() { return (e = cudaGetLastError()); };
+  const bool f32 = dtype == 0;
+  if (total[kFcbCols] > 0) {
+    if (f32) k_fcb_colpart<float><<<total[kFcbCols], dim3(32, 8), 0, s>>>(d_panels, off(kFcbCols), np);
+    else k_fcb_colpart<double><<<total[kFcbCols], dim3(32, 8), 0, s>>>(d_panels, off(kFcbCols), np);
+    if (chk() != cudaSuccess) return e;
+  }
+  if (total[kFcbColFinal] > 0) {
+    k_fcb_colfinal<<<total[kFcbColFinal], 128, 0, s>>>(d_panels, off(kFcbColFinal), np);
+    if (chk() != cudaSuccess) return e;
+  }
+  if (total[kFcbGram] > 0) {
+    if (f32) {
+      if ((e = cudaFuncSetAttribute(k_fcb_gram<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(gram_smem))) != cudaSuccess)
+        return e;
+      k_fcb_gram<float><<<total[kFcbGram], 256, gram_smem, s>>>(d_panels, off(kFcbGram), np);
+    } else {
+      if ((e = cudaFuncSetAttribute(k_fcb_gram<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(gram_smem))) != cudaSuccess)
+        return e;
+      k_fcb_gram<double><<<total[kFcbGram], 256, gram_smem, s>>>(d_panels, off(kFcbGram), np);
+    }
+    if (chk() != cudaSuccess) return e;
+  }
+  if (total[kFcbFinal] > 0) {
+    k_fcb_final<<<total[kFcbFinal], 256, 0, s>>>(d_panels, off(kFcbFinal), np);
+    if (chk() != cudaSuccess) return e;
+  }
+  if (total[kFcbSmall] > 0) {
+    if (f32) k_fcb_fallback<float><<<total[kFcbSmall], 256, 0, s>>>(d_panels, off(kFcbSmall), np);
+    else k_fcb_fallback<double><<<total[kFcbSmall], 256, 0, s>>>(d_panels, off(kFcbSmall), np);
+    if (chk() != cudaSuccess) return e;
+  }
+  if (total[kFcbFbPass] > 0) {
+    if (f32) k_fcb_fb_pass1<float><<<total[kFcbFbPass], kFbThreads, 0, s>>>(d_panels, off(kFcbFbPass), np);
+    else k_fcb_fb_pass1<double><<<total[kFcbFbPass], kFbThreads, 0, s>>>(d_panels, off(kFcbFbPass), np);
+    if (chk() != cudaSuccess) return e;
+    k_fcb_fb_mid<<<total[kFcbFbPair], 128, 0, s>>>(d_panels, off(kFcbFbPair), np);
+    if (chk() != cudaSuccess) return e;
+    if (f32) k_fcb_fb_pass2<float><<<total[kFcbFbPass], kFbThreads, 0, s>>>(d_panels, off(kFcbFbPass), np);
+    else k_fcb_fb_pass2<double><<<total[kFcbFbPass], kFbThreads, 0, s>>>(d_panels, off(kFcbFbPass), np);
+    if (chk() != cudaSuccess) return e;
+    k_fcb_fb_final<<<total[kFcbFbPair], 128, 0, s>>>(d_panels, off(kFcbFbPair), np);
+    if (chk() != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace fcb

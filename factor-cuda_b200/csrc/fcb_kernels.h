@@ -77,6 +77,31 @@ constexpr int kFcFbMaxNblk = 64;
 constexpr int kFcFbPartDoubles = 9;
 int fc_fb_nblk(long long R, int F);
 size_t fc_fb_part_doubles(long long R, int F);
+// One factor-plane panel (rows at unit stride, F planes of R rows) of a
+// batched factor_corr launch, with its single-panel launch geometry.
+struct FcBatchPanel {
+  const void* X;
+  const uint8_t* mask;
+  long long R;
+  int F, Fp;
+  long long rpb_cols, rpb_gram;   // rows per column / Gram block
+  int tasks_total, tasks_per_block, ytiles;
+  int maxpairs, fb_nblk, fb_ysl;  // flagged-pair slots, fallback row blocks, pair slots per row block
+  int large;                      // 1: multi-block fallback, 0: one block per flagged pair
+  FcWork w;
+  double* out;
+};
+// Kinds of batched grid (prefix offsets are kept per kind).
+constexpr int kFcbCols = 0, kFcbColFinal = 1, kFcbGram = 2, kFcbFinal = 3, kFcbFbPass = 4, kFcbFbPair = 5,
+              kFcbSmall = 6, kFcbGrids = 7;
+FcBatchPanel fc_batch_panel(const void* X, const uint8_t* mask, long long R, int F, const FcWork& w, double* out);
+// Blocks the panel contributes to each kind of batched grid.
+void fc_batch_grids(const FcBatchPanel& q, int (&blocks)[kFcbGrids]);
+// Up to nine launches for every panel: d_off holds kFcbGrids runs of np + 1
+// prefix offsets, total the grid sizes (host), gram_smem the largest Gram
+// staging of the panels; results equal launch_factor_corr_strided's per panel.
+cudaError_t launch_factor_corr_batch(const FcBatchPanel* d_panels, int np, const int* d_off, const int* total,
+                                     int dtype, size_t gram_smem, cudaStream_t s);
 
 // rank_kernels.cu
 cudaError_t launch_cs_rank(const float* X, const uint8_t* mask, int T, int N, int desc, float* out,

@@ -9,8 +9,8 @@ The reference's Python adapter ``fc/`` loads its two native modules,
 outside this repository, an unmodified copy of the reference's ``fc/``,
 ``tests/`` and ``benchmark_corpus/`` (the suite's fixtures and frozen
 anchors) plus its ``pytest.ini``, puts this build's three shared libraries in
-``build/`` -- the drop-in integration INTEGRATION.md describes -- and runs the
-suite there with pytest.  It prints the pytest summary and, with --out, writes
+``build/`` -- the whole drop-in integration -- and runs the suite there with
+pytest.  It prints the pytest summary and, with --out, writes
 the pass / skip / fail counts and the failing test ids as JSON.  Nothing of
 the reference is written into this repository.
 """

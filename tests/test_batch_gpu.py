@@ -53,7 +53,7 @@ def to_panels(torch, host, with_ranks=True):
 
 def snapshot(panels):
     return [(p["ranks"].cpu().numpy().copy() if p["ranks"] is not None else None, p["ic"].cpu().numpy().copy(),
-             p["corr"].cpu().numpy().copy()) for p in panels]
+             p["corr"].cpu().numpy().copy() if p["corr"] is not None else None) for p in panels]
 
 
 def same_f64(a, b):
@@ -203,3 +203,35 @@ def test_batch_learned_panels_bit_exact(env):
     got = snapshot(panels)
     for k in range(len(panels)):
         assert bitwise_f32(got[k][0], ref[k][0]) and same_f64(got[k][1], ref[k][1])
+
+
+def test_batched_factor_corr_small_and_large_pools_with_fallback(env):
+    """factor_corr of the whole batch runs as one launch per kernel kind.
+    Mixed pools -- below 4096 rows (one block per flagged pair), above (the
+    row-split fallback), a panel without a corr output -- and a column with a
+    large bias that the cancellation gate sends to the fallback: every panel
+    equals the single-panel entry point bit for bit and the oracle to 1e-12,
+    f32 and f64."""
+    torch, nat = env
+    import fcb200
+    for dt, seed in ((np.float32, 17), (np.float64, 19)):
+        rng = np.random.default_rng(seed)
+        specs = [(10, 300, 3, 0.1), (40, 2000, 4, 0.0), (12, 200, 5, 0.0), (30, 3000, 3, 0.2), (25, 150, 2, 0.0)]
+        host = []
+        for T, N, F, g in specs:
+            X, R, fm, rm = make_host(rng, T, N, F, g, dt)
+            X[F - 1] += dt(1e9)  # large bias: the pair's uncentred sums cancel -> fallback
+            host.append((X, R, fm, rm))
+        panels = to_panels(torch, host)
+        panels[2]["corr"] = None
+        b = fcb200.Batch(panels)
+        b.run()
+        b.status()
+        got = snapshot(panels)
+        for k, (X, R, fm, rm) in enumerate(host):
+            if k == 2:
+                continue
+            _, _, corr = single_panel(env, X, R, fm, rm)
+            assert same_f64(got[k][2], corr), (dt, k)
+            assert corr_match(got[k][2], O.factor_corr(np.moveaxis(X, 0, -1), fm.astype(bool))), (dt, k)
+        b.close()
