@@ -187,6 +187,37 @@ def test_rank_ic_panel_matches_per_factor_ops():
         assert _ic_equal(ic[f], O.rolling_ic(X[f], R, fm, rm, 30))
 
 
+def test_rank_ic_panel_returns_pass_edge_dates():
+    """The per-date returns pass ranks by sampled splitters and falls back to
+    the radix sort inside the same CTA.  Dates that take each branch: ordinary
+    heavy-tailed returns; returns with three distinct values (buckets far
+    above the cap); constant returns (no usable sample range); a single valid
+    return; a date where every sampled column is invalid but others are
+    valid; ±0 and a value spread of 1e30.  Ranks and IC bitwise vs the
+    oracle, N on both sides of the 2048 / 5120 kernel widths."""
+    import fcb200
+    rng = np.random.default_rng(23)
+    for N in (300, 2500, 5000, 7000):
+        F, T = 2, 8
+        X = rng.standard_normal((F, T, N)).astype(np.float32)
+        R = rng.standard_t(3, (T, N)).astype(np.float32)
+        R[1] = rng.integers(0, 3, N).astype(np.float32)
+        R[2] = 0.25
+        R[3] = np.nan
+        R[3, N // 3] = 1.0
+        S = min(N, 256)
+        sampled = (np.arange(S) * N) // 256 if N >= 256 else np.arange(S)
+        R[4, sampled] = np.nan
+        R[5, ::2] = -0.0
+        R[5, 1::2] = 0.0
+        R[6, : N // 2] *= 1e30
+        fm = rng.random((T, N)) < 0.95
+        ranks, ic = fcb200.rank_ic_panel(X, R, fm, None, min_valid=3)
+        for f in range(F):
+            assert bitwise_f32(ranks[f], O.cs_rank(X[f], fm, False)), N
+            assert _ic_equal(ic[f], O.rolling_ic(X[f], R, fm, None, 3)), (N, f)
+
+
 def test_stock_corr_random(fcb):
     rng = np.random.default_rng(5)
     T, N = 200, 300
