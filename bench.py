@@ -400,8 +400,8 @@ def run_b200(args, rank, world):
 # of each kernel at T=600: dram__bytes_read.sum + dram__bytes_write.sum.
 # Traffic grows with the number of dates at fixed N and F, so the bench's step
 # is that times T.
-TRAFFIC_PER_DATE = {"learned": (153.391360e6 + 103.361792e6 + 18.050048e6) / 600,
-                    "radix": (153.914368e6 + 102.658048e6 + 18.050048e6) / 600}
+TRAFFIC_PER_DATE = {"learned": (156.591104e6 + 88.684544e6 + 18.057728e6) / 600,
+                    "radix": (156.073472e6 + 86.176000e6 + 18.057728e6) / 600}
 
 
 def max_over_ranks(values, device):
