@@ -453,6 +453,26 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
   uint32_t w[C];
   load_row_f32<NT, V, true>(a.X + frow, N, x);
   load_words<NT, V>(rp.word + static_cast<size_t>(t) * rp.ld, N, w);
+  // warp 0 issues the loads of the location / scale sample (used below) right
+  // behind the row's, so that both wait out one memory latency, not two
+  float xs[8];
+  uint32_t vs = 0u;
+  if (wi == 0) {
+    const int S = min(N, 256);  // i = s*N/S: s*N/256 when N >= 256, else s
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int s = q * 32 + lane;
+      xs[q] = 0.0f;
+      if (s < S) {
+        const int i = N >= 256 ? (s * N) >> 8 : s;
+        const float v = a.X[frow + i];
+        if (finite_f32(v) && (rp.word[static_cast<size_t>(t) * rp.ld + i] & kFacMask)) {
+          xs[q] = v;
+          vs |= 1u << q;
+        }
+      }
+    }
+  }
   uint32_t key[C], P[C];
   int nval = 0;
 #pragma unroll
@@ -468,26 +488,14 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
   // (mean and mean absolute deviation of up to 256 valid cells; they only
   // shape the bucket map -- the order is exact whatever they are)
   if (wi == 0) {
-    const int S = min(N, 256);  // i = s*N/S: s*N/256 when N >= 256, else s
-    float xs[8];
-    uint32_t vs = 0u;
     int ns = 0;
     float s1 = 0.0f;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int s = q * 32 + lane;
-      xs[q] = 0.0f;
-      if (s < S) {
-        const int i = N >= 256 ? (s * N) >> 8 : s;
-        const float v = a.X[frow + i];
-        if (finite_f32(v) && (rp.word[static_cast<size_t>(t) * rp.ld + i] & kFacMask)) {
-          xs[q] = v;
-          vs |= 1u << q;
-          s1 += v;
-          ++ns;
-        }
+    for (int q = 0; q < 8; ++q)
+      if ((vs >> q) & 1u) {
+        s1 += xs[q];
+        ++ns;
       }
-    }
     const float n_s = static_cast<float>(warp_sum(ns));
     const float mean = warp_sum(s1) / n_s;
     float s2 = 0.0f;
