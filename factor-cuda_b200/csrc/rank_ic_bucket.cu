@@ -433,21 +433,6 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
   int* stats = a.learn_stats != nullptr ? a.learn_stats + (static_cast<size_t>(f) * a.T + t) * 4 : nullptr;
   const int nwd = (N + 31) / 32 + 1;
 
-  // ---- stage the table (checking that it is non-decreasing within [0, 1]: a
-  // NaN fails every comparison), clear the counters and the drop bitmap
-  int tab_bad = 0;
-  {
-    const float* tg = a.cdf_table + static_cast<size_t>(f) * kCdfKnots;
-    for (int k = tid; k < kCdfKnots / 4; k += NT) {
-      const float4 v = __ldg(reinterpret_cast<const float4*>(tg) + k);
-      reinterpret_cast<float4*>(tab)[k] = v;
-      const float nx = (4 * k + 4 < kCdfKnots) ? __ldg(tg + 4 * k + 4) : 1.0f;
-      tab_bad |= (0.0f <= v.x && v.x <= v.y && v.y <= v.z && v.z <= v.w && v.w <= nx && nx <= 1.0f) ? 0 : 1;
-    }
-  }
-  for (int k = tid; k < (N + 2 + 3) / 4; k += NT) reinterpret_cast<uint4*>(cnt)[k] = make_uint4(0u, 0u, 0u, 0u);
-  for (int k = tid; k < nwd; k += NT) reinterpret_cast<unsigned long long*>(dw32)[k] = 0ull;
-
   // ---- the row and the date's prepared returns words
   float x[C];
   uint32_t w[C];
@@ -473,6 +458,22 @@ FCB_DEV void ric_learned_body(const RankIcArgs<float, float>& a, const RicPrep& 
       }
     }
   }
+  // ---- stage the table (checking that it is non-decreasing within [0, 1]: a
+  // NaN fails every comparison), clear the counters and the drop bitmap --
+  // after the row's loads are out, so that their latencies overlap
+  int tab_bad = 0;
+  {
+    const float* tg = a.cdf_table + static_cast<size_t>(f) * kCdfKnots;
+    for (int k = tid; k < kCdfKnots / 4; k += NT) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(tg) + k);
+      reinterpret_cast<float4*>(tab)[k] = v;
+      const float nx = (4 * k + 4 < kCdfKnots) ? __ldg(tg + 4 * k + 4) : 1.0f;
+      tab_bad |= (0.0f <= v.x && v.x <= v.y && v.y <= v.z && v.z <= v.w && v.w <= nx && nx <= 1.0f) ? 0 : 1;
+    }
+  }
+  for (int k = tid; k < (N + 2 + 3) / 4; k += NT) reinterpret_cast<uint4*>(cnt)[k] = make_uint4(0u, 0u, 0u, 0u);
+  for (int k = tid; k < nwd; k += NT) reinterpret_cast<unsigned long long*>(dw32)[k] = 0ull;
+
   uint32_t key[C], P[C];
   int nval = 0;
 #pragma unroll
