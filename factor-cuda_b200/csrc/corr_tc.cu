@@ -191,18 +191,18 @@ struct TcMaps {
 };
 
 __global__ void __launch_bounds__(192, 1)
-    k_corr_bf16x3(const __grid_constant__ TcMaps maps, const int2* __restrict__ tiles, int N, int Tp,
+    k_corr_bf16x3(const __grid_constant__ TcMaps maps, const int2* __restrict__ tiles, int ntiles, int N, int Tp,
                   double* __restrict__ out, int* __restrict__ status) {
   extern __shared__ __align__(1024) uint8_t sm_raw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + kTcStages * kStageBytes);
   uint64_t* empty = full + kTcStages;
-  uint64_t* accb = empty + kTcStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
+  uint64_t* accb = empty + kTcStages;   // accumulators of a tile complete (MMA commit)
+  uint64_t* tfree = accb + 1;           // accumulators read out (one arrival per epilogue warp)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tfree + 1);
   int* err = reinterpret_cast<int*>(tmem_slot + 1);
+  volatile int* verr = err;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int2 tile = tiles[blockIdx.x];
-  const int i0 = tile.x * kTcM, j0 = tile.y * kTcN;
   const int nkt = Tp / kTcK;
 
   if (threadIdx.x == 0) {
@@ -211,6 +211,7 @@ __global__ void __launch_bounds__(192, 1)
       mbar_init(&empty[s], 1);
     }
     mbar_init(accb, 1);
+    mbar_init(tfree, 4);
     *err = 0;
     fence_mbar_init();
   }
@@ -224,18 +225,27 @@ __global__ void __launch_bounds__(192, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
+  // Persistent CTAs walk the tile list with a stride of the grid.  The stage
+  // ring runs on across tiles, so the producer fills the next tile's stages
+  // while the epilogue drains this tile's accumulators; the MMA warp starts a
+  // tile once the epilogue has read the previous one out of TMEM.
   if (warp == 0) {
     if (lane == 0) {
-      for (int kt = 0; kt < nkt; ++kt) {
-        const int s = kt % kTcStages, round = kt / kTcStages;
-        if (round > 0 && !mbar_wait(&empty[s], (round - 1) & 1)) {
-          atomicExch(err, 1);
-          break;
+      int g = 0;
+      for (int tl = blockIdx.x; tl < ntiles && *verr == 0; tl += gridDim.x) {
+        const int2 tile = tiles[tl];
+        const int i0 = tile.x * kTcM, j0 = tile.y * kTcN;
+        for (int kt = 0; kt < nkt; ++kt, ++g) {
+          const int s = g % kTcStages, round = g / kTcStages;
+          if (round > 0 && !mbar_wait(&empty[s], (round - 1) & 1)) {
+            atomicExch(err, 1);
+            break;
+          }
+          uint8_t* st = sm + s * kStageBytes;
+          mbar_expect_tx(&full[s], kStageBytes);
+          tma_load_3d(st, &maps.a, kt * kTcK, i0, 0, &full[s]);
+          tma_load_3d(st + kABytesStage, &maps.b, kt * kTcK, j0, 0, &full[s]);
         }
-        uint8_t* st = sm + s * kStageBytes;
-        mbar_expect_tx(&full[s], kStageBytes);
-        tma_load_3d(st, &maps.a, kt * kTcK, i0, 0, &full[s]);
-        tma_load_3d(st + kABytesStage, &maps.b, kt * kTcK, j0, 0, &full[s]);
       }
     }
   } else if (warp == 1) {
@@ -243,75 +253,97 @@ __global__ void __launch_bounds__(192, 1)
       constexpr uint32_t id256 = idesc_bf16(kTcM, 4 * kTcN);
       constexpr uint32_t id128 = idesc_bf16(kTcM, 2 * kTcN);
       constexpr uint32_t id64 = idesc_bf16(kTcM, kTcN);
-      for (int kt = 0; kt < nkt; ++kt) {
-        const int s = kt % kTcStages, round = kt / kTcStages;
-        if (!mbar_wait(&full[s], round & 1)) {
+      int g = 0, it = 0;
+      for (int tl = blockIdx.x; tl < ntiles && *verr == 0; tl += gridDim.x, ++it) {
+        if (it > 0 && !mbar_wait(tfree, (it - 1) & 1)) {
           atomicExch(err, 1);
           break;
         }
         tc_fence_after();
-        const uint32_t abase = smem_u32(sm + s * kStageBytes);
-        const uint32_t bbase = abase + kABytesStage;
+        for (int kt = 0; kt < nkt; ++kt, ++g) {
+          const int s = g % kTcStages, round = g / kTcStages;
+          if (!mbar_wait(&full[s], round & 1)) {
+            atomicExch(err, 1);
+            break;
+          }
+          tc_fence_after();
+          const uint32_t abase = smem_u32(sm + s * kStageBytes);
+          const uint32_t bbase = abase + kABytesStage;
 #pragma unroll
-        for (int ks = 0; ks < kTcK / 16; ++ks) {
-          const uint32_t ak = abase + ks * 32, bk = bbase + ks * 32;
-          auto A = [&](int m) { return smem_desc_sw64(ak + m * kAMat); };  // rows of matrix m, stocks i
-          auto B = [&](int m) { return smem_desc_sw64(bk + m * kBMat); };  // from matrix m on, stocks j
-          const uint32_t first = (kt == 0 && ks == 0) ? 0u : 1u;
-          // D1: x limbs against [M; H; Mm; L]
-          mma_bf16(tmem + kD1, A(1), B(0), id256, first);
-          mma_bf16(tmem + kD1, A(2), B(0), id256, 1u);
-          mma_bf16(tmem + kD1, A(3), B(0), id256, 1u);
-          // n | sy: the mask against [M; H], then the other two y limbs into sy
-          mma_bf16(tmem + kDn, A(0), B(0), id128, first);
-          mma_bf16(tmem + kDsy, A(0), B(2), id64, 1u);
-          mma_bf16(tmem + kDsy, A(0), B(3), id64, 1u);
-          // sy2: the mask against the y'^2 limbs
-          mma_bf16(tmem + kDsy2, A(0), B(4), id64, first);
-          mma_bf16(tmem + kDsy2, A(0), B(5), id64, 1u);
-          mma_bf16(tmem + kDsy2, A(0), B(6), id64, 1u);
-          // sx2: the x'^2 limbs against the mask
-          mma_bf16(tmem + kDsx2, A(4), B(0), id64, first);
-          mma_bf16(tmem + kDsx2, A(5), B(0), id64, 1u);
-          mma_bf16(tmem + kDsx2, A(6), B(0), id64, 1u);
+          for (int ks = 0; ks < kTcK / 16; ++ks) {
+            const uint32_t ak = abase + ks * 32, bk = bbase + ks * 32;
+            auto A = [&](int m) { return smem_desc_sw64(ak + m * kAMat); };  // rows of matrix m, stocks i
+            auto B = [&](int m) { return smem_desc_sw64(bk + m * kBMat); };  // from matrix m on, stocks j
+            const uint32_t first = (kt == 0 && ks == 0) ? 0u : 1u;
+            // D1: x limbs against [M; H; Mm; L]
+            mma_bf16(tmem + kD1, A(1), B(0), id256, first);
+            mma_bf16(tmem + kD1, A(2), B(0), id256, 1u);
+            mma_bf16(tmem + kD1, A(3), B(0), id256, 1u);
+            // n | sy: the mask against [M; H], then the other two y limbs into sy
+            mma_bf16(tmem + kDn, A(0), B(0), id128, first);
+            mma_bf16(tmem + kDsy, A(0), B(2), id64, 1u);
+            mma_bf16(tmem + kDsy, A(0), B(3), id64, 1u);
+            // sy2: the mask against the y'^2 limbs
+            mma_bf16(tmem + kDsy2, A(0), B(4), id64, first);
+            mma_bf16(tmem + kDsy2, A(0), B(5), id64, 1u);
+            mma_bf16(tmem + kDsy2, A(0), B(6), id64, 1u);
+            // sx2: the x'^2 limbs against the mask
+            mma_bf16(tmem + kDsx2, A(4), B(0), id64, first);
+            mma_bf16(tmem + kDsx2, A(5), B(0), id64, 1u);
+            mma_bf16(tmem + kDsx2, A(6), B(0), id64, 1u);
+          }
+          mma_commit(&empty[s]);  // frees the stage when these MMAs complete
         }
-        mma_commit(&empty[s]);  // frees the stage when these MMAs complete
+        mma_commit(accb);
       }
-      mma_commit(accb);
     }
   } else {
     // epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 (its row quadrant)
     const int quad = warp & 3;
     const int row = quad * 32 + lane;
-    const bool ok = mbar_wait(accb, 0);
-    tc_fence_after();
-    if (!ok) atomicExch(err, 1);
-    const int i = i0 + row;
     const uint32_t t0 = tmem + (static_cast<uint32_t>(quad * 32) << 16);
-    for (int c0 = 0; c0 < kTcN; c0 += 16) {
-      float sx[16], n[16], sy[16], sy2[16], sx2[16], v[16];
-      double sxy[16];
-      tmem_ld16(t0 + kD1 + c0, sx);
-#pragma unroll
-      for (int u = 0; u < 16; ++u) sxy[u] = 0.0;
-#pragma unroll
-      for (int b = 1; b <= 3; ++b) {
-        tmem_ld16(t0 + kD1 + b * kTcN + c0, v);
-#pragma unroll
-        for (int u = 0; u < 16; ++u) sxy[u] += static_cast<double>(v[u]);
+    int it = 0;
+    for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x, ++it) {
+      const bool ok = mbar_wait(accb, it & 1);
+      tc_fence_after();
+      if (!ok) {
+        atomicExch(err, 1);
+        break;
       }
-      tmem_ld16(t0 + kDn + c0, n);
-      tmem_ld16(t0 + kDsy + c0, sy);
-      tmem_ld16(t0 + kDsy2 + c0, sy2);
-      tmem_ld16(t0 + kDsx2 + c0, sx2);
-      if (ok && *err == 0 && i < N) {
+      const int2 tile = tiles[tl];
+      const int i = tile.x * kTcM + row, j0 = tile.y * kTcN;
+      for (int c0 = 0; c0 < kTcN; c0 += 16) {
+        float sx[16], n[16], sy[16], sy2[16], sx2[16], v[16];
+        double sxy[16];
+        tmem_ld16(t0 + kD1 + c0, sx);
 #pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const int j = j0 + c0 + u;
-          if (j < N && i <= j)
-            write_pair(out, N, i, j, pearson_from_moments(n[u], sx[u], sy[u], sxy[u], sx2[u], sy2[u]));
+        for (int u = 0; u < 16; ++u) sxy[u] = 0.0;
+#pragma unroll
+        for (int b = 1; b <= 3; ++b) {
+          tmem_ld16(t0 + kD1 + b * kTcN + c0, v);
+#pragma unroll
+          for (int u = 0; u < 16; ++u) sxy[u] += static_cast<double>(v[u]);
+        }
+        tmem_ld16(t0 + kDn + c0, n);
+        tmem_ld16(t0 + kDsy + c0, sy);
+        tmem_ld16(t0 + kDsy2 + c0, sy2);
+        tmem_ld16(t0 + kDsx2 + c0, sx2);
+        if (c0 + 16 >= kTcN) {
+          // every column of this quadrant is in registers: hand TMEM back
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(tfree);
+        }
+        if (*verr == 0 && i < N) {
+#pragma unroll
+          for (int u = 0; u < 16; ++u) {
+            const int j = j0 + c0 + u;
+            if (j < N && i <= j)
+              write_pair(out, N, i, j, pearson_from_moments(n[u], sx[u], sy[u], sxy[u], sx2[u], sy2[u]));
+          }
         }
       }
+      if (*verr != 0) break;
     }
   }
   tc_fence_before();
@@ -494,7 +526,11 @@ cudaError_t launch_corr_bf16x3(const PrecOperands& op, const int2* tiles, int nt
   cudaError_t e = cudaFuncSetAttribute(k_corr_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  k_corr_bf16x3<<<ntiles, 192, smem, s>>>(maps, tiles, N, Tp, out, status);
+  int dev = 0, sms = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  const int grid = ntiles < sms ? ntiles : (sms > 0 ? sms : 1);  // one persistent CTA per SM
+  k_corr_bf16x3<<<grid, 192, smem, s>>>(maps, tiles, ntiles, N, Tp, out, status);
   return cudaGetLastError();
 }
 
