@@ -691,6 +691,37 @@ __host__ __device__ inline size_t fc_gram_raw_offset(int Fp, int tasks_per_block
   return ((stage > red ? stage : red) + 1) / 2 * 2;  // 16-byte aligned
 }
 
+// Gram pass on the FP64 tensor cores (mma.sync m8n8k4 .f64): 8 x 8 output
+// tiles of factors, four pooled rows per MMA.  The staged tiles hold Fq =
+// Fp rounded up to 8 factor rows (the extra rows stay zero) at a pitch of
+// chunk + 4 doubles: a fragment load (factor row lane / 4, pooled row lane % 4)
+// then touches 32 distinct banks per half-warp.  A unit of work is one A tile
+// (ti) against a group of up to two B tiles (tj); a block's eight warps split
+// its units and, when there are fewer than eight, the rows.
+constexpr int kFcMmaGroup = 2;
+__host__ __device__ inline int fc_mma_fq(int Fp) { return (Fp + 7) / 8 * 8; }
+__host__ __device__ inline int fc_mma_pitch(int Fp) { return fc_rows_chunk(Fp) + 4; }
+__host__ __device__ inline int fc_mma_units(int Fp) {
+  const int nt = fc_mma_fq(Fp) / 8;
+  return nt * ((nt + kFcMmaGroup - 1) / kFcMmaGroup);
+}
+__host__ __device__ inline int fc_mma_units_per_block(int Fp) {
+  const int u = fc_mma_units(Fp);
+  return u < 8 ? u : 8;
+}
+// Doubles before the raw-copy buffers: the staged tiles, or the slice
+// reduction buffer that reuses them after the row loop, whichever is larger.
+__host__ __device__ inline size_t fc_mma_raw_offset(int Fp, int units_per_block) {
+  const size_t stage = 2 * static_cast<size_t>(fc_mma_fq(Fp)) * fc_mma_pitch(Fp);
+  const size_t red = static_cast<size_t>(units_per_block) * kFcMmaGroup * 4 * 64;
+  return ((stage > red ? stage : red) + 1) / 2 * 2;  // 16-byte aligned
+}
+FCB_DEV void dmma_f64(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 // Asynchronous global -> shared copies of single elements (cp.async, L1
 // allocating); each thread waits for its own groups, a barrier publishes them.
 template <int BYTES>
@@ -702,7 +733,7 @@ FCB_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memo
 FCB_DEV void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 template <typename TIN>
-FCB_DEV void fc_gram_body(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+FCB_DEV void fc_gram_body_fma(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
                                                  long long R, int F, long long sr, long long sf, int Fp,
                                                  long long rows_per_block,
                                                  const FcColStat* __restrict__ st, int tasks_total,
@@ -848,12 +879,201 @@ FCB_DEV void fc_gram_body(const TIN* __restrict__ X, const uint8_t* __restrict__
 }
 
 template <typename TIN>
+FCB_DEV void fc_gram_body_mma(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
+                                                 long long R, int F, long long sr, long long sf, int Fp,
+                                                 long long rows_per_block,
+                                                 const FcColStat* __restrict__ st, int tasks_total,
+                                                 int tasks_per_block, double* __restrict__ part, const Blk bk) {
+  extern __shared__ __align__(16) double fsm[];
+  const int chunk = fc_rows_chunk(Fp);
+  const int pitch = fc_mma_pitch(Fp);
+  const int Fq = fc_mma_fq(Fp);
+  double* sx = fsm;                                  // [Fq][pitch] centred values
+  double* sm = sx + static_cast<size_t>(Fq) * pitch; // [Fq][pitch] validity
+  double* red = fsm;  // [unit][tj][product][64], over the staging tiles once they are idle
+  const int nt = Fq / 8, ng = (nt + kFcMmaGroup - 1) / kFcMmaGroup;
+  const int unit0 = bk.y * tasks_per_block;
+  const int nunit = min(tasks_per_block, tasks_total - unit0);
+  const int warp = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
+  const int slices = 8 / nunit;
+  const int my_unit = warp % nunit, my_slice = warp / nunit;
+  const bool active = my_slice < slices;
+  const int ti = (unit0 + my_unit) / ng, tj0 = ((unit0 + my_unit) % ng) * kFcMmaGroup;
+  const int ntj = min(kFcMmaGroup, nt - tj0);
+  double acc[kFcMmaGroup][4][2];  // [tj][product: n, sx, sx2, sxy][lane's two D values]
+#pragma unroll
+  for (int j = 0; j < kFcMmaGroup; ++j)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[j][q][0] = acc[j][q][1] = 0.0;
+  // the factor rows past Fp stay zero for the whole pass
+  for (int e = threadIdx.x; e < (Fq - Fp) * pitch; e += 256) {
+    sx[static_cast<size_t>(Fp) * pitch + e] = 0.0;
+    sm[static_cast<size_t>(Fp) * pitch + e] = 0.0;
+  }
+  const long long r0 = bk.x * rows_per_block;
+  const long long r1 = min(R, r0 + rows_per_block);
+  // Row chunks are pipelined: while chunk k is centred and multiplied, the raw
+  // elements of chunk k + 1 are in flight into the other raw buffer
+  // (cp.async) and its mask bytes in a register.
+  TIN* raw[2];
+  raw[0] = reinterpret_cast<TIN*>(fsm + fc_mma_raw_offset(Fp, tasks_per_block));
+  raw[1] = raw[0] + chunk * Fp;
+  uint8_t* smask = reinterpret_cast<uint8_t*>(raw[1] + chunk * Fp);
+  // Element e of a staged chunk is (row rr, factor f): rr = e / Fp, f = e % Fp
+  // for the (rows, F) layout, rr = e % chunk, f = e / chunk for factor planes,
+  // so that consecutive threads read consecutive elements of X either way.
+  // Each thread walks e = tid, tid + 256, ...: one division up front, then a
+  // constant step with a carry.
+  const bool planes = sf != 1;
+  const int inner = planes ? chunk : Fp;  // extent of the fast index
+  const int e0_in = threadIdx.x % inner, e0_out = threadIdx.x / inner;
+  const int step_in = 256 % inner, step_out = 256 / inner;
+  auto issue = [&](long long cs, TIN* dst) {
+    const int nrs = static_cast<int>(min(static_cast<long long>(chunk), r1 - cs));
+    const TIN* base = X + cs * sr;
+    int a = e0_in, b = e0_out;  // (fast, slow) index of element e
+    for (int e = threadIdx.x; e < chunk * Fp; e += 256) {
+      const int rr = planes ? a : b;
+      const int f = planes ? b : a;
+      if (rr < nrs && f < F) cp_async_elem<sizeof(TIN)>(dst + e, base + rr * sr + f * sf);
+      a += step_in;
+      b += step_out;
+      if (a >= inner) {
+        a -= inner;
+        ++b;
+      }
+    }
+  };
+  auto mask_of = [&](long long cs) -> uint8_t {
+    const long long r = cs + threadIdx.x;
+    return (mask == nullptr || threadIdx.x >= chunk || r >= r1) ? uint8_t(1) : mask[r];
+  };
+  uint8_t m_cur = 1;
+  if (r0 < r1) {
+    issue(r0, raw[0]);
+    m_cur = mask_of(r0);
+  }
+  cp_async_commit();
+  int it = 0;
+  for (long long c0 = r0; c0 < r1; c0 += chunk, ++it) {
+    const int nr = static_cast<int>(min(static_cast<long long>(chunk), r1 - c0));
+    uint8_t m_next = 1;
+    if (c0 + chunk < r1) {
+      issue(c0 + chunk, raw[(it + 1) & 1]);
+      m_next = mask_of(c0 + chunk);
+    }
+    cp_async_commit();
+    if (threadIdx.x < chunk) smask[threadIdx.x] = m_cur;
+    cp_async_wait_prev();  // this thread's copies of chunk `it` have landed
+    __syncthreads();
+    const TIN* rb = raw[it & 1];
+    int a = e0_in, b = e0_out;
+    for (int e = threadIdx.x; e < chunk * Fp; e += 256) {
+      const int rr = planes ? a : b;
+      const int f = planes ? b : a;
+      a += step_in;
+      b += step_out;
+      if (a >= inner) {
+        a -= inner;
+        ++b;
+      }
+      const int ei = f * pitch + rr;
+      double v = 0.0, mv = 0.0;
+      if (rr < nr && f < F) {
+        const double x = static_cast<double>(rb[e]);
+        if (finite_f64(x) && smask[rr] != 0) {
+          v = x - st[f].mean;
+          mv = 1.0;
+        }
+      }
+      sx[ei] = v;
+      sm[ei] = mv;
+    }
+    __syncthreads();
+    if (active) {
+      // fragments: lane holds factor row lane / 4 of a tile at pooled row
+      // r + lane % 4 (A row-major 8 x 4, B column-major 4 x 8: the same address)
+      const int fr = lane >> 2, kc = lane & 3;
+      const int kend = (nr + 3) & ~3;  // rows past nr are zero
+      for (int r = 4 * my_slice; r < kend; r += 4 * slices) {
+        const size_t ao = static_cast<size_t>(8 * ti + fr) * pitch + r + kc;
+        const double am = sm[ao], ax = sx[ao];
+        const double ax2 = ax * ax;
+#pragma unroll
+        for (int j = 0; j < kFcMmaGroup; ++j) {
+          if (j < ntj) {
+            const int tj = tj0 + j;
+            const size_t bo = static_cast<size_t>(8 * tj + fr) * pitch + r + kc;
+            const double bm = sm[bo], bx = sx[bo];
+            if (tj >= ti) {  // n and sxy: tiles on or above the diagonal
+              dmma_f64(acc[j][0], am, bm);
+              dmma_f64(acc[j][3], ax, bx);
+            }
+            dmma_f64(acc[j][1], ax, bm);
+            dmma_f64(acc[j][2], ax2, bm);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    m_cur = m_next;
+  }
+  // reduce the row slices in slice order (D value e of a lane: tile row
+  // lane / 4, column 2 (lane % 4) + e)
+  for (int sl = 0; sl < slices; ++sl) {
+    if (active && my_slice == sl) {
+#pragma unroll
+      for (int j = 0; j < kFcMmaGroup; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            double* d = red + ((static_cast<size_t>(my_unit) * kFcMmaGroup + j) * 4 + q) * 64 +
+                        (lane >> 2) * 8 + 2 * (lane & 3) + e;
+            *d = (sl == 0) ? acc[j][q][e] : *d + acc[j][q][e];
+          }
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < nunit * kFcMmaGroup * 4 * 64; e += 256) {
+    const int idx = e & 63, q = (e >> 6) & 3, j = (e >> 8) % kFcMmaGroup, ul = e / (256 * kFcMmaGroup);
+    const int uti = (unit0 + ul) / ng, utj = ((unit0 + ul) % ng) * kFcMmaGroup + j;
+    if (utj >= nt || ((q == 0 || q == 3) && utj < uti)) continue;
+    const int f = 8 * uti + (idx >> 3), g = 8 * utj + (idx & 7);
+    if (f < Fp && g < Fp) part[((static_cast<size_t>(bk.x) * 4 + q) * Fp + f) * Fp + g] = red[e];
+  }
+}
+
+// The Gram pass takes the FP64 tensor cores when the padded factor count is a
+// multiple of 8 (no padded tile rows); otherwise the 4 x 4 FMA tiles, which
+// waste less on padding.  tasks_total / tasks_per_block come from
+// fc_gram_plan for the same Fp.
+__host__ __device__ inline bool fc_gram_use_mma(int Fp) { return Fp % 8 == 0; }
+template <typename TIN>
+FCB_DEV void fc_gram_body(const TIN* __restrict__ X, const uint8_t* __restrict__ mask, long long R, int F,
+                          long long sr, long long sf, int Fp, long long rows_per_block,
+                          const FcColStat* __restrict__ st, int tasks_total, int tasks_per_block,
+                          double* __restrict__ part, const Blk bk) {
+  if (fc_gram_use_mma(Fp))
+    fc_gram_body_mma<TIN>(X, mask, R, F, sr, sf, Fp, rows_per_block, st, tasks_total, tasks_per_block, part, bk);
+  else
+    fc_gram_body_fma<TIN>(X, mask, R, F, sr, sf, Fp, rows_per_block, st, tasks_total, tasks_per_block, part, bk);
+}
+
+// Single panel: the path is chosen on the host (MMA = fc_gram_use_mma(Fp)), so
+// each instantiation holds one body.
+template <typename TIN, bool MMA>
 __global__ void __launch_bounds__(256, 3) k_fc_gram(const TIN* __restrict__ X, const uint8_t* __restrict__ mask,
                                                  long long R, int F, long long sr, long long sf, int Fp,
                                                  long long rows_per_block,
                                                  const FcColStat* __restrict__ st, int tasks_total,
                                                  int tasks_per_block, double* __restrict__ part) {
-  fc_gram_body<TIN>(X, mask, R, F, sr, sf, Fp, rows_per_block, st, tasks_total, tasks_per_block, part, launch_blk());
+  if (MMA)
+    fc_gram_body_mma<TIN>(X, mask, R, F, sr, sf, Fp, rows_per_block, st, tasks_total, tasks_per_block, part,
+                          launch_blk());
+  else
+    fc_gram_body_fma<TIN>(X, mask, R, F, sr, sf, Fp, rows_per_block, st, tasks_total, tasks_per_block, part,
+                          launch_blk());
 }
 
 // Sum the per-block Gram partials in block order, finalize each pair.
@@ -1367,7 +1587,20 @@ int fc_fb_nblk(long long R, int F) {
 
 size_t fc_gram_smem(int Fp, int tasks_per_block, int elem_bytes) {
   const size_t raw = 2 * static_cast<size_t>(fc_rows_chunk(Fp)) * Fp * elem_bytes + fc_rows_chunk(Fp);
-  return fc_gram_raw_offset(Fp, tasks_per_block) * sizeof(double) + (raw + 15) / 16 * 16;
+  const size_t off = fc_gram_use_mma(Fp) ? fc_mma_raw_offset(Fp, tasks_per_block)
+                                         : fc_gram_raw_offset(Fp, tasks_per_block);
+  return off * sizeof(double) + (raw + 15) / 16 * 16;
+}
+
+void fc_gram_plan(int Fp, int* tasks_total, int* tasks_per_block, int* ytiles) {
+  if (fc_gram_use_mma(Fp)) {
+    *tasks_total = fc_mma_units(Fp);
+    *tasks_per_block = fc_mma_units_per_block(Fp);
+  } else {
+    *tasks_total = fc_gram_tasks(Fp / 4);
+    *tasks_per_block = *tasks_total <= 256 ? *tasks_total : 256;
+  }
+  *ytiles = (*tasks_total + *tasks_per_block - 1) / *tasks_per_block;
 }
 
 cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* mask, long long R, int F,
@@ -1375,9 +1608,9 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
                                        cudaStream_t s) {
   const int Fp = (F + 3) / 4 * 4;
   const int tb = Fp / 4;
-  const int tasks_total = fc_gram_tasks(tb);
-  const int tasks_per_block = tasks_total <= 256 ? tasks_total : 256;
-  const int ytiles = (tasks_total + tasks_per_block - 1) / tasks_per_block;
+  (void)tb;
+  int tasks_total = 0, tasks_per_block = 0, ytiles = 0;
+  fc_gram_plan(Fp, &tasks_total, &tasks_per_block, &ytiles);
   const long long rpb_cols = (R + w.nblk_cols - 1) / w.nblk_cols;
   const long long rpb_gram = (R + w.nblk_gram - 1) / w.nblk_gram;
   dim3 cb(32, 8);
@@ -1400,17 +1633,21 @@ cudaError_t launch_factor_corr_strided(const void* X, int dtype, const uint8_t* 
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const size_t smem = fc_gram_smem(Fp, tasks_per_block, dtype == 0 ? 4 : 8);
   dim3 gg(w.nblk_gram, ytiles);
-  if (dtype == 0) {
-    e = cudaFuncSetAttribute(k_fc_gram<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    k_fc_gram<float><<<gg, 256, smem, s>>>(static_cast<const float*>(X), mask, R, F, sr, sf, Fp, rpb_gram,
-                                           w.colstat, tasks_total, tasks_per_block, w.gram);
-  } else {
-    e = cudaFuncSetAttribute(k_fc_gram<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    k_fc_gram<double><<<gg, 256, smem, s>>>(static_cast<const double*>(X), mask, R, F, sr, sf, Fp, rpb_gram,
-                                            w.colstat, tasks_total, tasks_per_block, w.gram);
-  }
+  auto gram = [&](auto kernel, const auto* x) -> cudaError_t {
+    const cudaError_t ge =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (ge != cudaSuccess) return ge;
+    kernel<<<gg, 256, smem, s>>>(x, mask, R, F, sr, sf, Fp, rpb_gram, w.colstat, tasks_total, tasks_per_block, w.gram);
+    return cudaSuccess;
+  };
+  const bool mma = fc_gram_use_mma(Fp);
+  if (dtype == 0)
+    e = mma ? gram(k_fc_gram<float, true>, static_cast<const float*>(X))
+            : gram(k_fc_gram<float, false>, static_cast<const float*>(X));
+  else
+    e = mma ? gram(k_fc_gram<double, true>, static_cast<const double*>(X))
+            : gram(k_fc_gram<double, false>, static_cast<const double*>(X));
+  if (e != cudaSuccess) return e;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(w.fb_count, 0, sizeof(int), s)) != cudaSuccess) return e;
   k_fc_final<<<(F * F * 32 + 255) / 256, 256, 0, s>>>(w.gram, w.nblk_gram, F, Fp, w.colstat, out, w.fb_list,
@@ -1572,9 +1809,8 @@ FcBatchPanel fc_batch_panel(const void* X, const uint8_t* mask, long long R, int
   q.w = w;
   q.out = out;
   const int tb = q.Fp / 4;
-  q.tasks_total = fc_gram_tasks(tb);
-  q.tasks_per_block = q.tasks_total <= 256 ? q.tasks_total : 256;
-  q.ytiles = (q.tasks_total + q.tasks_per_block - 1) / q.tasks_per_block;
+  (void)tb;
+  fc_gram_plan(q.Fp, &q.tasks_total, &q.tasks_per_block, &q.ytiles);
   q.rpb_cols = (R + w.nblk_cols - 1) / w.nblk_cols;
   q.rpb_gram = (R + w.nblk_gram - 1) / w.nblk_gram;
   q.maxpairs = F * (F - 1) / 2 > 0 ? F * (F - 1) / 2 : 1;

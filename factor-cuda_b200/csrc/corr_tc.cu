@@ -180,7 +180,7 @@ FCB_DEV void write_pair(double* out, int N, int i, int j, double r) {
 }
 
 // ---------------------------------------------------------------------------
-// BF16x3 tcgen05 kernel: one 128 x 32 output tile per CTA
+// BF16x3 tcgen05 kernel: persistent CTAs over 128 x 64 output tiles
 // warps: 0 TMA producer, 1 TMEM owner + MMA issuer, 2..5 epilogue
 // ---------------------------------------------------------------------------
 // Two 3D views of the [7][Np][Tp] operand buffer (64-byte swizzle): one TMA

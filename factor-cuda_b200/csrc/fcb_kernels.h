@@ -162,6 +162,9 @@ cudaError_t launch_corr_domain(const void* X, int dtype, const uint8_t* mask, lo
 cudaError_t launch_stock_corr_gram(const double* Xraw, const double* Xc, const double* Mc, const ColStat* st, int T,
                                    int N, int Tp, double* out, int* fb_list, int* fb_count, cudaStream_t s);
 size_t fc_gram_smem(int Fp, int tasks_per_block, int elem_bytes);
+// Work split of the Gram pass for Fp (factors rounded to 4): tiles or tile
+// units in all, per block (blockIdx.y), and the blocks along y.
+void fc_gram_plan(int Fp, int* tasks_total, int* tasks_per_block, int* ytiles);
 cudaError_t launch_factor_corr(const void* X, int dtype, const uint8_t* mask, long long R, int F, FcWork& w,
                                double* out, uint8_t* flags, cudaStream_t s);
 // Returns of each date prepared once for the per-(date, factor) rank + IC
