@@ -56,6 +56,10 @@ constexpr int kStageBytes = kABytesStage + kBBytesStage;
 // TMEM columns of the accumulators (64 columns = one tile width each)
 constexpr int kD1 = 0, kDn = 4 * kTcN, kDsy = 5 * kTcN, kDsy2 = 6 * kTcN, kDsx2 = 7 * kTcN;
 constexpr int kTmemCols = 8 * kTcN;
+// warps: 0 TMA producer, 1 TMEM owner + MMA issuer, 2..9 epilogue (two per TMEM
+// lane quadrant, each reading half of the tile's columns)
+constexpr int kTcEpiWarps = 8;
+constexpr int kTcThreads = (2 + kTcEpiWarps) * 32;
 static_assert(kTmemCols == 512, "the accumulators fill the TMEM of one CTA");
 
 // ---------------------------------------------------------------------------
@@ -181,7 +185,7 @@ FCB_DEV void write_pair(double* out, int N, int i, int j, double r) {
 
 // ---------------------------------------------------------------------------
 // BF16x3 tcgen05 kernel: persistent CTAs over 128 x 64 output tiles
-// warps: 0 TMA producer, 1 TMEM owner + MMA issuer, 2..5 epilogue
+// warps: 0 TMA producer, 1 TMEM owner + MMA issuer, 2..9 epilogue
 // ---------------------------------------------------------------------------
 // Two 3D views of the [7][Np][Tp] operand buffer (64-byte swizzle): one TMA
 // per operand fills a whole stage.
@@ -190,7 +194,7 @@ struct TcMaps {
   CUtensorMap b;  // box {32, 32, 7}
 };
 
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(kTcThreads, 1)
     k_corr_bf16x3(const __grid_constant__ TcMaps maps, const int2* __restrict__ tiles, int ntiles, int N, int Tp,
                   double* __restrict__ out, int* __restrict__ status) {
   extern __shared__ __align__(1024) uint8_t sm_raw[];
@@ -211,7 +215,7 @@ __global__ void __launch_bounds__(192, 1)
       mbar_init(&empty[s], 1);
     }
     mbar_init(accb, 1);
-    mbar_init(tfree, 4);
+    mbar_init(tfree, kTcEpiWarps);
     *err = 0;
     fence_mbar_init();
   }
@@ -298,9 +302,11 @@ __global__ void __launch_bounds__(192, 1)
       }
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 (its row quadrant)
-    const int quad = warp & 3;
+    // epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 (its row quadrant),
+    // columns [half * kTcN/2, (half + 1) * kTcN/2)
+    const int quad = warp & 3, half = (warp - 2) >> 2;
     const int row = quad * 32 + lane;
+    const int cb = half * (kTcN / 2), ce = cb + kTcN / 2;
     const uint32_t t0 = tmem + (static_cast<uint32_t>(quad * 32) << 16);
     int it = 0;
     for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x, ++it) {
@@ -312,7 +318,7 @@ __global__ void __launch_bounds__(192, 1)
       }
       const int2 tile = tiles[tl];
       const int i = tile.x * kTcM + row, j0 = tile.y * kTcN;
-      for (int c0 = 0; c0 < kTcN; c0 += 16) {
+      for (int c0 = cb; c0 < ce; c0 += 16) {
         float sx[16], n[16], sy[16], sy2[16], sx2[16], v[16];
         double sxy[16];
         tmem_ld16(t0 + kD1 + c0, sx);
@@ -328,7 +334,7 @@ __global__ void __launch_bounds__(192, 1)
         tmem_ld16(t0 + kDsy + c0, sy);
         tmem_ld16(t0 + kDsy2 + c0, sy2);
         tmem_ld16(t0 + kDsx2 + c0, sx2);
-        if (c0 + 16 >= kTcN) {
+        if (c0 + 16 >= ce) {
           // every column of this quadrant is in registers: hand TMEM back
           tc_fence_before();
           __syncwarp();
@@ -530,7 +536,7 @@ cudaError_t launch_corr_bf16x3(const PrecOperands& op, const int2* tiles, int nt
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
   const int grid = ntiles < sms ? ntiles : (sms > 0 ? sms : 1);  // one persistent CTA per SM
-  k_corr_bf16x3<<<grid, 192, smem, s>>>(maps, tiles, ntiles, N, Tp, out, status);
+  k_corr_bf16x3<<<grid, kTcThreads, smem, s>>>(maps, tiles, ntiles, N, Tp, out, status);
   return cudaGetLastError();
 }
 

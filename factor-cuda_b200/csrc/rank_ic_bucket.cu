@@ -294,7 +294,7 @@ FCB_DEV void ric_epilogue(const RankIcArgs<float, float>& a, const RicPrep& rp, 
       kmax = fkmax;
     }
     if (b) {
-      // the learned order failed its judge: the radix kernel redoes the section
+      // the caller's order check failed (bad): the radix kernel redoes the section
       if (stats != nullptr) stats[0] = kLearnJudge;
       fb.items[atomicAdd(fb.count, 1)] = item_id;
     } else {
