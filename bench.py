@@ -922,9 +922,11 @@ def bench_stock_corr(dev, N, T=1218, steps=5, warmup=2, oracle=True):
     stream = torch.cuda.current_stream(dev)
     ws = lib.fcb_workspace_create()
     Tp = (T + 31) // 32 * 32
-    n_i = (N + 127) // 128
-    tiles = sum(1 for ti in range(n_i) for tj in range((N + 31) // 32) if tj * 32 + 31 >= ti * 128)
-    exec_flops = tiles * (Tp // 16) * 2.0 * 128 * 704 * 16   # issued MMA work (N-total 704 per 16 dates)
+    n_i, n_j = (N + 127) // 128, (N + 63) // 64
+    tiles = n_i * n_j - n_i * (n_i - 1)   # 128 x 64 tiles with tj >= 2 ti
+    # issued MMA work: per tile and 16 dates, M=128 MMAs of N-total 1216
+    # (D1 256 + 192 + 128, n|sy 128 + 64 + 64, sy2 3 x 64, sx2 3 x 64)
+    exec_flops = tiles * (Tp // 16) * 2.0 * 128 * 1216 * 16
     out = {}
     for name, mode in (("bf16x3", 0), ("fp32", 1)):
         def call():

@@ -15,8 +15,13 @@
 // stocks.  Per 16-deep k step (tcgen05.mma kind::f16, bf16 in, fp32
 // accumulate in TMEM), with every limb of a sum accumulated into the same
 // TMEM columns:
-//   D1  (256 cols) += a . [M; H; Mm; L]_j^T   for a in {H, Mm, L}_i
+//   D1  (256 cols) += H_i . [M; H; Mm; L]_j^T, Mm_i . [M; H; Mm]_j^T,
+//                     L_i . [M; H]_j^T
 //                     -> sx | three column blocks whose sum is sxy
+//                     (the limb products Mm.L, L.Mm and L.L are left out: a
+//                     limb is below 2^-8 of the one above it, so they are
+//                     under 2^-26 of x'_i x'_j, below the FP32 accumulation's
+//                     own rounding)
 //   Dn|Dsy (128)    = M_i . [M; H]_j^T, then Dsy += M_i . Mm_j^T, M_i . L_j^T
 //   Dsy2 (64)      += M_i . q_j^T            for q in {Qh, Qm, Ql}
 //   Dsx2 (64)      += q_i . M_j^T            for q in {Qh, Qm, Ql}
@@ -255,6 +260,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t id256 = idesc_bf16(kTcM, 4 * kTcN);
+      constexpr uint32_t id192 = idesc_bf16(kTcM, 3 * kTcN);
       constexpr uint32_t id128 = idesc_bf16(kTcM, 2 * kTcN);
       constexpr uint32_t id64 = idesc_bf16(kTcM, kTcN);
       int g = 0, it = 0;
@@ -279,10 +285,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             auto A = [&](int m) { return smem_desc_sw64(ak + m * kAMat); };  // rows of matrix m, stocks i
             auto B = [&](int m) { return smem_desc_sw64(bk + m * kBMat); };  // from matrix m on, stocks j
             const uint32_t first = (kt == 0 && ks == 0) ? 0u : 1u;
-            // D1: x limbs against [M; H; Mm; L]
+            // D1: H against [M; H; Mm; L], Mm against [M; H; Mm], L against [M; H]
             mma_bf16(tmem + kD1, A(1), B(0), id256, first);
-            mma_bf16(tmem + kD1, A(2), B(0), id256, 1u);
-            mma_bf16(tmem + kD1, A(3), B(0), id256, 1u);
+            mma_bf16(tmem + kD1, A(2), B(0), id192, 1u);
+            mma_bf16(tmem + kD1, A(3), B(0), id128, 1u);
             // n | sy: the mask against [M; H], then the other two y limbs into sy
             mma_bf16(tmem + kDn, A(0), B(0), id128, first);
             mma_bf16(tmem + kDsy, A(0), B(2), id64, 1u);
