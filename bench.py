@@ -316,7 +316,7 @@ def run_b200(args, rank, world):
                         "speedup_vs_radix": radix_ms / learned_ms_cmp}
 
     # e2e: host entry point, pinned buffers, copies in the timed region
-    e2e_s = e2e_ok = None
+    e2e_s = e2e_ok = e2e_floor = None
     if not args.no_e2e:
         hX = torch.from_numpy(X).pin_memory()
         hR = torch.from_numpy(R).pin_memory()
@@ -351,7 +351,20 @@ def run_b200(args, rank, world):
         e2e_s = (time.perf_counter() - t0) / args.steps
         lib.fcb_workspace_destroy(ws)
         e2e_ok = bool(np.array_equal(hranks.numpy().view(np.uint32), timed_ranks.view(np.uint32)))
+        h2d = hX.numel() * 4 + hR.numel() * 4 + hfm.numel() + hrm.numel()
+        d2h = hranks.numel() * 4 + hic.numel() * 8
+        del hX, hR, hfm, hrm, hranks, hic
+        e2e_floor = transfer_floor(h2d, d2h, dev)
     res = finish(args, world, X, R, fm, rm, ms, e2e_s, e2e_ok, clk, dev, learned_info)
+    if e2e_floor is not None and res.get("e2e"):
+        e = res["e2e"]
+        floor_v = world * X.size / e2e_floor["both_s"] / 1e9
+        e["transfer_floor"] = {
+            "what": "this box's copy floor: the step's input and output bytes as one plain pinned copy each way, "
+                    "both directions at once, no compute (best of 3)",
+            "value": floor_v, "unit": "Gelem/s", "ms": e2e_floor["both_s"] * 1e3,
+            "h2d_gb_s": e2e_floor["h2d_gb_s"], "d2h_gb_s": e2e_floor["d2h_gb_s"],
+            "both_gb_s": e2e_floor["both_gb_s"], "e2e_frac_of_floor": e["value"] / floor_v}
     fcl = bench_factor_corr(dX, dfm, X, fm, dev, steps=max(3, args.steps // 2))
     res["factor_corr"] = fcl
     res["c2_stages"] = bench_c2_stages(dX, X, fm, dev, ms, fcl["f64"]["ms"])
@@ -402,6 +415,34 @@ def run_b200(args, rank, world):
 # is that times T.
 TRAFFIC_PER_DATE = {"learned": (156.591104e6 + 88.684544e6 + 18.057728e6) / 600,
                     "radix": (156.073472e6 + 86.176000e6 + 18.057728e6) / 600}
+
+
+def transfer_floor(h2d_bytes, d2h_bytes, dev, reps=3):
+    """The host<->device copy floor of the e2e leg on this box: the same bytes
+    as one pinned copy per direction, alone and both at once (best of reps)."""
+    hin = torch.empty(h2d_bytes, dtype=torch.uint8).pin_memory()
+    hout = torch.empty(d2h_bytes, dtype=torch.uint8).pin_memory()
+    din = torch.empty(h2d_bytes, dtype=torch.uint8, device=dev)
+    dout = torch.zeros(d2h_bytes, dtype=torch.uint8, device=dev)
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    best = {}
+    for mode in ("h2d", "d2h", "both"):
+        t = []
+        for _ in range(reps):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            if mode in ("h2d", "both"):
+                with torch.cuda.stream(s_in):
+                    din.copy_(hin, non_blocking=True)
+            if mode in ("d2h", "both"):
+                with torch.cuda.stream(s_out):
+                    hout.copy_(dout, non_blocking=True)
+            torch.cuda.synchronize(dev)
+            t.append(time.perf_counter() - t0)
+        best[mode] = min(t)
+    del hin, hout, din, dout
+    return {"h2d_gb_s": h2d_bytes / best["h2d"] / 1e9, "d2h_gb_s": d2h_bytes / best["d2h"] / 1e9,
+            "both_gb_s": (h2d_bytes + d2h_bytes) / best["both"] / 1e9, "both_s": best["both"]}
 
 
 def max_over_ranks(values, device):
