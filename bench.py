@@ -420,6 +420,7 @@ TRAFFIC_PER_DATE = {"learned": (156.591104e6 + 88.684544e6 + 18.057728e6) / 600,
 def transfer_floor(h2d_bytes, d2h_bytes, dev, reps=3):
     """The host<->device copy floor of the e2e leg on this box: the same bytes
     as one pinned copy per direction, alone and both at once (best of reps)."""
+    import torch
     hin = torch.empty(h2d_bytes, dtype=torch.uint8).pin_memory()
     hout = torch.empty(d2h_bytes, dtype=torch.uint8).pin_memory()
     din = torch.empty(h2d_bytes, dtype=torch.uint8, device=dev)
