@@ -360,7 +360,7 @@ def run_b200(args, rank, world):
         e = res["e2e"]
         floor_v = world * X.size / e2e_floor["both_s"] / 1e9
         e["transfer_floor"] = {
-            "what": "this box's copy floor: the step's input and output bytes as one plain pinned copy each way, "
+            "what": "this machine's copy floor: the step's input and output bytes as one plain pinned copy each way, "
                     "both directions at once, no compute (best of 3)",
             "value": floor_v, "unit": "Gelem/s", "ms": e2e_floor["both_s"] * 1e3,
             "h2d_gb_s": e2e_floor["h2d_gb_s"], "d2h_gb_s": e2e_floor["d2h_gb_s"],
@@ -418,7 +418,7 @@ TRAFFIC_PER_DATE = {"learned": (156.591104e6 + 88.684544e6 + 18.057728e6) / 600,
 
 
 def transfer_floor(h2d_bytes, d2h_bytes, dev, reps=3):
-    """The host<->device copy floor of the e2e leg on this box: the same bytes
+    """The host<->device copy floor of the e2e leg on this machine: the same bytes
     as one pinned copy per direction, alone and both at once (best of reps)."""
     import torch
     hin = torch.empty(h2d_bytes, dtype=torch.uint8).pin_memory()
