@@ -243,7 +243,7 @@ def run_b200(args, rank, world):
             return
         rc = lib.fcb_dev_rank_ic_panel_learned(dX.data_ptr(), dR.data_ptr(), dfm.data_ptr(), drm.data_ptr(), F, T,
                                                N, MIN_VALID, dranks.data_ptr(), dic.data_ptr(),
-                                               learn["model"].handle, 64, learn["stats"].data_ptr(),
+                                               learn["model"].handle, args.learn_cap, learn["stats"].data_ptr(),
                                                stream.cuda_stream)
         nat.check(rc, "fcb_dev_rank_ic_panel_learned")
 
@@ -828,7 +828,7 @@ def bench_c5(dev, T=5000, N=8000, F=128, Tb=250, seed=20261206, cpu_sample=True,
     def learned(model, b, X, R, fm, rm, out):
         nat.check(lib.fcb_dev_rank_ic_panel_learned(X.data_ptr(), R.data_ptr(), fm.data_ptr(), rm.data_ptr(), F,
                                                     Tb, N, MIN_VALID, out.data_ptr(), ic.data_ptr(), model.handle,
-                                                    64, stats[b].data_ptr(), s), "learned")
+                                                    256, stats[b].data_ptr(), s), "learned")
 
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     # ---- radix run (per-block events for the same-blocks comparison)
@@ -1082,6 +1082,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--method", choices=["radix", "learned"], default="learned")
+    ap.add_argument("--learn-cap", type=int, default=256,
+                    help="largest bucket the learned rank kernel ranks itself (larger ones go to radix)")
     ap.add_argument("--no-stock-corr", action="store_true", help="skip the stock_corr precision-form leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")

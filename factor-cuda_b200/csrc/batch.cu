@@ -183,7 +183,7 @@ int upload_args(fcb_batch& b) {
       r.cdf_table = q.model->table[q.model->cur];
       r.cdf_zrange = q.model->zrange[q.model->cur];
     }
-    r.learn_cap = b.cfg.learn_cap > 0 ? b.cfg.learn_cap : 64;
+    r.learn_cap = b.cfg.learn_cap > 0 ? b.cfg.learn_cap : kLearnCapDefault;
     r.ic_ld = 0;
     a[i] = r;
   }
@@ -279,7 +279,7 @@ int plan_items(fcb_batch& b) {
         a.cdf_zrange = q.model->zrange[q.model->cur];
         v.learned = true;
       }
-      a.learn_cap = b.cfg.learn_cap > 0 ? b.cfg.learn_cap : 64;
+      a.learn_cap = b.cfg.learn_cap > 0 ? b.cfg.learn_cap : kLearnCapDefault;
       hp[j] = RicPanel{a, b.preps[i]};
       hd[j] = od;
       hi[j] = oi;
@@ -472,7 +472,7 @@ extern "C" void fcb_batch_default_config(fcb_batch_config* cfg) {
   cfg->ctas_per_sm = 0;
   cfg->concurrent = 0;
   cfg->order = 1;
-  cfg->learn_cap = 64;
+  cfg->learn_cap = kLearnCapDefault;
 }
 
 extern "C" int fcb_batch_create(const fcb_panel* panels, int npanels, int dtype_x, int dtype_r, int min_valid,
@@ -667,7 +667,7 @@ extern "C" int fcb_batch_run_per_panel(fcb_batch* b, void* stream) {
       if (lrn) {
         a.cdf_table = q.model->table[q.model->cur];
         a.cdf_zrange = q.model->zrange[q.model->cur];
-        a.learn_cap = b->cfg.learn_cap > 0 ? b->cfg.learn_cap : 64;
+        a.learn_cap = b->cfg.learn_cap > 0 ? b->cfg.learn_cap : kLearnCapDefault;
       }
       // as the single-panel entry points: several factors go through the
       // prepared returns and per-(date, factor) items, one factor per date
@@ -804,7 +804,7 @@ extern "C" int fcb_batch_autotune(fcb_batch* b, int reps, const char* cache_path
   // coordinate descent over the knobs, each alternative tried once
   const int small_opts[] = {1024, 2048, 4096};
   const int cps_opts[] = {0, 1, 2};
-  const int cap_opts[] = {32, 64, 128};
+  const int cap_opts[] = {64, 128, 256, 512};
   auto consider = [&](const fcb_batch_config& c) -> int {
     if (!valid_cfg(c)) return FCB_OK;
     b->cfg = c;

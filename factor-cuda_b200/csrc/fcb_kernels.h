@@ -24,6 +24,13 @@ struct ScanOut {
   float* out[4];  // group g output panel (T,N) or nullptr when the group is inactive
 };
 
+// Default largest bucket the learned rank path ranks itself.  A bucket of b
+// cells costs each of its cells b comparisons; above the cap the section goes
+// to the radix kernel, whose single-section latency is far larger (C2: cap 64
+// sent one section in 14616 there and took 1.215 ms per step, cap 256 none
+// and 1.195 ms).
+constexpr int kLearnCapDefault = 256;
+
 template <typename TF, typename TR>
 struct RankIcArgs {
   const TF* X;              // (F,T,N) factor panels

@@ -250,7 +250,7 @@ int fcb::rank_ic_learned_ld(const float* d_x, const float* d_r, const uint8_t* d
   int* d_status = nullptr;
   FCB_TRY(dev_status_sink(&d_status));
   RankIcArgs<float, float> a{d_x, d_r, d_fmask, d_rmask, F, T, N, min_valid, d_ranks, d_ic, nullptr, nullptr,
-                             model->table[model->cur], model->zrange[model->cur], cap > 0 ? cap : 64, d_stats,
+                             model->table[model->cur], model->zrange[model->cur], cap > 0 ? cap : kLearnCapDefault, d_stats,
                              ic_ld};
   if (F >= 2 && ric_items_fit(N)) {
     // several factors: returns prepared once per date, one CTA per (date, factor)

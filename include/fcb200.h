@@ -305,7 +305,10 @@ int fcb_cdf_grad(const float* params, const float* z, const float* u, int n, flo
  * bucket, the sum of squared bucket sizes (the per-date comparison work; m
  * for perfectly even buckets of one) and m, the number of ranked cells.
  * Sections too wide for the shared-memory kernel are ranked by the
- * global-memory radix path (same results); their statistics read 0. */
+ * global-memory radix path (same results); their statistics read 0.  cap:
+ * the largest bucket the learned kernel ranks itself; 0 = the default, 256
+ * (a bucket of b cells costs each of its cells b comparisons, far less than
+ * sending the section to the radix kernel). */
 int fcb_dev_rank_ic_panel_learned(const float* d_x, const float* d_r, const uint8_t* d_fmask,
                                   const uint8_t* d_rmask, int F, int T, int N, int min_valid, float* d_ranks,
                                   double* d_ic, const fcb_cdf_model* model, int cap, int* d_stats, void* stream);

@@ -116,7 +116,7 @@ def test_batch_contract_errors_without_device(native):
     cfg = native.FcbBatchConfig()
     lib.fcb_batch_default_config(C.byref(cfg))
     assert cfg.as_dict() == {"nt_small_max": 4096, "nt_mid_max": 8192, "ctas_per_sm": 0, "concurrent": 0,
-                             "order": 1, "learn_cap": 64}
+                             "order": 1, "learn_cap": 256}
     h = C.c_void_p()
     arr = (native.FcbPanel * 2)()
     arr[0] = native.FcbPanel(10, 500, 2, 16, 16, None, None, None, 16, None, None)
